@@ -1,0 +1,241 @@
+"""apgar_b200: B200-native batched routing search behind a C ABI.
+
+This package is a thin Python host mirror over ``libapgar_b200.so`` (the C ABI
+declared in include/apgar_b200.h).  Every search runs in the CUDA kernels of
+that library; there is no CPU fallback.  Importing works without a GPU (so the
+ABI can be inspected), but every call that needs the device raises
+``BackendError`` when the library or the device is missing.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import synth  # noqa: F401  (seeded inputs for tests and benchmarks)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libapgar_b200.so")
+
+STATUS_NAMES = {
+    0: "ok",
+    1: "unsupported",
+    2: "resource_exhausted",
+    3: "backend_failure",
+    4: "internal_invariant",
+}
+
+COMPLETION_REACHED = 0
+COMPLETION_DISCONNECTED = 1
+COMPLETION_BUDGET_EXHAUSTED = 2
+COMPLETION_CANCELLED = 3
+COMPLETION_REJECTED = 4
+UNREACHABLE = 0xFFFFFFFF
+
+
+class BackendError(RuntimeError):
+    """A C-ABI call failed; ``code`` mirrors the reference BackendErrorCode."""
+
+    def __init__(self, code: int, detail: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {detail}")
+        self.code = code
+        self.detail = detail
+
+
+class LatticeDesc(ctypes.Structure):
+    _fields_ = [
+        ("layers", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+        ("width", ctypes.c_int32),
+        ("blocked", ctypes.c_void_p),
+        ("via_ok", ctypes.c_void_p),
+        ("orth", ctypes.c_uint32),
+        ("diag", ctypes.c_uint32),
+        ("via", ctypes.c_uint32),
+    ]
+
+
+class PlanInfo(ctypes.Structure):
+    _fields_ = [
+        ("net_count", ctypes.c_uint32),
+        ("kernel_launches", ctypes.c_uint32),
+        ("class_count", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+        ("workspace_bytes", ctypes.c_uint64),
+        ("label_cells", ctypes.c_uint64),
+        ("path_arena_capacity", ctypes.c_uint64),
+    ]
+
+
+class Metadata(ctypes.Structure):
+    _fields_ = [
+        ("device_name", ctypes.c_char * 256),
+        ("device_uuid", ctypes.c_char * 40),
+        ("compute_capability_major", ctypes.c_uint32),
+        ("compute_capability_minor", ctypes.c_uint32),
+        ("runtime_version", ctypes.c_uint32),
+        ("driver_version", ctypes.c_uint32),
+        ("global_memory_bytes", ctypes.c_uint64),
+        ("multiprocessor_count", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+    ]
+
+
+RESULT_DTYPE = np.dtype(
+    [
+        ("cost", "<u4"),
+        ("completion", "<u4"),
+        ("sweeps", "<u4"),
+        ("path_len", "<u4"),
+        ("path_offset", "<u8"),
+        ("arena_offset", "<u8"),
+        ("row_steps", "<u4"),
+        ("row_stores", "<u4"),
+        ("row_loads", "<u4"),
+        ("reserved", "<u4"),
+    ]
+)
+assert RESULT_DTYPE.itemsize == 48
+
+_lib = None
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def lib():
+    """Loads libapgar_b200.so; raises BackendError if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise BackendError(3, f"CUDA library not built: {LIB_PATH} (run python -m apgar_b200.build)")
+        _lib = ctypes.CDLL(LIB_PATH)
+        _lib.apgar_b200_last_error.restype = ctypes.c_size_t
+        _lib.apgar_b200_abi_version.restype = ctypes.c_uint32
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        buf = ctypes.create_string_buffer(1024)
+        lib().apgar_b200_last_error(buf, ctypes.c_size_t(len(buf)))
+        raise BackendError(rc, buf.value.decode(errors="replace"))
+
+
+def query_metadata() -> dict:
+    m = Metadata()
+    _check(lib().apgar_b200_query_metadata(ctypes.byref(m)))
+    return {f: (getattr(m, f).decode() if isinstance(getattr(m, f), bytes) else getattr(m, f))
+            for f, _ in Metadata._fields_ if f != "reserved"}
+
+
+def _vp(a: np.ndarray | None):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+class DeviceLattice:
+    """A lattice uploaded to the current CUDA device (the prepared view)."""
+
+    def __init__(self, lat):
+        self.layers, self.height, self.width = lat.layers, lat.height, lat.width
+        self._blocked = np.ascontiguousarray(lat.blocked, dtype=np.uint32)
+        self._via = None if lat.via_ok is None else np.ascontiguousarray(lat.via_ok, np.uint32)
+        desc = LatticeDesc(lat.layers, lat.height, lat.width, _vp(self._blocked), _vp(self._via),
+                           lat.orth, lat.diag, lat.via)
+        handle = ctypes.c_void_p()
+        _check(lib().apgar_b200_lattice_upload(ctypes.byref(desc), ctypes.byref(handle)))
+        self.handle = handle
+
+    def close(self):
+        if self.handle:
+            lib().apgar_b200_lattice_release(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def route(self, nets: np.ndarray, max_sweeps: int = 4096, cancel: np.ndarray | None = None,
+              want_paths: bool = True, path_capacity: int | None = None, out=None):
+        """Searches every net; returns (results record array, packed paths).
+
+        ``out`` may supply preallocated (results, paths) host arrays (pinned
+        memory makes the transfers faster)."""
+        nets = np.ascontiguousarray(nets)
+        count = len(nets)
+        if out is not None:
+            results, paths = out
+        else:
+            results = np.empty(count, dtype=RESULT_DTYPE)
+            cap = path_capacity or int(8 * (nets["win_w"].astype(np.int64)
+                                            + nets["win_h"].astype(np.int64)).sum() + 64 * self.layers * count + 64)
+            paths = np.empty(cap if want_paths else 0, dtype=np.uint32)
+        total = ctypes.c_uint64(0)
+        _check(lib().apgar_b200_lattice_route(
+            self.handle, _vp(nets), ctypes.c_uint32(count), ctypes.c_uint32(max_sweeps),
+            _vp(cancel), _vp(results), _vp(paths) if want_paths else None,
+            ctypes.c_uint64(paths.size if want_paths else 0), ctypes.byref(total)))
+        return results, (paths[: total.value] if want_paths else None)
+
+    def plan(self, nets: np.ndarray, max_sweeps: int = 4096) -> "Plan":
+        return Plan(self, nets, max_sweeps)
+
+
+class Plan:
+    """A planned batch resident on the device (execute may be graph-captured)."""
+
+    def __init__(self, lattice: DeviceLattice, nets: np.ndarray, max_sweeps: int):
+        self.lattice = lattice
+        self.nets = np.ascontiguousarray(nets)
+        handle = ctypes.c_void_p()
+        _check(lib().apgar_b200_lattice_plan(lattice.handle, _vp(self.nets),
+                                             ctypes.c_uint32(len(self.nets)),
+                                             ctypes.c_uint32(max_sweeps), ctypes.byref(handle)))
+        self.handle = handle
+
+    def execute(self, stream: int = 0) -> None:
+        _check(lib().apgar_b200_lattice_execute(self.handle, ctypes.c_void_p(stream)))
+
+    def info(self) -> dict:
+        info = PlanInfo()
+        _check(lib().apgar_b200_lattice_plan_info(self.handle, ctypes.byref(info)))
+        return {f: getattr(info, f) for f, _ in PlanInfo._fields_ if f != "reserved"}
+
+    def readback(self, want_paths: bool = True):
+        count = len(self.nets)
+        results = np.empty(count, dtype=RESULT_DTYPE)
+        cap = int(self.info()["path_arena_capacity"]) if want_paths else 0
+        paths = np.empty(cap, dtype=np.uint32)
+        total = ctypes.c_uint64(0)
+        _check(lib().apgar_b200_lattice_readback(self.handle, _vp(results),
+                                                 _vp(paths) if want_paths else None,
+                                                 ctypes.c_uint64(cap), ctypes.byref(total)))
+        return results, (paths[: total.value] if want_paths else None)
+
+    def close(self):
+        if self.handle:
+            lib().apgar_b200_lattice_plan_release(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def split_paths(results: np.ndarray, paths: np.ndarray) -> list:
+    """Per-net reverse paths (goal first) from the packed array."""
+    out = []
+    for r in results:
+        if r["completion"] == COMPLETION_REACHED:
+            o = int(r["path_offset"])
+            out.append(paths[o:o + int(r["path_len"])])
+        else:
+            out.append(None)
+    return out

@@ -1,0 +1,66 @@
+// Shared definitions for the lattice-mode kernels (dense bit-packed layers,
+// per-net windows, uint32 labels, bend 0, vias).
+//
+// Move model (identical to the CPU oracle):
+//   orthogonal move legal iff both cells are free;
+//   diagonal move legal iff both cells and both side cells are free;
+//   via (l,x,y)<->(l+1,x,y) legal iff both cells are free and the via bit of
+//   layer pair l is set (no via mask = all set);
+//   a cell is free iff it is inside the net window and not blocked.
+#pragma once
+
+#include <cstdint>
+
+#include "apgar_b200.h"
+
+namespace apgar_b200 {
+
+// Labels inside the kernels use 0x7FFFFFFF as "unreachable" so that
+// label + cost never wraps in 32-bit arithmetic; the host admits a net only
+// when (window cells) * (largest move cost) stays below this sentinel.
+constexpr uint32_t kLabelInf = 0x7FFFFFFFu;
+constexpr int kMaxLayers = 8;
+
+struct LatticeDeviceView {
+  const uint32_t* blocked;  // [layers][height][words]
+  const uint32_t* via_ok;   // [layers-1][height][words] or nullptr
+  int32_t layers, height, width, words;
+  uint32_t orth, diag, via;
+};
+
+// Per-net workspace record produced by the host planner.
+struct NetPlan {
+  uint32_t net;         // index into the caller's net array
+  uint32_t pitch;       // row pitch in cells (multiple of 4)
+  uint64_t dist_offset; // cell offset of this net's label slab in the pool
+  uint64_t mat_offset;  // word offset of this net's materialised-row bitmap
+};
+
+struct SweepLaunch {
+  LatticeDeviceView lat;
+  const apgar_b200_lattice_net* nets;
+  const NetPlan* plans;
+  uint32_t plan_count;
+  uint32_t max_sweeps;
+  uint32_t* dist_pool;
+  uint32_t* mat_pool;
+  apgar_b200_lattice_result* results;
+  uint32_t* path_arena;
+  uint64_t path_arena_capacity;
+  unsigned long long* arena_cursor;
+  const volatile uint32_t* cancel;  // host-mapped flag or nullptr
+};
+
+__device__ __forceinline__ uint32_t sat(uint32_t v) { return v < kLabelInf ? v : kLabelInf; }
+
+// 32 bits of a bit-packed row starting at signed bit position `pos`; bits
+// outside [0, words*32) read as 1 (blocked).
+__device__ __forceinline__ uint32_t fetch_bits32(const uint32_t* row, int words, int pos) {
+  const int wi = pos >= 0 ? (pos >> 5) : -(((-pos) + 31) >> 5);
+  const int sh = pos - wi * 32;
+  const uint32_t lo = (wi >= 0 && wi < words) ? __ldg(row + wi) : 0xFFFFFFFFu;
+  const uint32_t hi = (wi + 1 >= 0 && wi + 1 < words) ? __ldg(row + wi + 1) : 0xFFFFFFFFu;
+  return __funnelshift_r(lo, hi, sh);
+}
+
+}  // namespace apgar_b200

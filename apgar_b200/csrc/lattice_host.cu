@@ -1,0 +1,456 @@
+// Host side of lattice mode: lattice upload (the prepared view), the batch
+// planner (admission, width classes, label-slab layout, LPT order) and the
+// C-ABI entry points.  No CPU search fallback exists: every admitted net is
+// searched by the CUDA kernels in lattice_sweep.cu.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "host_common.h"
+#include "lattice_common.cuh"
+
+namespace apgar_b200 {
+
+size_t lattice_sweep_smem_bytes(int cells_per_lane, int layers, int max_rows);
+cudaError_t launch_lattice_sweep(int cells_per_lane, const SweepLaunch& launch, int layers,
+                                 int max_rows, cudaStream_t stream);
+cudaError_t launch_lattice_pack(apgar_b200_lattice_result* results, uint32_t count,
+                                unsigned long long* total, const uint32_t* arena, uint32_t* paths,
+                                int sm_count, cudaStream_t stream);
+
+namespace {
+
+constexpr int kClasses[] = {4, 8, 16, 32, 64};
+constexpr int kClassCount = 5;
+constexpr size_t kMaxSmemPerBlock = 227 * 1024;
+
+struct LatticeObject;
+
+struct ClassRange {
+  int cells_per_lane = 0;
+  uint32_t begin = 0;  // into plans
+  uint32_t count = 0;
+  int max_rows = 0;
+};
+
+struct PlanObject {
+  LatticeObject* lattice = nullptr;
+  int device = -1;
+  int sm_count = 0;
+  uint32_t count = 0;
+  uint32_t max_sweeps = 0;
+  uint32_t* cancel_host = nullptr;  // pinned, mapped; polled by the kernels
+  uint32_t* cancel_dev = nullptr;
+  std::vector<ClassRange> classes;
+  std::vector<apgar_b200_lattice_result> rejected_template;
+  DeviceBuffer<apgar_b200_lattice_net> nets;
+  DeviceBuffer<NetPlan> plans;
+  DeviceBuffer<uint32_t> dist_pool;
+  DeviceBuffer<apgar_b200_lattice_result> results;
+  DeviceBuffer<uint32_t> arena;
+  DeviceBuffer<uint32_t> paths;
+  DeviceBuffer<unsigned long long> counters;  // [0] arena cursor, [1] packed total
+  uint64_t label_cells = 0;
+  uint64_t arena_capacity = 0;
+  cudaStream_t class_streams[kClassCount] = {};
+  cudaEvent_t fork = nullptr;
+  cudaEvent_t joins[kClassCount] = {};
+
+  ~PlanObject() {
+    for (cudaStream_t& s : class_streams) {
+      if (s != nullptr) cudaStreamDestroy(s);
+    }
+    for (cudaEvent_t& e : joins) {
+      if (e != nullptr) cudaEventDestroy(e);
+    }
+    if (fork != nullptr) cudaEventDestroy(fork);
+    if (cancel_host != nullptr) cudaFreeHost(cancel_host);
+  }
+
+  uint64_t workspace_bytes() const {
+    return nets.bytes() + plans.bytes() + dist_pool.bytes() + results.bytes() + arena.bytes() +
+           paths.bytes() + counters.bytes();
+  }
+};
+
+struct LatticeObject {
+  int device = -1;
+  LatticeDeviceView view{};
+  DeviceBuffer<uint32_t> blocked;
+  DeviceBuffer<uint32_t> via_ok;
+  std::mutex route_mutex;
+  std::unique_ptr<PlanObject> route_plan;  // reusable workspace for route()
+};
+
+int check_device(int expected) {
+  int current = -1;
+  APGAR_B200_CUDA("cudaGetDevice", cudaGetDevice(&current));
+  if (current != expected) {
+    return set_error(APGAR_B200_BACKEND_FAILURE,
+                     "current CUDA device differs from the device the lattice was uploaded on");
+  }
+  return APGAR_B200_OK;
+}
+
+int class_for_width(uint32_t w) {
+  for (int c : kClasses) {
+    if (static_cast<uint32_t>(c) * 32u >= w) return c;
+  }
+  return 0;
+}
+
+// Builds (or rebuilds into existing buffers) a plan for `nets`.
+int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint32_t count,
+               uint32_t max_sweeps, PlanObject* plan) {
+  const LatticeDeviceView& v = lat->view;
+  plan->lattice = lat;
+  plan->device = lat->device;
+  plan->count = count;
+  plan->max_sweeps = max_sweeps;
+  APGAR_B200_CUDA("cudaDeviceGetAttribute",
+                  cudaDeviceGetAttribute(&plan->sm_count, cudaDevAttrMultiProcessorCount,
+                                         lat->device));
+  const uint64_t max_move = std::max(v.orth, std::max(v.diag, v.via));
+
+  std::vector<std::vector<uint32_t>> members(kClassCount);
+  std::vector<apgar_b200_lattice_result> init(count);
+  std::memset(init.data(), 0, init.size() * sizeof(apgar_b200_lattice_result));
+  for (uint32_t i = 0; i < count; ++i) {
+    const apgar_b200_lattice_net& n = host_nets[i];
+    apgar_b200_lattice_result& r = init[i];
+    r.cost = APGAR_B200_UNREACHABLE;
+    r.completion = APGAR_B200_COMPLETION_REJECTED;
+    const bool in_lattice =
+        n.start_layer < static_cast<uint32_t>(v.layers) &&
+        n.goal_layer < static_cast<uint32_t>(v.layers) && n.win_w > 0 && n.win_h > 0 &&
+        static_cast<uint64_t>(n.win_x0) + n.win_w <= static_cast<uint64_t>(v.width) &&
+        static_cast<uint64_t>(n.win_y0) + n.win_h <= static_cast<uint64_t>(v.height) &&
+        n.start_x >= n.win_x0 && n.start_x < n.win_x0 + n.win_w && n.start_y >= n.win_y0 &&
+        n.start_y < n.win_y0 + n.win_h && n.goal_x >= n.win_x0 && n.goal_x < n.win_x0 + n.win_w &&
+        n.goal_y >= n.win_y0 && n.goal_y < n.win_y0 + n.win_h;
+    if (!in_lattice) continue;
+    const uint64_t cells = static_cast<uint64_t>(v.layers) * n.win_w * n.win_h;
+    if (cells * max_move >= kLabelInf) continue;  // uint32 cost domain not provable
+    const int c = class_for_width(n.win_w);
+    if (c == 0 || n.win_h > 32000u) continue;
+    int ci = 0;
+    while (kClasses[ci] != c) ++ci;
+    members[ci].push_back(i);
+  }
+  plan->rejected_template = init;
+
+  std::vector<NetPlan> plans;
+  plans.reserve(count);
+  plan->classes.clear();
+  uint64_t dist_cells = 0;
+  uint64_t arena_cells = 0;
+  for (int ci = 0; ci < kClassCount; ++ci) {
+    std::vector<uint32_t>& m = members[ci];
+    if (m.empty()) continue;
+    // longest-processing-time first: larger windows launch first
+    std::stable_sort(m.begin(), m.end(), [&](uint32_t a, uint32_t b) {
+      const uint64_t ca = static_cast<uint64_t>(host_nets[a].win_w) * host_nets[a].win_h;
+      const uint64_t cb = static_cast<uint64_t>(host_nets[b].win_w) * host_nets[b].win_h;
+      return ca > cb;
+    });
+    ClassRange range;
+    range.cells_per_lane = kClasses[ci];
+    range.begin = static_cast<uint32_t>(plans.size());
+    range.count = static_cast<uint32_t>(m.size());
+    for (uint32_t i : m) {
+      const apgar_b200_lattice_net& n = host_nets[i];
+      NetPlan np{};
+      np.net = i;
+      np.pitch = (n.win_w + 3u) & ~3u;
+      np.dist_offset = dist_cells;
+      np.mat_offset = 0;
+      dist_cells += static_cast<uint64_t>(v.layers) * n.win_h * np.pitch;
+      arena_cells += 8ull * (n.win_w + n.win_h) + 64ull * v.layers;
+      range.max_rows = std::max(range.max_rows, static_cast<int>(n.win_h));
+      plans.push_back(np);
+    }
+    if (lattice_sweep_smem_bytes(range.cells_per_lane, v.layers, range.max_rows) >
+        kMaxSmemPerBlock) {
+      return set_error(APGAR_B200_UNSUPPORTED, "window too tall for the shared-memory row map");
+    }
+    plan->classes.push_back(range);
+  }
+  plan->label_cells = dist_cells;
+  plan->arena_capacity = std::max<uint64_t>(arena_cells, 64);
+
+  APGAR_B200_CUDA("cudaMalloc(nets)", plan->nets.ensure(std::max<uint32_t>(count, 1)));
+  APGAR_B200_CUDA("cudaMalloc(plans)", plan->plans.ensure(std::max<size_t>(plans.size(), 1)));
+  APGAR_B200_CUDA("cudaMalloc(label slabs)", plan->dist_pool.ensure(std::max<uint64_t>(dist_cells, 4)));
+  APGAR_B200_CUDA("cudaMalloc(results)", plan->results.ensure(std::max<uint32_t>(count, 1)));
+  APGAR_B200_CUDA("cudaMalloc(path arena)", plan->arena.ensure(plan->arena_capacity));
+  APGAR_B200_CUDA("cudaMalloc(paths)", plan->paths.ensure(plan->arena_capacity));
+  APGAR_B200_CUDA("cudaMalloc(counters)", plan->counters.ensure(2));
+  if (count > 0) {
+    APGAR_B200_CUDA("cudaMemcpy(nets)",
+                    cudaMemcpy(plan->nets.get(), host_nets, count * sizeof(apgar_b200_lattice_net),
+                               cudaMemcpyHostToDevice));
+    APGAR_B200_CUDA("cudaMemcpy(results init)",
+                    cudaMemcpy(plan->results.get(), init.data(),
+                               count * sizeof(apgar_b200_lattice_result), cudaMemcpyHostToDevice));
+  }
+  if (!plans.empty()) {
+    APGAR_B200_CUDA("cudaMemcpy(plans)",
+                    cudaMemcpy(plan->plans.get(), plans.data(), plans.size() * sizeof(NetPlan),
+                               cudaMemcpyHostToDevice));
+  }
+  for (int ci = 0; ci < kClassCount; ++ci) {
+    if (plan->class_streams[ci] == nullptr) {
+      APGAR_B200_CUDA("cudaStreamCreate",
+                      cudaStreamCreateWithFlags(&plan->class_streams[ci], cudaStreamNonBlocking));
+      APGAR_B200_CUDA("cudaEventCreate",
+                      cudaEventCreateWithFlags(&plan->joins[ci], cudaEventDisableTiming));
+    }
+  }
+  if (plan->fork == nullptr) {
+    APGAR_B200_CUDA("cudaEventCreate", cudaEventCreateWithFlags(&plan->fork, cudaEventDisableTiming));
+  }
+  if (plan->cancel_host == nullptr) {
+    void* h = nullptr;
+    APGAR_B200_CUDA("cudaHostAlloc(cancel flag)",
+                    cudaHostAlloc(&h, sizeof(uint32_t), cudaHostAllocMapped));
+    plan->cancel_host = static_cast<uint32_t*>(h);
+    void* d = nullptr;
+    APGAR_B200_CUDA("cudaHostGetDevicePointer(cancel flag)",
+                    cudaHostGetDevicePointer(&d, h, 0));
+    plan->cancel_dev = static_cast<uint32_t*>(d);
+  }
+  *reinterpret_cast<volatile uint32_t*>(plan->cancel_host) = 0u;
+  return APGAR_B200_OK;
+}
+
+int execute_plan(PlanObject* plan, cudaStream_t stream) {
+  if (int rc = check_device(plan->device); rc != APGAR_B200_OK) return rc;
+  APGAR_B200_CUDA("cudaMemsetAsync(counters)",
+                  cudaMemsetAsync(plan->counters.get(), 0, 2 * sizeof(unsigned long long), stream));
+  const LatticeDeviceView& v = plan->lattice->view;
+  SweepLaunch base{};
+  base.lat = v;
+  base.nets = plan->nets.get();
+  base.max_sweeps = plan->max_sweeps;
+  base.dist_pool = plan->dist_pool.get();
+  base.mat_pool = nullptr;
+  base.results = plan->results.get();
+  base.path_arena = plan->arena.get();
+  base.path_arena_capacity = plan->arena_capacity;
+  base.arena_cursor = plan->counters.get();
+  base.cancel = plan->cancel_dev;
+  const bool fan_out = plan->classes.size() > 1;
+  if (fan_out) APGAR_B200_CUDA("cudaEventRecord(fork)", cudaEventRecord(plan->fork, stream));
+  for (size_t k = 0; k < plan->classes.size(); ++k) {
+    const ClassRange& c = plan->classes[k];
+    SweepLaunch launch = base;
+    launch.plans = plan->plans.get() + c.begin;
+    launch.plan_count = c.count;
+    cudaStream_t s = stream;
+    if (fan_out) {
+      s = plan->class_streams[k];
+      APGAR_B200_CUDA("cudaStreamWaitEvent", cudaStreamWaitEvent(s, plan->fork, 0));
+    }
+    APGAR_B200_CUDA("lattice sweep launch",
+                    launch_lattice_sweep(c.cells_per_lane, launch, v.layers, c.max_rows, s));
+    if (fan_out) {
+      APGAR_B200_CUDA("cudaEventRecord(join)", cudaEventRecord(plan->joins[k], s));
+      APGAR_B200_CUDA("cudaStreamWaitEvent", cudaStreamWaitEvent(stream, plan->joins[k], 0));
+    }
+  }
+  APGAR_B200_CUDA("lattice pack launch",
+                  launch_lattice_pack(plan->results.get(), plan->count, plan->counters.get() + 1,
+                                      plan->arena.get(), plan->paths.get(), plan->sm_count, stream));
+  return APGAR_B200_OK;
+}
+
+int readback_plan(PlanObject* plan, apgar_b200_lattice_result* results, uint32_t* paths,
+                  uint64_t path_capacity, uint64_t* path_total) {
+  if (int rc = check_device(plan->device); rc != APGAR_B200_OK) return rc;
+  unsigned long long total = 0;
+  APGAR_B200_CUDA("cudaMemcpy(path total)",
+                  cudaMemcpy(&total, plan->counters.get() + 1, sizeof(total), cudaMemcpyDeviceToHost));
+  if (results != nullptr && plan->count > 0) {
+    APGAR_B200_CUDA("cudaMemcpy(results)",
+                    cudaMemcpy(results, plan->results.get(),
+                               plan->count * sizeof(apgar_b200_lattice_result),
+                               cudaMemcpyDeviceToHost));
+  }
+  if (path_total != nullptr) *path_total = total;
+  if (paths != nullptr && total > 0) {
+    if (total > path_capacity) {
+      return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "path output buffer is too small");
+    }
+    APGAR_B200_CUDA("cudaMemcpy(paths)", cudaMemcpy(paths, plan->paths.get(),
+                                                    total * sizeof(uint32_t),
+                                                    cudaMemcpyDeviceToHost));
+  }
+  return APGAR_B200_OK;
+}
+
+}  // namespace
+}  // namespace apgar_b200
+
+using namespace apgar_b200;
+
+extern "C" int apgar_b200_lattice_upload(const apgar_b200_lattice_desc* d, void** out) {
+  if (d == nullptr || out == nullptr || d->blocked == nullptr) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "lattice upload received a null argument");
+  }
+  if (d->layers < 1 || d->layers > kMaxLayers || d->height < 1 || d->width < 32 ||
+      d->width % 32 != 0 || d->orth == 0 || d->diag == 0 || d->via == 0 ||
+      d->orth > 0xFFFFu || d->diag > 0xFFFFu || d->via > 0xFFFFu) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT,
+                     "lattice upload rejected layer count, dimensions or move costs");
+  }
+  try {
+    auto lat = std::make_unique<LatticeObject>();
+    APGAR_B200_CUDA("cudaGetDevice", cudaGetDevice(&lat->device));
+    const size_t words = static_cast<size_t>(d->width / 32);
+    const size_t plane = static_cast<size_t>(d->height) * words;
+    const size_t blocked_words = plane * d->layers;
+    APGAR_B200_CUDA("cudaMalloc(blocked)", lat->blocked.ensure(blocked_words));
+    APGAR_B200_CUDA("cudaMemcpy(blocked)",
+                    cudaMemcpy(lat->blocked.get(), d->blocked, blocked_words * sizeof(uint32_t),
+                               cudaMemcpyHostToDevice));
+    if (d->via_ok != nullptr && d->layers > 1) {
+      const size_t via_words = plane * (d->layers - 1);
+      APGAR_B200_CUDA("cudaMalloc(via)", lat->via_ok.ensure(via_words));
+      APGAR_B200_CUDA("cudaMemcpy(via)",
+                      cudaMemcpy(lat->via_ok.get(), d->via_ok, via_words * sizeof(uint32_t),
+                                 cudaMemcpyHostToDevice));
+    }
+    lat->view.blocked = lat->blocked.get();
+    lat->view.via_ok = lat->via_ok.get();
+    lat->view.layers = d->layers;
+    lat->view.height = d->height;
+    lat->view.width = d->width;
+    lat->view.words = static_cast<int32_t>(words);
+    lat->view.orth = d->orth;
+    lat->view.diag = d->diag;
+    lat->view.via = d->via;
+    *out = lat.release();
+    clear_error();
+    return APGAR_B200_OK;
+  } catch (const std::bad_alloc&) {
+    return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "host allocation failed during upload");
+  }
+}
+
+extern "C" int apgar_b200_lattice_release(void* lattice) {
+  delete static_cast<LatticeObject*>(lattice);
+  return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_lattice_plan(void* lattice, const apgar_b200_lattice_net* nets,
+                                       uint32_t count, uint32_t max_sweeps, void** out_plan) {
+  if (lattice == nullptr || out_plan == nullptr || (count > 0 && nets == nullptr) ||
+      max_sweeps == 0 || max_sweeps > 30000) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "lattice plan received invalid arguments");
+  }
+  auto* lat = static_cast<LatticeObject*>(lattice);
+  if (int rc = check_device(lat->device); rc != APGAR_B200_OK) return rc;
+  try {
+    auto plan = std::make_unique<PlanObject>();
+    if (int rc = build_plan(lat, nets, count, max_sweeps, plan.get()); rc != APGAR_B200_OK) {
+      return rc;
+    }
+    *out_plan = plan.release();
+    clear_error();
+    return APGAR_B200_OK;
+  } catch (const std::bad_alloc&) {
+    return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "host allocation failed during planning");
+  }
+}
+
+extern "C" int apgar_b200_lattice_execute(void* plan, void* stream) {
+  if (plan == nullptr) return set_error(APGAR_B200_INTERNAL_INVARIANT, "null plan");
+  const int rc = execute_plan(static_cast<PlanObject*>(plan), static_cast<cudaStream_t>(stream));
+  if (rc == APGAR_B200_OK) clear_error();
+  return rc;
+}
+
+extern "C" int apgar_b200_lattice_readback(void* plan, apgar_b200_lattice_result* results,
+                                           uint32_t* paths, uint64_t path_capacity,
+                                           uint64_t* path_total) {
+  if (plan == nullptr) return set_error(APGAR_B200_INTERNAL_INVARIANT, "null plan");
+  const int rc = readback_plan(static_cast<PlanObject*>(plan), results, paths, path_capacity,
+                               path_total);
+  if (rc == APGAR_B200_OK) clear_error();
+  return rc;
+}
+
+extern "C" int apgar_b200_lattice_device_results(void* plan,
+                                                 const apgar_b200_lattice_result** results,
+                                                 const uint32_t** paths) {
+  if (plan == nullptr) return set_error(APGAR_B200_INTERNAL_INVARIANT, "null plan");
+  auto* p = static_cast<PlanObject*>(plan);
+  if (results != nullptr) *results = p->results.get();
+  if (paths != nullptr) *paths = p->paths.get();
+  return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_lattice_plan_info(void* plan, apgar_b200_plan_info* out) {
+  if (plan == nullptr || out == nullptr) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "null plan or output");
+  }
+  auto* p = static_cast<PlanObject*>(plan);
+  std::memset(out, 0, sizeof(*out));
+  out->net_count = p->count;
+  out->class_count = static_cast<uint32_t>(p->classes.size());
+  out->kernel_launches = out->class_count + (p->count > 0 ? 2u : 0u);
+  out->workspace_bytes = p->workspace_bytes();
+  out->label_cells = p->label_cells;
+  out->path_arena_capacity = p->arena_capacity;
+  return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_lattice_plan_release(void* plan) {
+  delete static_cast<PlanObject*>(plan);
+  return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_lattice_route(void* lattice, const apgar_b200_lattice_net* nets,
+                                        uint32_t count, uint32_t max_sweeps,
+                                        const volatile uint32_t* cancel,
+                                        apgar_b200_lattice_result* results, uint32_t* paths,
+                                        uint64_t path_capacity, uint64_t* path_total) {
+  if (lattice == nullptr || (count > 0 && nets == nullptr) || results == nullptr ||
+      max_sweeps == 0 || max_sweeps > 30000) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "lattice route received invalid arguments");
+  }
+  auto* lat = static_cast<LatticeObject*>(lattice);
+  if (int rc = check_device(lat->device); rc != APGAR_B200_OK) return rc;
+  try {
+    std::scoped_lock lock(lat->route_mutex);
+    if (lat->route_plan == nullptr) lat->route_plan = std::make_unique<PlanObject>();
+    PlanObject* plan = lat->route_plan.get();
+    if (int rc = build_plan(lat, nets, count, max_sweeps, plan); rc != APGAR_B200_OK) return rc;
+    *reinterpret_cast<volatile uint32_t*>(plan->cancel_host) = 0u;
+    if (int rc = execute_plan(plan, nullptr); rc != APGAR_B200_OK) return rc;
+    // The caller's flag is sampled on the host while the batch runs and is
+    // forwarded through the plan's own mapped flag, which the kernels poll
+    // between sweeps (the kernels never dereference caller memory).
+    for (;;) {
+      const cudaError_t q = cudaStreamQuery(nullptr);
+      if (q == cudaSuccess) break;
+      if (q != cudaErrorNotReady) return cuda_failure("cudaStreamQuery(route)", q);
+      if (cancel != nullptr && *cancel != 0u) {
+        *reinterpret_cast<volatile uint32_t*>(plan->cancel_host) = 1u;
+      }
+      std::this_thread::yield();
+    }
+    const int rc = readback_plan(plan, results, paths, path_capacity, path_total);
+    if (rc == APGAR_B200_OK) clear_error();
+    return rc;
+  } catch (const std::bad_alloc&) {
+    return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "host allocation failed during routing");
+  }
+}

@@ -1,0 +1,342 @@
+#!/usr/bin/env python
+"""Benchmark: certified-optimal nets/s of the batched lattice search on B200.
+
+Workload (the medium lattice configuration, the largest that is quoted on one
+GPU): 4 layers of 2048x2048 cells, 25% blocked (rectangles + pad keep-outs),
+4096 two-terminal nets with lognormal(200, 1.0) half-perimeter, each searched
+in its bbox + 32 window with uint32 labels and bit-packed masks.  Synthetic,
+seeded inputs (no public dataset exists for this path).
+
+One step = one batched search of all nets of the batch (plain batched sweep:
+exact labels + canonical reverse paths for every net).  A net is certified when
+its search converged (reached or proved disconnected inside its window).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun every rank searches its own batch (same lattice, rank-specific
+net seed): weak scaling, no data-path collective; the timed region is
+bracketed by a barrier and synchronize and reported as the max over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "certified-optimal nets/sec on 1 B200: learned+batched vs plain sweep"
+UNIT = "nets/s"
+WORKLOAD = ("medium lattice: 4 layers x 2048x2048, 25% blocked (rectangles + 4x4 pad keep-outs "
+            "on a 20-cell pitch), 4096 two-terminal nets, half-perimeter lognormal(median 200, "
+            "sigma 1.0), bbox+32 windows, costs orth 10 / diag 14 / via 50, bend 0")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--size", type=int, default=2048)
+    ap.add_argument("--nets", type=int, default=4096)
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--cpu-sample", type=int, default=512,
+                    help="nets timed by the CPU baseline (bounded sample)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    """DRAM bytes per sweep launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "lattice_sweep_traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during timing."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"apgar_b200_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.out.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return None
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def certified(results):
+    import apgar_b200
+
+    c = results["completion"]
+    return int(np.count_nonzero((c == apgar_b200.COMPLETION_REACHED)
+                                | (c == apgar_b200.COMPLETION_DISCONNECTED)))
+
+
+def algorithmic_bytes(lat, nets, results):
+    """Bytes the sweep schedule must move (see the DESIGN roofline section).
+
+    Per processed window row: the layer rows read and written (4 B per cell of
+    the window width) plus the obstacle and via bits (2 bits per cell per
+    layer); plus 4 B per emitted path cell.  The per-net row counters are the
+    CPU restatement's counts (the GPU tests check they are identical)."""
+    w = nets["win_w"].astype(np.float64)
+    rows_moved = results["row_loads"].astype(np.float64) + results["row_stores"].astype(np.float64)
+    label_bytes = (4.0 * w * rows_moved).sum()
+    mask_bytes = (results["row_steps"].astype(np.float64) * lat.layers * w * 2.0 / 8.0).sum()
+    path_bytes = 4.0 * results["path_len"].astype(np.float64).sum()
+    one_pass = (nets["win_w"].astype(np.float64) * nets["win_h"] * lat.layers * 4.25).sum()
+    return label_bytes + mask_bytes + path_bytes, one_pass
+
+
+def cpu_baseline(lat, nets, sample: int):
+    """The CPU A* port (reference RouteWithCpuAStar restated with vias), all host
+    threads, on a bounded sample of the same nets."""
+    import oracle
+
+    threads = os.cpu_count() or 1
+    sub = np.ascontiguousarray(nets[:sample])
+    t0 = time.perf_counter()
+    costs = oracle.astar_batch(lat, sub, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": len(sub) / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"first {len(sub)} of the {len(nets)} nets, A* port of RouteWithCpuAStar "
+                      f"(cpu_astar.cc:323-638) extended with vias, {threads} threads, {dt:.2f} s"}, costs
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    import oracle
+    from apgar_b200 import synth
+
+    lat, nets = synth.config_medium(args.seed, nets=args.nets, size=args.size)
+    threads = os.cpu_count() or 1
+    sample = np.ascontiguousarray(nets[: args.cpu_sample])
+    for _ in range(args.warmup):
+        oracle.astar_batch(lat, sample[:64], threads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.astar_batch(lat, sample, threads=threads)
+    dt = time.perf_counter() - t0
+    value = len(sample) * args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1000.0 / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "step": f"A* over {len(sample)} nets of the batch"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{len(sample)} nets per step, all {threads} host threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    import apgar_b200
+    from apgar_b200 import synth
+
+    lat, nets = synth.config_medium(args.seed, nets=args.nets, size=args.size)
+    if world > 1 and rank > 0:
+        nets = synth.make_nets(lat, args.seed + 1000 + 7919 * rank, args.nets, hpwl_median=200.0,
+                               hpwl_sigma=1.0)
+    dev = apgar_b200.DeviceLattice(lat)
+    plan = dev.plan(nets)
+    info = plan.info()
+    stream = torch.cuda.current_stream()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---------------- device-resident throughput (value) ----------------
+    for _ in range(max(args.warmup, 3)):
+        plan.execute(stream.cuda_stream)
+    barrier()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    with ClockSampler(local) as clocks:
+        barrier()
+        for i in range(args.steps):
+            starts[i].record(stream)
+            plan.execute(stream.cuda_stream)
+            ends[i].record(stream)
+        barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = starts[0].elapsed_time(ends[-1])
+    results, paths = plan.readback()
+    cert = certified(results)
+    if dist is not None:
+        t = torch.tensor([total_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+        c = torch.tensor([cert], device="cuda", dtype=torch.int64)
+        dist.all_reduce(c)
+        cert_all = int(c.item())
+    else:
+        cert_all = cert
+    value = cert_all * args.steps / (total_ms / 1000.0)
+
+    # ---------------- end to end through the public API (e2e) ----------------
+    pinned_nets = torch.from_numpy(nets.view(np.uint8)).pin_memory()
+    nets_host = pinned_nets.numpy().view(synth.NET_DTYPE)
+    res_host = torch.empty(len(nets) * apgar_b200.RESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+    res_arr = res_host.numpy().view(apgar_b200.RESULT_DTYPE)
+    path_host = torch.empty(int(info["path_arena_capacity"]), dtype=torch.int32).pin_memory()
+    path_arr = path_host.numpy().view(np.uint32)
+    for _ in range(2):
+        dev.route(nets_host, out=(res_arr, path_arr))
+    barrier()
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_end = torch.cuda.Event(enable_timing=True)
+    path_cells = 0
+    e_start.record()
+    for _ in range(args.steps):
+        r, p = dev.route(nets_host, out=(res_arr, path_arr))
+        path_cells = len(p)
+    e_end.record()
+    barrier()
+    e2e_ms = e_start.elapsed_time(e_end)
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = cert_all * args.steps / (e2e_ms / 1000.0)
+    h2d = nets.nbytes
+    d2h = len(nets) * apgar_b200.RESULT_DTYPE.itemsize + 4 * path_cells + 8
+
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        bytes_alg, one_pass = algorithmic_bytes(lat, nets, results)
+        avg_ms = total_ms / args.steps
+        achieved = bytes_alg / (avg_ms / 1000.0) / 1e9
+        traffic = load_traffic()
+        cl = clocks.summary()
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": avg_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
+            "config": {
+                "workload": WORKLOAD, "form": "plain batched sweep",
+                "nets_per_gpu": len(nets), "lattice": [lat.layers, lat.height, lat.width],
+                "seed": args.seed, "parallelism": f"weak x{world} (independent net batches)",
+                "l2": "label slabs larger than L2 (126 MB) every step",
+                "label_slab_bytes": int(info["label_cells"]) * 4,
+                "certified_per_step": cert_all,
+            },
+            "gpu_launches": int(info["kernel_launches"]) * args.steps,
+            "roofline": {
+                "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind,
+                "traffic": (traffic or {}).get("dram_bytes_per_launch"),
+                "bytes_alg_per_step": bytes_alg, "one_pass_bytes_per_step": one_pass,
+            },
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms / args.steps},
+            "clocks": cl,
+            "step_ms_min_max": [min(step_ms), max(step_ms)],
+            "sweeps_mean": float(results["sweeps"].mean()),
+        }
+        if not args.no_cpu_baseline and world == 1:
+            line["cpu_baseline"], cpu_costs = cpu_baseline(lat, nets, args.cpu_sample)
+            ok = results["completion"][: args.cpu_sample] != apgar_b200.COMPLETION_REJECTED
+            line["cpu_baseline"]["costs_match_gpu"] = bool(
+                np.array_equal(cpu_costs[ok], results["cost"][: args.cpu_sample][ok]))
+        print(json.dumps(line), flush=True)
+    plan.close()
+    dev.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

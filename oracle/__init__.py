@@ -1,0 +1,195 @@
+"""ctypes binding for the CPU oracle.  TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference arm
+may import this package; the product (apgar_b200) never does.  See oracle.h for
+what each routine restates and which reference file:line it follows.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle.so")
+_lib = None
+
+U32P = ctypes.POINTER(ctypes.c_uint32)
+U64P = ctypes.POINTER(ctypes.c_uint64)
+
+
+class LoLattice(ctypes.Structure):
+    _fields_ = [
+        ("layers", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+        ("width", ctypes.c_int32),
+        ("blocked", U32P),
+        ("via_ok", U32P),
+        ("orth", ctypes.c_uint32),
+        ("diag", ctypes.c_uint32),
+        ("via", ctypes.c_uint32),
+    ]
+
+
+class LoSweepStats(ctypes.Structure):
+    _fields_ = [
+        ("sweeps", ctypes.c_uint32),
+        ("row_visits", ctypes.c_uint64),
+        ("row_stores", ctypes.c_uint64),
+        ("cells_loaded", ctypes.c_uint64),
+        ("cells_stored", ctypes.c_uint64),
+        ("row_loads", ctypes.c_uint64),
+    ]
+
+
+class GoCosts(ctypes.Structure):
+    _fields_ = [
+        ("orthogonal_step", ctypes.c_uint32),
+        ("diagonal_step", ctypes.c_uint32),
+        ("bend", ctypes.c_uint32),
+    ]
+
+
+class GoQuery(ctypes.Structure):
+    _fields_ = [
+        ("start_node", ctypes.c_uint32),
+        ("goal_node", ctypes.c_uint32),
+        ("orthogonal_step_surcharge", ctypes.c_uint64),
+        ("diagonal_step_surcharge", ctypes.c_uint64),
+        ("bend_surcharge", ctypes.c_uint64),
+        ("policy", ctypes.c_void_p),
+        ("policy_count", ctypes.c_uint32),
+    ]
+
+
+def lo_inf() -> int:
+    return 0xFFFFFFFF
+
+
+def build() -> str:
+    """Compile the oracle with make (gcc); returns the library path."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(_LIB_PATH)
+        _lib.lo_dijkstra.restype = ctypes.c_uint32
+        _lib.lo_astar.restype = ctypes.c_uint32
+        _lib.lo_sweep_schedule.restype = ctypes.c_uint32
+        _lib.go_search.restype = ctypes.c_int
+        _lib.po_epoch_update.restype = ctypes.c_int
+        _lib.po_snapshot_costs.restype = ctypes.c_int
+        _lib.po_history_update.restype = ctypes.c_int
+    return _lib
+
+
+def _ptr(a, t=U32P):
+    return a.ctypes.data_as(t)
+
+
+class LatticeRef:
+    """Keeps the numpy buffers alive while the C struct points at them."""
+
+    def __init__(self, lat):
+        self.blocked = np.ascontiguousarray(lat.blocked, dtype=np.uint32)
+        self.via_ok = None if lat.via_ok is None else np.ascontiguousarray(lat.via_ok, np.uint32)
+        self.c = LoLattice(
+            lat.layers, lat.height, lat.width, _ptr(self.blocked),
+            _ptr(self.via_ok) if self.via_ok is not None else U32P(),
+            lat.orth, lat.diag, lat.via)
+
+
+def _net_ptr(nets):
+    return nets.ctypes.data_as(ctypes.c_void_p)
+
+
+def dijkstra(lat, net_row, full=False, want_dist=False, path_cap=1 << 22):
+    """Returns (cost, reverse canonical path as uint32 array, dist or None)."""
+    L = lib()
+    ref = LatticeRef(lat)
+    net = np.array([net_row], dtype=net_row.dtype) if not isinstance(net_row, np.ndarray) else net_row
+    net = np.ascontiguousarray(net.reshape(1))
+    cells = lat.layers * int(net["win_w"][0]) * int(net["win_h"][0])
+    dist = np.empty(cells, dtype=np.uint32) if want_dist else None
+    path = np.empty(path_cap, dtype=np.uint32)
+    plen = ctypes.c_uint32(0)
+    cost = L.lo_dijkstra(ctypes.byref(ref.c), _net_ptr(net), int(full),
+                         _ptr(dist) if dist is not None else U32P(), _ptr(path),
+                         ctypes.c_uint32(path_cap), ctypes.byref(plen))
+    n = plen.value
+    return cost, (path[:n].copy() if n != 0xFFFFFFFF else None), dist
+
+
+def dijkstra_batch(lat, nets, threads=None, path_cap_per_net=None):
+    L = lib()
+    ref = LatticeRef(lat)
+    nets = np.ascontiguousarray(nets)
+    count = len(nets)
+    threads = threads or os.cpu_count() or 1
+    # canonical paths are bounded by window cells; use the Chebyshev-bounded
+    # estimate w*h*layers capped to keep memory small for tests
+    caps = (nets["win_w"].astype(np.uint64) * nets["win_h"].astype(np.uint64) * lat.layers)
+    if path_cap_per_net is not None:
+        caps = np.minimum(caps, np.uint64(path_cap_per_net))
+    offsets = np.zeros(count, dtype=np.uint64)
+    offsets[1:] = np.cumsum(caps)[:-1]
+    total = int(caps.sum())
+    paths = np.empty(total, dtype=np.uint32)
+    costs = np.empty(count, dtype=np.uint32)
+    lens = np.empty(count, dtype=np.uint32)
+    L.lo_dijkstra_batch(ctypes.byref(ref.c), _net_ptr(nets), ctypes.c_uint32(count),
+                        ctypes.c_int(threads), _ptr(costs), _ptr(lens), _ptr(offsets, U64P),
+                        _ptr(paths), ctypes.c_uint64(total))
+    out = []
+    for i in range(count):
+        n = int(lens[i])
+        if n == 0xFFFFFFFF:
+            out.append(None)
+        else:
+            o = int(offsets[i])
+            out.append(paths[o:o + n].copy())
+    return costs, out
+
+
+def astar_batch(lat, nets, threads=None):
+    L = lib()
+    ref = LatticeRef(lat)
+    nets = np.ascontiguousarray(nets)
+    costs = np.empty(len(nets), dtype=np.uint32)
+    L.lo_astar_batch(ctypes.byref(ref.c), _net_ptr(nets), ctypes.c_uint32(len(nets)),
+                     ctypes.c_int(threads or os.cpu_count() or 1), _ptr(costs))
+    return costs
+
+
+def sweep_batch(lat, nets, threads=None, max_sweeps=100000):
+    L = lib()
+    ref = LatticeRef(lat)
+    nets = np.ascontiguousarray(nets)
+    costs = np.empty(len(nets), dtype=np.uint32)
+    stats = (LoSweepStats * len(nets))()
+    L.lo_sweep_batch(ctypes.byref(ref.c), _net_ptr(nets), ctypes.c_uint32(len(nets)),
+                     ctypes.c_int(threads or os.cpu_count() or 1), ctypes.c_uint32(max_sweeps),
+                     _ptr(costs), stats)
+    rows = [(s.sweeps, s.row_visits, s.row_stores, s.cells_loaded, s.cells_stored, s.row_loads)
+            for s in stats]
+    return costs, np.array(rows, dtype=np.uint64).reshape(len(nets), 6)
+
+
+def sweep_one(lat, net_row, max_sweeps=100000):
+    L = lib()
+    ref = LatticeRef(lat)
+    net = np.ascontiguousarray(np.asarray(net_row).reshape(1))
+    cells = lat.layers * int(net["win_w"][0]) * int(net["win_h"][0])
+    dist = np.empty(cells, dtype=np.uint32)
+    st = LoSweepStats()
+    cost = L.lo_sweep_schedule(ctypes.byref(ref.c), _net_ptr(net), ctypes.c_uint32(max_sweeps),
+                               _ptr(dist), ctypes.byref(st))
+    return cost, dist, st

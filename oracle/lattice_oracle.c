@@ -1,0 +1,637 @@
+/*
+ * Lattice-mode CPU oracle.  TEST INFRASTRUCTURE ONLY (see oracle.h).
+ *
+ * Move model shared with the GPU kernels (apgar_b200/csrc/lattice_sweep.cu):
+ *   orthogonal move legal iff both cells are free;
+ *   diagonal move legal iff both cells and both side cells are free;
+ *   via (l, x, y) <-> (l+1, x, y) legal iff both cells are free and the via
+ *   bit of layer pair l is set (no via mask = every via bit set);
+ *   a cell is free iff it lies inside the net window and is not blocked.
+ * Costs: orthogonal, diagonal, via (no bend term: the lattice configs use
+ * bend 0, which is what makes node-level labels sufficient).
+ *
+ * Canonical path (reference planar_router.cu:1084-1165 reverse walk, applied
+ * to exact labels): from the goal, repeatedly step to the predecessor through
+ * the smallest incoming heading h whose move is legal and satisfies
+ * label[pred] + cost(h) == label[cur].  Headings 0..7 are the planar
+ * directions E, NE, N, NW, W, SW, S, SE (geometry_compiler::Direction order);
+ * 8 = via arriving from the layer below, 9 = via arriving from the layer above.
+ */
+#include "oracle.h"
+
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+
+static const int kDx[8] = {1, 1, 0, -1, -1, -1, 0, 1};
+static const int kDy[8] = {0, 1, 1, 1, 0, -1, -1, -1};
+
+typedef struct win_ctx {
+  const lo_lattice* lat;
+  const lo_net* net;
+  int L, w, h, x0, y0, words;
+} win_ctx;
+
+static inline int lat_blocked(const lo_lattice* lat, int l, int gx, int gy) {
+  const uint32_t word = lat->blocked[((size_t)l * lat->height + gy) * (lat->width / 32) + gx / 32];
+  return (word >> (gx & 31)) & 1u;
+}
+
+static inline int cell_free(const win_ctx* c, int l, int x, int y) {
+  if (x < 0 || y < 0 || x >= c->w || y >= c->h || l < 0 || l >= c->L) return 0;
+  return !lat_blocked(c->lat, l, c->x0 + x, c->y0 + y);
+}
+
+static inline int via_bit(const win_ctx* c, int lower, int x, int y) {
+  if (c->lat->via_ok == NULL) return 1;
+  const int gx = c->x0 + x, gy = c->y0 + y;
+  const uint32_t word =
+      c->lat->via_ok[((size_t)lower * c->lat->height + gy) * (c->lat->width / 32) + gx / 32];
+  return (word >> (gx & 31)) & 1u;
+}
+
+/* Planar move from (x,y) in direction d on layer l. */
+static inline int planar_legal(const win_ctx* c, int l, int x, int y, int d) {
+  const int nx = x + kDx[d], ny = y + kDy[d];
+  if (!cell_free(c, l, x, y) || !cell_free(c, l, nx, ny)) return 0;
+  if ((d & 1) == 0) return 1;
+  return cell_free(c, l, nx, y) && cell_free(c, l, x, ny);
+}
+
+static inline int via_legal(const win_ctx* c, int lower, int x, int y) {
+  return cell_free(c, lower, x, y) && cell_free(c, lower + 1, x, y) && via_bit(c, lower, x, y);
+}
+
+static void ctx_init(win_ctx* c, const lo_lattice* lat, const lo_net* net) {
+  c->lat = lat;
+  c->net = net;
+  c->L = lat->layers;
+  c->w = (int)net->win_w;
+  c->h = (int)net->win_h;
+  c->x0 = (int)net->win_x0;
+  c->y0 = (int)net->win_y0;
+  c->words = lat->width / 32;
+}
+
+static inline size_t cell_index(const win_ctx* c, int l, int x, int y) {
+  return ((size_t)l * c->h + y) * c->w + x;
+}
+
+/* ---------------------------- binary heap ---------------------------- */
+
+typedef struct heap_item {
+  uint64_t key; /* label << 32 | tiebreak */
+  uint32_t cell;
+} heap_item;
+
+typedef struct heap {
+  heap_item* items;
+  size_t size, cap;
+} heap;
+
+static void heap_push(heap* hp, uint64_t key, uint32_t cell) {
+  if (hp->size == hp->cap) {
+    hp->cap = hp->cap ? hp->cap * 2 : 1024;
+    hp->items = (heap_item*)realloc(hp->items, hp->cap * sizeof(heap_item));
+  }
+  size_t i = hp->size++;
+  while (i > 0) {
+    size_t p = (i - 1) / 2;
+    if (hp->items[p].key <= key) break;
+    hp->items[i] = hp->items[p];
+    i = p;
+  }
+  hp->items[i].key = key;
+  hp->items[i].cell = cell;
+}
+
+static heap_item heap_pop(heap* hp) {
+  heap_item top = hp->items[0];
+  heap_item last = hp->items[--hp->size];
+  size_t i = 0;
+  for (;;) {
+    size_t l = 2 * i + 1;
+    if (l >= hp->size) break;
+    size_t r = l + 1;
+    size_t m = (r < hp->size && hp->items[r].key < hp->items[l].key) ? r : l;
+    if (hp->items[m].key >= last.key) break;
+    hp->items[i] = hp->items[m];
+    i = m;
+  }
+  if (hp->size > 0) hp->items[i] = last;
+  return top;
+}
+
+/* --------------------------- canonical walk --------------------------- */
+
+static inline uint32_t move_cost(const lo_lattice* lat, int h) {
+  if (h >= 8) return lat->via;
+  return (h & 1) ? lat->diag : lat->orth;
+}
+
+/* Reverse canonical path from exact labels.  Returns path length, or
+ * UINT32_MAX when the capacity is exceeded or the labels are inconsistent. */
+static uint32_t canonical_walk(const win_ctx* c, const uint32_t* dist, int gl, int gx, int gy,
+                               int sl, int sx, int sy, uint32_t* path, uint32_t cap) {
+  const lo_lattice* lat = c->lat;
+  int l = gl, x = gx, y = gy;
+  uint32_t n = 0;
+  for (;;) {
+    if (n >= cap) return UINT32_MAX;
+    path[n++] = (uint32_t)((((size_t)l * lat->height) + (c->y0 + y)) * lat->width + (c->x0 + x));
+    if (l == sl && x == sx && y == sy) return n;
+    const uint32_t here = dist[cell_index(c, l, x, y)];
+    int chosen = -1;
+    for (int h = 0; h < 10 && chosen < 0; ++h) {
+      int pl = l, px = x, py = y;
+      int legal;
+      if (h < 8) {
+        px = x - kDx[h];
+        py = y - kDy[h];
+        legal = planar_legal(c, l, px, py, h);
+      } else if (h == 8) {
+        pl = l - 1;
+        legal = pl >= 0 && via_legal(c, pl, x, y);
+      } else {
+        pl = l + 1;
+        legal = pl < c->L && via_legal(c, l, x, y);
+      }
+      if (!legal) continue;
+      const uint32_t pd = dist[cell_index(c, pl, px, py)];
+      if (pd == LO_INF) continue;
+      if ((uint64_t)pd + move_cost(lat, h) == here) {
+        chosen = h;
+        l = pl;
+        x = px;
+        y = py;
+      }
+    }
+    if (chosen < 0) return UINT32_MAX;
+  }
+}
+
+/* ------------------------------ Dijkstra ------------------------------ */
+
+uint32_t lo_dijkstra(const lo_lattice* lat, const lo_net* net, int full, uint32_t* dist_out,
+                     uint32_t* path, uint32_t path_cap, uint32_t* path_len) {
+  win_ctx c;
+  ctx_init(&c, lat, net);
+  const size_t cells = (size_t)c.L * c.w * c.h;
+  uint32_t* dist = dist_out ? dist_out : (uint32_t*)malloc(cells * sizeof(uint32_t));
+  for (size_t i = 0; i < cells; ++i) dist[i] = LO_INF;
+  const int sl = (int)net->start_layer, sx = (int)(net->start_x - net->win_x0),
+            sy = (int)(net->start_y - net->win_y0);
+  const int gl = (int)net->goal_layer, gx = (int)(net->goal_x - net->win_x0),
+            gy = (int)(net->goal_y - net->win_y0);
+  if (path_len) *path_len = 0;
+  if (!cell_free(&c, sl, sx, sy) || !cell_free(&c, gl, gx, gy)) {
+    if (!dist_out) free(dist);
+    return LO_INF;
+  }
+  heap hp = {0};
+  dist[cell_index(&c, sl, sx, sy)] = 0;
+  heap_push(&hp, 0, (uint32_t)cell_index(&c, sl, sx, sy));
+  const size_t goal_index = cell_index(&c, gl, gx, gy);
+  while (hp.size) {
+    heap_item it = heap_pop(&hp);
+    const uint32_t d = (uint32_t)(it.key >> 32);
+    if (d != dist[it.cell]) continue;
+    if (!full && dist[goal_index] != LO_INF && d > dist[goal_index]) break;
+    const int l = (int)(it.cell / ((size_t)c.w * c.h));
+    const int rem = (int)(it.cell % ((size_t)c.w * c.h));
+    const int y = rem / c.w, x = rem % c.w;
+    for (int h = 0; h < 10; ++h) {
+      int nl = l, nx = x, ny = y, legal;
+      if (h < 8) {
+        nx = x + kDx[h];
+        ny = y + kDy[h];
+        legal = planar_legal(&c, l, x, y, h);
+      } else if (h == 8) {
+        nl = l + 1;
+        legal = nl < c.L && via_legal(&c, l, x, y);
+      } else {
+        nl = l - 1;
+        legal = nl >= 0 && via_legal(&c, nl, x, y);
+      }
+      if (!legal) continue;
+      const uint64_t cand = (uint64_t)d + move_cost(lat, h);
+      const size_t ni = cell_index(&c, nl, nx, ny);
+      if (cand < dist[ni]) {
+        dist[ni] = (uint32_t)cand;
+        heap_push(&hp, (cand << 32) | (uint32_t)ni, (uint32_t)ni);
+      }
+    }
+  }
+  free(hp.items);
+  const uint32_t cost = dist[goal_index];
+  if (cost != LO_INF && path && path_len) {
+    *path_len = canonical_walk(&c, dist, gl, gx, gy, sl, sx, sy, path, path_cap);
+  }
+  if (!dist_out) free(dist);
+  return cost;
+}
+
+/* -------------------------------- A* -------------------------------- */
+
+/* Pop key of RouteWithCpuAStar (cpu_astar.cc:67-74): (f, h, g, y, x, heading,
+ * sequence), extended with the layer between g and y.  The heuristic is the
+ * reference octile bound for diag >= orth (cpu_astar.cc:176-190) plus one via
+ * cost per layer of separation, which keeps it admissible and consistent. */
+typedef struct astar_item {
+  uint64_t f, h, g;
+  int32_t l, y, x, heading;
+  uint64_t seq;
+} astar_item;
+
+static int astar_less(const astar_item* a, const astar_item* b) {
+  if (a->f != b->f) return a->f < b->f;
+  if (a->h != b->h) return a->h < b->h;
+  if (a->g != b->g) return a->g < b->g;
+  if (a->l != b->l) return a->l < b->l;
+  if (a->y != b->y) return a->y < b->y;
+  if (a->x != b->x) return a->x < b->x;
+  if (a->heading != b->heading) return a->heading < b->heading;
+  return a->seq < b->seq;
+}
+
+typedef struct aheap {
+  astar_item* items;
+  size_t size, cap;
+} aheap;
+
+static void aheap_push(aheap* hp, astar_item it) {
+  if (hp->size == hp->cap) {
+    hp->cap = hp->cap ? hp->cap * 2 : 1024;
+    hp->items = (astar_item*)realloc(hp->items, hp->cap * sizeof(astar_item));
+  }
+  size_t i = hp->size++;
+  while (i > 0) {
+    size_t p = (i - 1) / 2;
+    if (!astar_less(&it, &hp->items[p])) break;
+    hp->items[i] = hp->items[p];
+    i = p;
+  }
+  hp->items[i] = it;
+}
+
+static astar_item aheap_pop(aheap* hp) {
+  astar_item top = hp->items[0];
+  astar_item last = hp->items[--hp->size];
+  size_t i = 0;
+  for (;;) {
+    size_t l = 2 * i + 1;
+    if (l >= hp->size) break;
+    size_t r = l + 1;
+    size_t m = (r < hp->size && astar_less(&hp->items[r], &hp->items[l])) ? r : l;
+    if (!astar_less(&hp->items[m], &last)) break;
+    hp->items[i] = hp->items[m];
+    i = m;
+  }
+  if (hp->size > 0) hp->items[i] = last;
+  return top;
+}
+
+static uint64_t octile(const lo_lattice* lat, int dx, int dy, int dl) {
+  const uint64_t ax = (uint64_t)(dx < 0 ? -dx : dx), ay = (uint64_t)(dy < 0 ? -dy : dy);
+  const uint64_t al = (uint64_t)(dl < 0 ? -dl : dl);
+  uint64_t planar;
+  if (lat->diag < lat->orth) {
+    planar = (ax > ay ? ax : ay) * lat->diag;
+  } else {
+    const uint64_t dmin = ax < ay ? ax : ay, dmax = ax < ay ? ay : ax;
+    const uint64_t eff = lat->diag < 2ull * lat->orth ? lat->diag : 2ull * lat->orth;
+    planar = dmin * eff + (dmax - dmin) * lat->orth;
+  }
+  return planar + al * lat->via;
+}
+
+uint32_t lo_astar(const lo_lattice* lat, const lo_net* net, uint64_t* expanded_out) {
+  win_ctx c;
+  ctx_init(&c, lat, net);
+  const size_t cells = (size_t)c.L * c.w * c.h;
+  /* Record per (cell, heading): heading 0..7 planar, 8 start / none, 9 via up,
+   * 10 via down.  Only the cost is needed here. */
+  const size_t states = cells * 11;
+  uint32_t* g = (uint32_t*)malloc(states * sizeof(uint32_t));
+  for (size_t i = 0; i < states; ++i) g[i] = LO_INF;
+  const int sl = (int)net->start_layer, sx = (int)(net->start_x - net->win_x0),
+            sy = (int)(net->start_y - net->win_y0);
+  const int gl = (int)net->goal_layer, gx = (int)(net->goal_x - net->win_x0),
+            gy = (int)(net->goal_y - net->win_y0);
+  uint64_t expanded = 0;
+  uint32_t result = LO_INF;
+  if (cell_free(&c, sl, sx, sy) && cell_free(&c, gl, gx, gy)) {
+    aheap hp = {0};
+    uint64_t seq = 0;
+    const uint64_t h0 = octile(lat, gx - sx, gy - sy, gl - sl);
+    g[cell_index(&c, sl, sx, sy) * 11 + 8] = 0;
+    astar_item s = {h0, h0, 0, sl, sy, sx, 8, seq++};
+    aheap_push(&hp, s);
+    while (hp.size) {
+      astar_item cur = aheap_pop(&hp);
+      const size_t ci = cell_index(&c, cur.l, cur.x, cur.y);
+      if (g[ci * 11 + (size_t)cur.heading] != cur.g) continue;
+      if (cur.l == gl && cur.x == gx && cur.y == gy) {
+        result = (uint32_t)cur.g;
+        break;
+      }
+      ++expanded;
+      for (int mv = 0; mv < 10; ++mv) {
+        int nl = cur.l, nx = cur.x, ny = cur.y, legal, heading;
+        if (mv < 8) {
+          nx = cur.x + kDx[mv];
+          ny = cur.y + kDy[mv];
+          legal = planar_legal(&c, cur.l, cur.x, cur.y, mv);
+          heading = mv;
+        } else if (mv == 8) {
+          nl = cur.l + 1;
+          legal = nl < c.L && via_legal(&c, cur.l, cur.x, cur.y);
+          heading = 9;
+        } else {
+          nl = cur.l - 1;
+          legal = nl >= 0 && via_legal(&c, nl, cur.x, cur.y);
+          heading = 10;
+        }
+        if (!legal) continue;
+        const uint64_t ng = cur.g + move_cost(lat, mv);
+        const size_t ni = cell_index(&c, nl, nx, ny) * 11 + (size_t)heading;
+        if (g[ni] != LO_INF && g[ni] <= ng) continue;
+        g[ni] = (uint32_t)ng;
+        const uint64_t hh = octile(lat, gx - nx, gy - ny, gl - nl);
+        astar_item it = {ng + hh, hh, ng, nl, ny, nx, heading, seq++};
+        aheap_push(&hp, it);
+      }
+    }
+    free(hp.items);
+  }
+  free(g);
+  if (expanded_out) *expanded_out = expanded;
+  return result;
+}
+
+/* --------------------------- sweep schedule --------------------------- */
+
+/* Row step semantics (one window row, all layers together), identical to the
+ * GPU kernel: relax from the previous row in sweep order (orthogonal plus the
+ * two diagonals), then repeat {east scan, west scan, via cascade up then down}
+ * until the via cascade changes nothing.  A row is skipped when neither it nor
+ * its predecessor row changed since the last sweep in the same direction (or,
+ * for the first sweep in each direction, when both rows are still all-INF). */
+uint32_t lo_sweep_schedule(const lo_lattice* lat, const lo_net* net, uint32_t max_sweeps,
+                           uint32_t* dist, lo_sweep_stats* stats) {
+  win_ctx c;
+  ctx_init(&c, lat, net);
+  const int L = c.L, w = c.w, h = c.h;
+  const size_t cells = (size_t)L * w * h;
+  for (size_t i = 0; i < cells; ++i) dist[i] = LO_INF;
+  lo_sweep_stats st = {0};
+  const int sl = (int)net->start_layer, sx = (int)(net->start_x - net->win_x0),
+            sy = (int)(net->start_y - net->win_y0);
+  const int gl = (int)net->goal_layer, gx = (int)(net->goal_x - net->win_x0),
+            gy = (int)(net->goal_y - net->win_y0);
+  if (!cell_free(&c, sl, sx, sy) || !cell_free(&c, gl, gx, gy)) {
+    if (stats) *stats = st;
+    return LO_INF;
+  }
+  const int32_t kNever = -1000000;
+  int32_t* modified = (int32_t*)malloc((size_t)h * sizeof(int32_t));
+  for (int y = 0; y < h; ++y) modified[y] = kNever;
+  dist[cell_index(&c, sl, sx, sy)] = 0;
+  modified[sy] = 0; /* initialisation writes the start row on every layer */
+  st.row_stores += (uint64_t)L;
+  st.cells_stored += (uint64_t)L * w;
+  uint32_t* row = (uint32_t*)malloc((size_t)L * w * sizeof(uint32_t));
+  uint32_t* orig = (uint32_t*)malloc((size_t)L * w * sizeof(uint32_t));
+  uint32_t sweeps = 0;
+  for (uint32_t k = 1; k <= max_sweeps; ++k) {
+    sweeps = k;
+    const int up = (k & 1) != 0;
+    const int dy = up ? 1 : -1;
+    int any_change = 0;
+    int prev_in_regs = 0;
+    for (int step = 0; step < h; ++step) {
+      const int y = up ? step : h - 1 - step;
+      const int p = y - dy; /* previous row in sweep order */
+      const int32_t mp = (p >= 0 && p < h) ? modified[p] : kNever;
+      const int32_t my = modified[y];
+      int skip;
+      if (k <= 2) {
+        skip = (mp == kNever && my == kNever);
+      } else {
+        skip = (mp <= (int32_t)k - 2 && my <= (int32_t)k - 2);
+      }
+      if (skip) {
+        prev_in_regs = 0;
+        continue;
+      }
+      if (mp != kNever && !prev_in_regs) {
+        st.cells_loaded += (uint64_t)L * w; /* predecessor row reload */
+        st.row_loads += (uint64_t)L;
+      }
+      if (my != kNever) {
+        st.cells_loaded += (uint64_t)L * w;
+        st.row_loads += (uint64_t)L;
+      }
+      st.row_visits += 1;
+      for (int l = 0; l < L; ++l) {
+        for (int x = 0; x < w; ++x) {
+          row[l * w + x] = dist[cell_index(&c, l, x, y)];
+        }
+      }
+      memcpy(orig, row, (size_t)L * w * sizeof(uint32_t));
+      if (p >= 0 && p < h && mp != kNever) {
+        /* moves from row p into row y: straight (dy), and diagonals from x-1 and x+1 */
+        const int d_straight = up ? 2 : 6;        /* N or S */
+        const int d_from_left = up ? 1 : 7;       /* NE or SE: from (x-1, p) */
+        const int d_from_right = up ? 3 : 5;      /* NW or SW: from (x+1, p) */
+        for (int l = 0; l < L; ++l) {
+          for (int x = 0; x < w; ++x) {
+            uint64_t best = row[l * w + x];
+            uint32_t pd = dist[cell_index(&c, l, x, p)];
+            if (pd != LO_INF && planar_legal(&c, l, x, p, d_straight)) {
+              if ((uint64_t)pd + lat->orth < best) best = (uint64_t)pd + lat->orth;
+            }
+            if (x > 0) {
+              pd = dist[cell_index(&c, l, x - 1, p)];
+              if (pd != LO_INF && planar_legal(&c, l, x - 1, p, d_from_left)) {
+                if ((uint64_t)pd + lat->diag < best) best = (uint64_t)pd + lat->diag;
+              }
+            }
+            if (x + 1 < w) {
+              pd = dist[cell_index(&c, l, x + 1, p)];
+              if (pd != LO_INF && planar_legal(&c, l, x + 1, p, d_from_right)) {
+                if ((uint64_t)pd + lat->diag < best) best = (uint64_t)pd + lat->diag;
+              }
+            }
+            row[l * w + x] = (uint32_t)best;
+          }
+        }
+      }
+      for (;;) {
+        for (int l = 0; l < L; ++l) {
+          for (int x = 1; x < w; ++x) { /* east scan */
+            const uint32_t a = row[l * w + x - 1];
+            if (a != LO_INF && planar_legal(&c, l, x - 1, y, 0) &&
+                (uint64_t)a + lat->orth < row[l * w + x]) {
+              row[l * w + x] = a + lat->orth;
+            }
+          }
+          for (int x = w - 2; x >= 0; --x) { /* west scan */
+            const uint32_t a = row[l * w + x + 1];
+            if (a != LO_INF && planar_legal(&c, l, x + 1, y, 4) &&
+                (uint64_t)a + lat->orth < row[l * w + x]) {
+              row[l * w + x] = a + lat->orth;
+            }
+          }
+        }
+        int via_change = 0;
+        for (int l = 1; l < L; ++l) {
+          for (int x = 0; x < w; ++x) {
+            const uint32_t a = row[(l - 1) * w + x];
+            if (a != LO_INF && via_legal(&c, l - 1, x, y) &&
+                (uint64_t)a + lat->via < row[l * w + x]) {
+              row[l * w + x] = a + lat->via;
+              via_change = 1;
+            }
+          }
+        }
+        for (int l = L - 2; l >= 0; --l) {
+          for (int x = 0; x < w; ++x) {
+            const uint32_t a = row[(l + 1) * w + x];
+            if (a != LO_INF && via_legal(&c, l, x, y) &&
+                (uint64_t)a + lat->via < row[l * w + x]) {
+              row[l * w + x] = a + lat->via;
+              via_change = 1;
+            }
+          }
+        }
+        if (!via_change) break;
+      }
+      int changed = memcmp(orig, row, (size_t)L * w * sizeof(uint32_t)) != 0;
+      if (changed) {
+        /* a newly materialised row stores every layer; afterwards only the
+         * layers whose labels changed are written back */
+        const int materialise = (my == kNever);
+        for (int l = 0; l < L; ++l) {
+          const int layer_changed =
+              memcmp(orig + (size_t)l * w, row + (size_t)l * w, (size_t)w * sizeof(uint32_t)) != 0;
+          if (!layer_changed && !materialise) continue;
+          for (int x = 0; x < w; ++x) dist[cell_index(&c, l, x, y)] = row[l * w + x];
+          st.row_stores += 1;
+          st.cells_stored += (uint64_t)w;
+        }
+        modified[y] = (int32_t)k;
+        any_change = 1;
+      }
+      prev_in_regs = 1;
+    }
+    if (!any_change && k >= 2) break;
+  }
+  st.sweeps = sweeps;
+  free(row);
+  free(orig);
+  free(modified);
+  if (stats) *stats = st;
+  return dist[cell_index(&c, gl, gx, gy)];
+}
+
+/* ----------------------------- batches ----------------------------- */
+
+typedef struct batch_job {
+  const lo_lattice* lat;
+  const lo_net* nets;
+  uint32_t count;
+  int kind; /* 0 dijkstra, 1 astar, 2 sweep */
+  uint32_t max_sweeps;
+  uint32_t* costs;
+  uint32_t* path_lens;
+  const uint64_t* path_offsets;
+  uint32_t* paths;
+  uint64_t path_capacity;
+  lo_sweep_stats* stats;
+  uint32_t next;
+  pthread_mutex_t lock;
+} batch_job;
+
+static void* batch_worker(void* arg) {
+  batch_job* job = (batch_job*)arg;
+  for (;;) {
+    pthread_mutex_lock(&job->lock);
+    const uint32_t i = job->next++;
+    pthread_mutex_unlock(&job->lock);
+    if (i >= job->count) break;
+    const lo_net* net = &job->nets[i];
+    if (job->kind == 0) {
+      uint32_t len = 0;
+      uint32_t* path = NULL;
+      uint32_t cap = 0;
+      if (job->paths) {
+        path = job->paths + job->path_offsets[i];
+        const uint64_t end = (i + 1 < job->count) ? job->path_offsets[i + 1] : job->path_capacity;
+        cap = (uint32_t)(end - job->path_offsets[i]);
+      }
+      job->costs[i] = lo_dijkstra(job->lat, net, 0, NULL, path, cap, path ? &len : NULL);
+      if (job->path_lens) job->path_lens[i] = len;
+    } else if (job->kind == 1) {
+      job->costs[i] = lo_astar(job->lat, net, NULL);
+    } else {
+      const size_t cells = (size_t)job->lat->layers * net->win_w * net->win_h;
+      uint32_t* dist = (uint32_t*)malloc(cells * sizeof(uint32_t));
+      job->costs[i] =
+          lo_sweep_schedule(job->lat, net, job->max_sweeps, dist, job->stats ? &job->stats[i] : NULL);
+      free(dist);
+    }
+  }
+  return NULL;
+}
+
+static void run_batch(batch_job* job, int threads) {
+  if (threads < 1) threads = 1;
+  if (threads > 256) threads = 256;
+  pthread_mutex_init(&job->lock, NULL);
+  job->next = 0;
+  pthread_t tids[256];
+  for (int t = 0; t < threads; ++t) pthread_create(&tids[t], NULL, batch_worker, job);
+  for (int t = 0; t < threads; ++t) pthread_join(tids[t], NULL);
+  pthread_mutex_destroy(&job->lock);
+}
+
+void lo_dijkstra_batch(const lo_lattice* lat, const lo_net* nets, uint32_t count, int threads,
+                       uint32_t* costs, uint32_t* path_lens, uint64_t* path_offsets,
+                       uint32_t* paths, uint64_t path_capacity) {
+  batch_job job = {0};
+  job.lat = lat;
+  job.nets = nets;
+  job.count = count;
+  job.kind = 0;
+  job.costs = costs;
+  job.path_lens = path_lens;
+  job.path_offsets = path_offsets;
+  job.paths = paths;
+  job.path_capacity = path_capacity;
+  run_batch(&job, threads);
+}
+
+void lo_astar_batch(const lo_lattice* lat, const lo_net* nets, uint32_t count, int threads,
+                    uint32_t* costs) {
+  batch_job job = {0};
+  job.lat = lat;
+  job.nets = nets;
+  job.count = count;
+  job.kind = 1;
+  job.costs = costs;
+  run_batch(&job, threads);
+}
+
+void lo_sweep_batch(const lo_lattice* lat, const lo_net* nets, uint32_t count, int threads,
+                    uint32_t max_sweeps, uint32_t* costs, lo_sweep_stats* stats) {
+  batch_job job = {0};
+  job.lat = lat;
+  job.nets = nets;
+  job.count = count;
+  job.kind = 2;
+  job.max_sweeps = max_sweeps;
+  job.costs = costs;
+  job.stats = stats;
+  run_batch(&job, threads);
+}

@@ -1,0 +1,115 @@
+"""CPU checks of the lattice-mode oracle: three independent restatements
+(Dijkstra, reference-key A*, row-sweep schedule) agree, and the canonical
+path obeys the tie-break rule and the move model."""
+
+import numpy as np
+import pytest
+
+import oracle
+from apgar_b200 import synth
+
+DX = [1, 1, 0, -1, -1, -1, 0, 1]
+DY = [0, 1, 1, 1, 0, -1, -1, -1]
+
+
+def _free(dense, net, l, x, y):
+    if not (0 <= l < dense.shape[0]):
+        return False
+    if not (net["win_x0"] <= x < net["win_x0"] + net["win_w"]):
+        return False
+    if not (net["win_y0"] <= y < net["win_y0"] + net["win_h"]):
+        return False
+    return not dense[l, y, x]
+
+
+def _check_path(lat, net, cost, path):
+    """Reverse path legality + exact cost (move model of oracle.h)."""
+    dense = lat.blocked_dense()
+    H, W = lat.height, lat.width
+    cells = [(int(c) // (H * W), (int(c) % (H * W)) // W, int(c) % W) for c in path]
+    assert cells[0] == (net["goal_layer"], net["goal_y"], net["goal_x"])
+    assert cells[-1] == (net["start_layer"], net["start_y"], net["start_x"])
+    total = 0
+    for (l1, y1, x1), (l0, y0, x0) in zip(cells[:-1], cells[1:]):
+        assert _free(dense, net, l0, x0, y0) and _free(dense, net, l1, x1, y1)
+        if l1 != l0:
+            assert (x1, y1) == (x0, y0) and abs(l1 - l0) == 1
+            total += lat.via
+        else:
+            dx, dy = x1 - x0, y1 - y0
+            assert max(abs(dx), abs(dy)) == 1
+            if dx and dy:
+                assert _free(dense, net, l0, x1, y0) and _free(dense, net, l0, x0, y1)
+                total += lat.diag
+            else:
+                total += lat.orth
+    assert total == cost
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_small_config_restatements_agree(seed):
+    lat, nets = synth.config_small(seed)
+    cd, paths = oracle.dijkstra_batch(lat, nets)
+    ca = oracle.astar_batch(lat, nets)
+    cs, _ = oracle.sweep_batch(lat, nets)
+    assert np.array_equal(cd, ca)
+    assert np.array_equal(cd, cs)
+    for i in range(len(nets)):
+        if cd[i] != oracle.lo_inf():
+            _check_path(lat, nets[i], int(cd[i]), paths[i])
+
+
+def test_medium_like_restatements_agree():
+    lat, nets = synth.config_medium(5, nets=48, size=512)
+    cd, paths = oracle.dijkstra_batch(lat, nets)
+    ca = oracle.astar_batch(lat, nets)
+    cs, st = oracle.sweep_batch(lat, nets)
+    assert np.array_equal(cd, ca) and np.array_equal(cd, cs)
+    assert (st[:, 0] >= 2).all()
+    for i in range(len(nets)):
+        if cd[i] != oracle.lo_inf():
+            _check_path(lat, nets[i], int(cd[i]), paths[i])
+
+
+def test_via_mask_and_single_layer():
+    lat = synth.make_lattice(7, 3, 96, 0.22, via_mask=True)
+    nets = synth.make_nets(lat, 70, 24, hpwl_median=40.0, hpwl_sigma=0.6, margin=8)
+    cd, _ = oracle.dijkstra_batch(lat, nets)
+    assert np.array_equal(cd, oracle.astar_batch(lat, nets))
+    assert np.array_equal(cd, oracle.sweep_batch(lat, nets)[0])
+    lat1 = synth.make_lattice(8, 1, 64, 0.3)
+    nets1 = synth.make_nets(lat1, 80, 20, hpwl_median=None, margin=None)
+    cd1, _ = oracle.dijkstra_batch(lat1, nets1)
+    assert np.array_equal(cd1, oracle.astar_batch(lat1, nets1))
+    assert np.array_equal(cd1, oracle.sweep_batch(lat1, nets1)[0])
+
+
+def test_known_answers_open_field():
+    # Open 1-layer field: octile distance, canonical path prefers east/north-east first.
+    lat = synth.Lattice(1, 32, 32, np.zeros((1, 32, 1), np.uint32), None)
+    net = np.array([(0, 2, 3, 0, 9, 5, 0, 0, 32, 32)], dtype=synth.NET_DTYPE)
+    cost, path, _ = oracle.dijkstra(lat, net[0])
+    assert cost == 2 * 14 + 5 * 10  # dx=7, dy=2
+    _check_path(lat, net[0], cost, path)
+    # blocked start -> disconnected
+    dense = np.zeros((1, 32, 32), bool)
+    dense[0, 3, 2] = True
+    lat2 = synth.Lattice(1, 32, 32, synth.pack_bits(dense), None)
+    cost2, _, _ = oracle.dijkstra(lat2, net[0])
+    assert cost2 == oracle.lo_inf()
+
+
+def test_disconnected_by_wall():
+    dense = np.zeros((2, 32, 32), bool)
+    dense[:, :, 16] = True  # full wall on both layers
+    lat = synth.Lattice(2, 32, 32, synth.pack_bits(dense), None)
+    net = np.array([(0, 2, 3, 1, 30, 5, 0, 0, 32, 32)], dtype=synth.NET_DTYPE)
+    assert oracle.dijkstra(lat, net[0])[0] == oracle.lo_inf()
+    assert oracle.astar_batch(lat, net)[0] == oracle.lo_inf()
+    assert oracle.sweep_batch(lat, net)[0][0] == oracle.lo_inf()
+    # a via hole does not help when both layers are walled; open one layer's wall
+    dense[1, 10, 16] = False
+    lat = synth.Lattice(2, 32, 32, synth.pack_bits(dense), None)
+    c = oracle.dijkstra(lat, net[0])[0]
+    assert c != oracle.lo_inf()
+    assert c == oracle.astar_batch(lat, net)[0] == oracle.sweep_batch(lat, net)[0][0]
