@@ -22,18 +22,32 @@ constexpr uint32_t kLabelInf = 0x7FFFFFFFu;
 constexpr int kMaxLayers = 8;
 
 struct LatticeDeviceView {
-  const uint32_t* blocked;  // [layers][height][words]
-  const uint32_t* via_ok;   // [layers-1][height][words] or nullptr
-  int32_t layers, height, width, words;
+  const uint32_t* blocked;    // row planes [layers][height][words], as uploaded
+  const uint32_t* via_ok;     // row planes [layers-1][height][words] or nullptr
+  // Sweep planes: every plane row carries one guard word on each side (data
+  // at +1), so a lane's 32-bit span fetch needs no bounds test.  Row-major
+  // planes serve frames whose rows are lattice rows; column-major planes
+  // (plane row = lattice column, bit = y) serve transposed frames.
+  const uint32_t* sweep_rows;      // [layers][height][words + 2]
+  const uint32_t* sweep_cols;      // [layers][width][words_t + 2]
+  const uint32_t* sweep_via_rows;  // [layers-1][height][words + 2] or nullptr
+  const uint32_t* sweep_via_cols;  // [layers-1][width][words_t + 2] or nullptr
+  int32_t layers, height, width, words, words_t;
   uint32_t orth, diag, via;
 };
 
-// Per-net workspace record produced by the host planner.
+// Per-net workspace record produced by the host planner.  The net is swept
+// in a frame whose rows are lattice rows (transposed == 0) or lattice
+// columns (transposed == 1, chosen when the window is taller than wide), so
+// the sequential sweep dimension is the window's shorter side.
 struct NetPlan {
-  uint32_t net;         // index into the caller's net array
-  uint32_t pitch;       // row pitch in cells (multiple of 4)
-  uint64_t dist_offset; // cell offset of this net's label slab in the pool
-  uint64_t mat_offset;  // word offset of this net's materialised-row bitmap
+  uint32_t net;          // index into the caller's net array
+  uint32_t pitch;        // frame row pitch in cells (multiple of 4)
+  uint64_t dist_offset;  // cell offset of this net's label slab in the pool
+  uint32_t rows;         // frame rows (swept sequentially)
+  uint32_t width;        // frame row width
+  uint32_t transposed;
+  uint32_t reserved;
 };
 
 struct SweepLaunch {
@@ -43,7 +57,6 @@ struct SweepLaunch {
   uint32_t plan_count;
   uint32_t max_sweeps;
   uint32_t* dist_pool;
-  uint32_t* mat_pool;
   apgar_b200_lattice_result* results;
   uint32_t* path_arena;
   uint64_t path_arena_capacity;

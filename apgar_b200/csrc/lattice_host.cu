@@ -18,8 +18,9 @@
 
 namespace apgar_b200 {
 
-size_t lattice_sweep_smem_bytes(int cells_per_lane, int layers, int max_rows);
-cudaError_t launch_lattice_sweep(int cells_per_lane, const SweepLaunch& launch, int layers,
+int lattice_cells_per_lane(int layers);
+size_t lattice_sweep_smem_bytes(int layers, int warps_per_net, int max_rows);
+cudaError_t launch_lattice_sweep(int layers, int warps_per_net, const SweepLaunch& launch,
                                  int max_rows, cudaStream_t stream);
 cudaError_t launch_lattice_pack(apgar_b200_lattice_result* results, uint32_t count,
                                 unsigned long long* total, const uint32_t* arena, uint32_t* paths,
@@ -27,14 +28,16 @@ cudaError_t launch_lattice_pack(apgar_b200_lattice_result* results, uint32_t cou
 
 namespace {
 
-constexpr int kClasses[] = {4, 8, 16, 32, 64};
+// Width classes: warps per net (each lane holds lattice_cells_per_lane(L)
+// cells of every layer, so a class covers 32 * C * G cells of a frame row).
+constexpr int kGroupSizes[] = {1, 2, 4, 8, 16};
 constexpr int kClassCount = 5;
 constexpr size_t kMaxSmemPerBlock = 227 * 1024;
 
 struct LatticeObject;
 
 struct ClassRange {
-  int cells_per_lane = 0;
+  int warps_per_net = 0;
   uint32_t begin = 0;  // into plans
   uint32_t count = 0;
   int max_rows = 0;
@@ -85,6 +88,7 @@ struct LatticeObject {
   LatticeDeviceView view{};
   DeviceBuffer<uint32_t> blocked;
   DeviceBuffer<uint32_t> via_ok;
+  DeviceBuffer<uint32_t> sweep_rows, sweep_cols, sweep_via_rows, sweep_via_cols;
   std::mutex route_mutex;
   std::unique_ptr<PlanObject> route_plan;  // reusable workspace for route()
 };
@@ -99,11 +103,62 @@ int check_device(int expected) {
   return APGAR_B200_OK;
 }
 
-int class_for_width(uint32_t w) {
-  for (int c : kClasses) {
-    if (static_cast<uint32_t>(c) * 32u >= w) return c;
+// Smallest width class whose row coverage holds `width` cells; -1 if none.
+int class_for_width(uint32_t width, int layers) {
+  const uint32_t per_warp = 32u * static_cast<uint32_t>(lattice_cells_per_lane(layers));
+  for (int i = 0; i < kClassCount; ++i) {
+    if (per_warp * static_cast<uint32_t>(kGroupSizes[i]) >= width) return i;
   }
-  return 0;
+  return -1;
+}
+
+// Guard-padded sweep planes from row-major bit planes `in`
+// ([planes][height][width/32], bit x%32 of word x/32).  Row form: each plane
+// row is [guard][words][guard]; column form: plane row x holds bit y of
+// column x.  Guards and the bits past `height` in the column form read as
+// `pad`.
+std::vector<uint32_t> sweep_planes(const uint32_t* in, int planes, int height, int width,
+                                   bool columns, uint32_t pad) {
+  const int words = width / 32;
+  const int words_t = (height + 31) / 32;
+  if (!columns) {
+    const size_t stride = static_cast<size_t>(words) + 2;
+    std::vector<uint32_t> out(static_cast<size_t>(planes) * height * stride, pad);
+    for (int l = 0; l < planes; ++l) {
+      for (int y = 0; y < height; ++y) {
+        const uint32_t* src = in + (static_cast<size_t>(l) * height + y) * words;
+        uint32_t* dst = out.data() + (static_cast<size_t>(l) * height + y) * stride + 1;
+        std::memcpy(dst, src, static_cast<size_t>(words) * sizeof(uint32_t));
+      }
+    }
+    return out;
+  }
+  const size_t stride = static_cast<size_t>(words_t) + 2;
+  std::vector<uint32_t> out(static_cast<size_t>(planes) * width * stride, 0u);
+  for (int l = 0; l < planes; ++l) {
+    uint32_t* plane = out.data() + static_cast<size_t>(l) * width * stride;
+    for (int x = 0; x < width; ++x) {
+      plane[static_cast<size_t>(x) * stride] = pad;
+      plane[static_cast<size_t>(x) * stride + stride - 1] = pad;
+    }
+    for (int y = 0; y < height; ++y) {
+      const uint32_t* row = in + (static_cast<size_t>(l) * height + y) * words;
+      for (int wi = 0; wi < words; ++wi) {
+        uint32_t bits = row[wi];
+        while (bits != 0u) {
+          const int b = __builtin_ctz(bits);
+          bits &= bits - 1u;
+          const int x = wi * 32 + b;
+          plane[static_cast<size_t>(x) * stride + 1 + (y >> 5)] |= 1u << (y & 31);
+        }
+      }
+    }
+    if (pad != 0u && (height & 31) != 0) {
+      const uint32_t tail = ~((1u << (height & 31)) - 1u);
+      for (int x = 0; x < width; ++x) plane[static_cast<size_t>(x) * stride + words_t] |= tail;
+    }
+  }
+  return out;
 }
 
 // Builds (or rebuilds into existing buffers) a plan for `nets`.
@@ -138,10 +193,10 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
     if (!in_lattice) continue;
     const uint64_t cells = static_cast<uint64_t>(v.layers) * n.win_w * n.win_h;
     if (cells * max_move >= kLabelInf) continue;  // uint32 cost domain not provable
-    const int c = class_for_width(n.win_w);
-    if (c == 0 || n.win_h > 32000u) continue;
-    int ci = 0;
-    while (kClasses[ci] != c) ++ci;
+    const uint32_t frame_width = std::max(n.win_w, n.win_h);
+    const uint32_t frame_rows = std::min(n.win_w, n.win_h);
+    const int ci = class_for_width(frame_width, v.layers);
+    if (ci < 0 || frame_rows > 32000u) continue;
     members[ci].push_back(i);
   }
   plan->rejected_template = init;
@@ -161,22 +216,24 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
       return ca > cb;
     });
     ClassRange range;
-    range.cells_per_lane = kClasses[ci];
+    range.warps_per_net = kGroupSizes[ci];
     range.begin = static_cast<uint32_t>(plans.size());
     range.count = static_cast<uint32_t>(m.size());
     for (uint32_t i : m) {
       const apgar_b200_lattice_net& n = host_nets[i];
       NetPlan np{};
       np.net = i;
-      np.pitch = (n.win_w + 3u) & ~3u;
+      np.transposed = n.win_h > n.win_w ? 1u : 0u;
+      np.rows = np.transposed ? n.win_w : n.win_h;
+      np.width = np.transposed ? n.win_h : n.win_w;
+      np.pitch = (np.width + 3u) & ~3u;
       np.dist_offset = dist_cells;
-      np.mat_offset = 0;
-      dist_cells += static_cast<uint64_t>(v.layers) * n.win_h * np.pitch;
+      dist_cells += static_cast<uint64_t>(v.layers) * np.rows * np.pitch;
       arena_cells += 8ull * (n.win_w + n.win_h) + 64ull * v.layers;
-      range.max_rows = std::max(range.max_rows, static_cast<int>(n.win_h));
+      range.max_rows = std::max(range.max_rows, static_cast<int>(np.rows));
       plans.push_back(np);
     }
-    if (lattice_sweep_smem_bytes(range.cells_per_lane, v.layers, range.max_rows) >
+    if (lattice_sweep_smem_bytes(v.layers, range.warps_per_net, range.max_rows) >
         kMaxSmemPerBlock) {
       return set_error(APGAR_B200_UNSUPPORTED, "window too tall for the shared-memory row map");
     }
@@ -240,7 +297,6 @@ int execute_plan(PlanObject* plan, cudaStream_t stream) {
   base.nets = plan->nets.get();
   base.max_sweeps = plan->max_sweeps;
   base.dist_pool = plan->dist_pool.get();
-  base.mat_pool = nullptr;
   base.results = plan->results.get();
   base.path_arena = plan->arena.get();
   base.path_arena_capacity = plan->arena_capacity;
@@ -259,7 +315,7 @@ int execute_plan(PlanObject* plan, cudaStream_t stream) {
       APGAR_B200_CUDA("cudaStreamWaitEvent", cudaStreamWaitEvent(s, plan->fork, 0));
     }
     APGAR_B200_CUDA("lattice sweep launch",
-                    launch_lattice_sweep(c.cells_per_lane, launch, v.layers, c.max_rows, s));
+                    launch_lattice_sweep(v.layers, c.warps_per_net, launch, c.max_rows, s));
     if (fan_out) {
       APGAR_B200_CUDA("cudaEventRecord(join)", cudaEventRecord(plan->joins[k], s));
       APGAR_B200_CUDA("cudaStreamWaitEvent", cudaStreamWaitEvent(stream, plan->joins[k], 0));
@@ -304,7 +360,8 @@ extern "C" int apgar_b200_lattice_upload(const apgar_b200_lattice_desc* d, void*
   if (d == nullptr || out == nullptr || d->blocked == nullptr) {
     return set_error(APGAR_B200_INTERNAL_INVARIANT, "lattice upload received a null argument");
   }
-  if (d->layers < 1 || d->layers > kMaxLayers || d->height < 1 || d->width < 32 ||
+  if (d->layers < 1 || d->layers > kMaxLayers || d->layers == 5 || d->layers == 7 ||
+      d->height < 1 || d->width < 32 ||
       d->width % 32 != 0 || d->orth == 0 || d->diag == 0 || d->via == 0 ||
       d->orth > 0xFFFFu || d->diag > 0xFFFFu || d->via > 0xFFFFu) {
     return set_error(APGAR_B200_INTERNAL_INVARIANT,
@@ -327,8 +384,48 @@ extern "C" int apgar_b200_lattice_upload(const apgar_b200_lattice_desc* d, void*
                       cudaMemcpy(lat->via_ok.get(), d->via_ok, via_words * sizeof(uint32_t),
                                  cudaMemcpyHostToDevice));
     }
+    // guard-padded sweep planes in both orientations
+    const size_t words_t = static_cast<size_t>((d->height + 31) / 32);
+    auto upload = [&](DeviceBuffer<uint32_t>& dst, const std::vector<uint32_t>& src,
+                      const char* what) -> int {
+      APGAR_B200_CUDA(what, dst.ensure(src.size()));
+      APGAR_B200_CUDA(what, cudaMemcpy(dst.get(), src.data(), src.size() * sizeof(uint32_t),
+                                       cudaMemcpyHostToDevice));
+      return APGAR_B200_OK;
+    };
+    if (int rc = upload(lat->sweep_rows,
+                        sweep_planes(d->blocked, d->layers, d->height, d->width, false, ~0u),
+                        "upload(sweep rows)");
+        rc != APGAR_B200_OK) {
+      return rc;
+    }
+    if (int rc = upload(lat->sweep_cols,
+                        sweep_planes(d->blocked, d->layers, d->height, d->width, true, ~0u),
+                        "upload(sweep columns)");
+        rc != APGAR_B200_OK) {
+      return rc;
+    }
+    if (d->via_ok != nullptr && d->layers > 1) {
+      if (int rc = upload(lat->sweep_via_rows,
+                          sweep_planes(d->via_ok, d->layers - 1, d->height, d->width, false, 0u),
+                          "upload(sweep via rows)");
+          rc != APGAR_B200_OK) {
+        return rc;
+      }
+      if (int rc = upload(lat->sweep_via_cols,
+                          sweep_planes(d->via_ok, d->layers - 1, d->height, d->width, true, 0u),
+                          "upload(sweep via columns)");
+          rc != APGAR_B200_OK) {
+        return rc;
+      }
+    }
     lat->view.blocked = lat->blocked.get();
     lat->view.via_ok = lat->via_ok.get();
+    lat->view.sweep_rows = lat->sweep_rows.get();
+    lat->view.sweep_cols = lat->sweep_cols.get();
+    lat->view.sweep_via_rows = lat->sweep_via_rows.get();
+    lat->view.sweep_via_cols = lat->sweep_via_cols.get();
+    lat->view.words_t = static_cast<int32_t>(words_t);
     lat->view.layers = d->layers;
     lat->view.height = d->height;
     lat->view.width = d->width;

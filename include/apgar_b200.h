@@ -105,7 +105,7 @@ typedef struct apgar_b200_lattice_result {
   uint32_t sweeps;       /* row sweeps executed (including the final quiet one) */
   uint32_t path_len;     /* cells in the reverse path (goal first) */
   uint64_t path_offset;  /* into the packed path array */
-  uint64_t arena_offset; /* internal staging offset */
+  uint64_t arena_offset; /* internal staging offset; zero once results are packed */
   uint32_t row_steps;    /* window rows processed (all layers of a row = 1) */
   uint32_t row_stores;   /* layer rows written back */
   uint32_t row_loads;    /* layer rows read (current and re-read predecessor rows) */

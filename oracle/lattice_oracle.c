@@ -371,17 +371,51 @@ uint32_t lo_astar(const lo_lattice* lat, const lo_net* net, uint64_t* expanded_o
 
 /* --------------------------- sweep schedule --------------------------- */
 
-/* Row step semantics (one window row, all layers together), identical to the
- * GPU kernel: relax from the previous row in sweep order (orthogonal plus the
- * two diagonals), then repeat {east scan, west scan, via cascade up then down}
- * until the via cascade changes nothing.  A row is skipped when neither it nor
- * its predecessor row changed since the last sweep in the same direction (or,
- * for the first sweep in each direction, when both rows are still all-INF). */
+/* The GPU sweeps a window along its shorter side: when the window is taller
+ * than wide it works in a transposed frame whose rows are lattice columns.
+ * Frame cell (r, p) is lattice (x = p, y = r) normally and (x = r, y = p) when
+ * transposed; the move model is symmetric under that swap. */
+typedef struct frame {
+  const win_ctx* c;
+  int transposed;
+  int R, K; /* rows (swept sequentially) and row width */
+} frame;
+
+static inline int ffree(const frame* f, int l, int r, int p) {
+  if (r < 0 || p < 0 || r >= f->R || p >= f->K) return 0;
+  return f->transposed ? cell_free(f->c, l, r, p) : cell_free(f->c, l, p, r);
+}
+
+static inline int fvia(const frame* f, int lower, int r, int p) {
+  return f->transposed ? via_legal(f->c, lower, r, p) : via_legal(f->c, lower, p, r);
+}
+
+/* planar move (r0,p0) -> (r1,p1) with |dr|,|dp| <= 1 */
+static inline int fmove(const frame* f, int l, int r0, int p0, int r1, int p1) {
+  if (!ffree(f, l, r0, p0) || !ffree(f, l, r1, p1)) return 0;
+  if (r0 == r1 || p0 == p1) return 1;
+  return ffree(f, l, r0, p1) && ffree(f, l, r1, p0);
+}
+
+/* Row step semantics (one frame row, all layers together), identical to the
+ * GPU kernel: relax from the previous row in sweep order (straight plus the
+ * two diagonals), then repeat {two-sided row scan, via cascade up then down}
+ * until the via cascade changes nothing.  A row is skipped when neither it
+ * nor its predecessor row changed since the last sweep in the same direction
+ * (or, for the first sweep in each direction, when both rows are all-INF). */
 uint32_t lo_sweep_schedule(const lo_lattice* lat, const lo_net* net, uint32_t max_sweeps,
                            uint32_t* dist, lo_sweep_stats* stats) {
+  return lo_sweep_schedule_oriented(lat, net, max_sweeps, -1, dist, stats);
+}
+
+uint32_t lo_sweep_schedule_oriented(const lo_lattice* lat, const lo_net* net, uint32_t max_sweeps,
+                                    int transposed, uint32_t* dist, lo_sweep_stats* stats) {
   win_ctx c;
   ctx_init(&c, lat, net);
   const int L = c.L, w = c.w, h = c.h;
+  const int tr = transposed < 0 ? (h > w) : transposed;
+  frame f = {&c, tr, tr ? w : h, tr ? h : w};
+  const int R = f.R, K = f.K;
   const size_t cells = (size_t)L * w * h;
   for (size_t i = 0; i < cells; ++i) dist[i] = LO_INF;
   lo_sweep_stats st = {0};
@@ -393,27 +427,32 @@ uint32_t lo_sweep_schedule(const lo_lattice* lat, const lo_net* net, uint32_t ma
     if (stats) *stats = st;
     return LO_INF;
   }
+  const int sr = f.transposed ? sx : sy, sp = f.transposed ? sy : sx;
+  uint32_t* fd = (uint32_t*)malloc(cells * sizeof(uint32_t)); /* frame labels */
+  for (size_t i = 0; i < cells; ++i) fd[i] = LO_INF;
+#define FD(l, r, p) fd[((size_t)(l) * R + (r)) * K + (p)]
   const int32_t kNever = -1000000;
-  int32_t* modified = (int32_t*)malloc((size_t)h * sizeof(int32_t));
-  for (int y = 0; y < h; ++y) modified[y] = kNever;
-  dist[cell_index(&c, sl, sx, sy)] = 0;
-  modified[sy] = 0; /* initialisation writes the start row on every layer */
+  int32_t* modified = (int32_t*)malloc((size_t)R * sizeof(int32_t));
+  for (int r = 0; r < R; ++r) modified[r] = kNever;
+  FD(sl, sr, sp) = 0;
+  modified[sr] = 0; /* initialisation writes the start row on every layer */
   st.row_stores += (uint64_t)L;
-  st.cells_stored += (uint64_t)L * w;
-  uint32_t* row = (uint32_t*)malloc((size_t)L * w * sizeof(uint32_t));
-  uint32_t* orig = (uint32_t*)malloc((size_t)L * w * sizeof(uint32_t));
+  st.cells_stored += (uint64_t)L * K;
+  uint32_t* row = (uint32_t*)malloc((size_t)L * K * sizeof(uint32_t));
+  uint32_t* orig = (uint32_t*)malloc((size_t)L * K * sizeof(uint32_t));
+  uint32_t* east = (uint32_t*)malloc((size_t)K * sizeof(uint32_t));
   uint32_t sweeps = 0;
   for (uint32_t k = 1; k <= max_sweeps; ++k) {
     sweeps = k;
     const int up = (k & 1) != 0;
-    const int dy = up ? 1 : -1;
+    const int dr = up ? 1 : -1;
     int any_change = 0;
     int prev_in_regs = 0;
-    for (int step = 0; step < h; ++step) {
-      const int y = up ? step : h - 1 - step;
-      const int p = y - dy; /* previous row in sweep order */
-      const int32_t mp = (p >= 0 && p < h) ? modified[p] : kNever;
-      const int32_t my = modified[y];
+    for (int step = 0; step < R; ++step) {
+      const int r = up ? step : R - 1 - step;
+      const int pr = r - dr; /* previous row in sweep order */
+      const int32_t mp = (pr >= 0 && pr < R) ? modified[pr] : kNever;
+      const int32_t my = modified[r];
       int skip;
       if (k <= 2) {
         skip = (mp == kNever && my == kNever);
@@ -425,102 +464,94 @@ uint32_t lo_sweep_schedule(const lo_lattice* lat, const lo_net* net, uint32_t ma
         continue;
       }
       if (mp != kNever && !prev_in_regs) {
-        st.cells_loaded += (uint64_t)L * w; /* predecessor row reload */
+        st.cells_loaded += (uint64_t)L * K; /* predecessor row reload */
         st.row_loads += (uint64_t)L;
       }
       if (my != kNever) {
-        st.cells_loaded += (uint64_t)L * w;
+        st.cells_loaded += (uint64_t)L * K;
         st.row_loads += (uint64_t)L;
       }
       st.row_visits += 1;
       for (int l = 0; l < L; ++l) {
-        for (int x = 0; x < w; ++x) {
-          row[l * w + x] = dist[cell_index(&c, l, x, y)];
-        }
+        for (int p = 0; p < K; ++p) row[l * K + p] = FD(l, r, p);
       }
-      memcpy(orig, row, (size_t)L * w * sizeof(uint32_t));
-      if (p >= 0 && p < h && mp != kNever) {
-        /* moves from row p into row y: straight (dy), and diagonals from x-1 and x+1 */
-        const int d_straight = up ? 2 : 6;        /* N or S */
-        const int d_from_left = up ? 1 : 7;       /* NE or SE: from (x-1, p) */
-        const int d_from_right = up ? 3 : 5;      /* NW or SW: from (x+1, p) */
+      memcpy(orig, row, (size_t)L * K * sizeof(uint32_t));
+      if (pr >= 0 && pr < R && mp != kNever) {
         for (int l = 0; l < L; ++l) {
-          for (int x = 0; x < w; ++x) {
-            uint64_t best = row[l * w + x];
-            uint32_t pd = dist[cell_index(&c, l, x, p)];
-            if (pd != LO_INF && planar_legal(&c, l, x, p, d_straight)) {
-              if ((uint64_t)pd + lat->orth < best) best = (uint64_t)pd + lat->orth;
+          for (int p = 0; p < K; ++p) {
+            uint64_t best = row[l * K + p];
+            for (int q = p - 1; q <= p + 1; ++q) {
+              if (q < 0 || q >= K) continue;
+              const uint32_t pd = FD(l, pr, q);
+              if (pd == LO_INF || !fmove(&f, l, pr, q, r, p)) continue;
+              const uint64_t cand = (uint64_t)pd + (q == p ? lat->orth : lat->diag);
+              if (cand < best) best = cand;
             }
-            if (x > 0) {
-              pd = dist[cell_index(&c, l, x - 1, p)];
-              if (pd != LO_INF && planar_legal(&c, l, x - 1, p, d_from_left)) {
-                if ((uint64_t)pd + lat->diag < best) best = (uint64_t)pd + lat->diag;
-              }
-            }
-            if (x + 1 < w) {
-              pd = dist[cell_index(&c, l, x + 1, p)];
-              if (pd != LO_INF && planar_legal(&c, l, x + 1, p, d_from_right)) {
-                if ((uint64_t)pd + lat->diag < best) best = (uint64_t)pd + lat->diag;
-              }
-            }
-            row[l * w + x] = (uint32_t)best;
+            row[l * K + p] = (uint32_t)best;
           }
         }
       }
       for (;;) {
         for (int l = 0; l < L; ++l) {
-          for (int x = 1; x < w; ++x) { /* east scan */
-            const uint32_t a = row[l * w + x - 1];
-            if (a != LO_INF && planar_legal(&c, l, x - 1, y, 0) &&
-                (uint64_t)a + lat->orth < row[l * w + x]) {
-              row[l * w + x] = a + lat->orth;
+          uint32_t* v = row + (size_t)l * K;
+          /* two-sided scan: min(east scan, west scan) of the same input,
+           * which equals an east scan followed by a west scan */
+          uint64_t carry = LO_INF;
+          for (int p = 0; p < K; ++p) {
+            uint64_t e = v[p];
+            if (p > 0 && carry != LO_INF && fmove(&f, l, r, p - 1, r, p) &&
+                carry + lat->orth < e) {
+              e = carry + lat->orth;
             }
+            east[p] = (uint32_t)e;
+            carry = e;
           }
-          for (int x = w - 2; x >= 0; --x) { /* west scan */
-            const uint32_t a = row[l * w + x + 1];
-            if (a != LO_INF && planar_legal(&c, l, x + 1, y, 4) &&
-                (uint64_t)a + lat->orth < row[l * w + x]) {
-              row[l * w + x] = a + lat->orth;
+          carry = LO_INF;
+          for (int p = K - 1; p >= 0; --p) {
+            uint64_t wv = v[p];
+            if (p + 1 < K && carry != LO_INF && fmove(&f, l, r, p + 1, r, p) &&
+                carry + lat->orth < wv) {
+              wv = carry + lat->orth;
             }
+            carry = wv;
+            v[p] = east[p] < wv ? east[p] : (uint32_t)wv;
           }
         }
         int via_change = 0;
         for (int l = 1; l < L; ++l) {
-          for (int x = 0; x < w; ++x) {
-            const uint32_t a = row[(l - 1) * w + x];
-            if (a != LO_INF && via_legal(&c, l - 1, x, y) &&
-                (uint64_t)a + lat->via < row[l * w + x]) {
-              row[l * w + x] = a + lat->via;
+          for (int p = 0; p < K; ++p) {
+            const uint32_t a = row[(l - 1) * K + p];
+            if (a != LO_INF && fvia(&f, l - 1, r, p) && (uint64_t)a + lat->via < row[l * K + p]) {
+              row[l * K + p] = a + lat->via;
               via_change = 1;
             }
           }
         }
         for (int l = L - 2; l >= 0; --l) {
-          for (int x = 0; x < w; ++x) {
-            const uint32_t a = row[(l + 1) * w + x];
-            if (a != LO_INF && via_legal(&c, l, x, y) &&
-                (uint64_t)a + lat->via < row[l * w + x]) {
-              row[l * w + x] = a + lat->via;
+          for (int p = 0; p < K; ++p) {
+            const uint32_t a = row[(l + 1) * K + p];
+            if (a != LO_INF && fvia(&f, l, r, p) && (uint64_t)a + lat->via < row[l * K + p]) {
+              row[l * K + p] = a + lat->via;
               via_change = 1;
             }
           }
         }
         if (!via_change) break;
       }
-      int changed = memcmp(orig, row, (size_t)L * w * sizeof(uint32_t)) != 0;
+      int changed = memcmp(orig, row, (size_t)L * K * sizeof(uint32_t)) != 0;
       if (changed) {
         /* a newly materialised row stores every layer; afterwards only the
          * layers whose labels changed are written back */
         const int materialise = (my == kNever);
         for (int l = 0; l < L; ++l) {
           const int layer_changed =
-              memcmp(orig + (size_t)l * w, row + (size_t)l * w, (size_t)w * sizeof(uint32_t)) != 0;
+              memcmp(orig + (size_t)l * K, row + (size_t)l * K, (size_t)K * sizeof(uint32_t)) != 0;
           if (!layer_changed && !materialise) continue;
-          for (int x = 0; x < w; ++x) dist[cell_index(&c, l, x, y)] = row[l * w + x];
+          for (int p = 0; p < K; ++p) FD(l, r, p) = row[l * K + p];
           st.row_stores += 1;
-          st.cells_stored += (uint64_t)w;
+          st.cells_stored += (uint64_t)K;
         }
-        modified[y] = (int32_t)k;
+        modified[r] = (int32_t)k;
         any_change = 1;
       }
       prev_in_regs = 1;
@@ -528,9 +559,19 @@ uint32_t lo_sweep_schedule(const lo_lattice* lat, const lo_net* net, uint32_t ma
     if (!any_change && k >= 2) break;
   }
   st.sweeps = sweeps;
+  for (int l = 0; l < L; ++l) {
+    for (int y = 0; y < h; ++y) {
+      for (int x = 0; x < w; ++x) {
+        dist[cell_index(&c, l, x, y)] = f.transposed ? FD(l, x, y) : FD(l, y, x);
+      }
+    }
+  }
+#undef FD
+  free(east);
   free(row);
   free(orig);
   free(modified);
+  free(fd);
   if (stats) *stats = st;
   return dist[cell_index(&c, gl, gx, gy)];
 }

@@ -79,6 +79,11 @@ typedef struct lo_sweep_stats {
 uint32_t lo_sweep_schedule(const lo_lattice* lat, const lo_net* net, uint32_t max_sweeps,
                            uint32_t* dist, lo_sweep_stats* stats);
 
+/* Same schedule with the frame orientation forced (transposed = 0 sweeps along
+ * lattice y, 1 along lattice x, -1 picks the window's shorter side). */
+uint32_t lo_sweep_schedule_oriented(const lo_lattice* lat, const lo_net* net, uint32_t max_sweeps,
+                                    int transposed, uint32_t* dist, lo_sweep_stats* stats);
+
 /* Batch helpers, parallel over nets with up to `threads` POSIX threads. */
 void lo_dijkstra_batch(const lo_lattice* lat, const lo_net* nets, uint32_t count, int threads,
                        uint32_t* costs, uint32_t* path_lens, uint64_t* path_offsets,
