@@ -1,0 +1,48 @@
+// Shared definitions for the drop-in (reference device-view) engine.
+//
+// States are node*9 + incoming heading (planar_router.h:261-272); labels are
+// uint64 with UINT64_MAX as the unreachable sentinel and every sum checked
+// against it (planar_router.cu:332-340).
+#pragma once
+
+#include <cstdint>
+
+#include "apgar_b200.h"
+
+namespace apgar_b200 {
+
+constexpr uint64_t kGraphInf = ~0ull;
+constexpr uint32_t kInvalid32 = 0xFFFFFFFFu;
+
+struct GraphDeviceView {
+  const uint32_t* neighbors;  // [8][nodes], kInvalid32 where no edge
+  const uint8_t* legal;       // [nodes] legal-edge masks
+  uint32_t node_count;
+  uint32_t orth, diag, bend;
+  // association fields repeated into every result header
+  uint32_t compiler_version;
+  uint64_t source_board_content_hash, compiler_profile_fingerprint, rule_bucket_identity;
+  uint64_t device_view_fingerprint;
+};
+
+struct GraphLaunch {
+  GraphDeviceView g;
+  const apgar_b200_batch_query_v1* queries;
+  uint32_t query_count;
+  const apgar_b200_policy_edge_v1* policy;
+  uint64_t* labels;         // [Q][9N]
+  uint32_t* queues;         // [Q][2][N] node frontier queues
+  uint32_t* stamps;         // [Q][N] enqueue round stamps
+  apgar_b200_batch_result_v1* results;   // [Q]
+  apgar_b200_compact_path_v1* compact;   // [Q] (compact mode)
+  uint32_t* path_stage;     // [Q][9N] reverse paths before packing (compact mode)
+  uint32_t* predecessors;   // [Q][9N] (workspace mode)
+  uint64_t* state_owners;   // [Q][9N] (workspace mode)
+  uint64_t* predecessor_owners;  // [Q][9N] (workspace mode)
+  uint32_t maximum_rounds;
+  uint8_t generator;
+  uint8_t workspace_mode;   // 1: converge fully and emit predecessors; 0: compact path
+  const volatile uint32_t* cancel;  // host-mapped flag or nullptr
+};
+
+}  // namespace apgar_b200

@@ -1,0 +1,677 @@
+// Host side of the drop-in seam: device-view upload with validation,
+// candidate-batch admission, execution on the device engine
+// (graph_search.cu) and readback in the reference V1 record formats.  No CPU
+// search fallback exists: every admitted query is searched on the GPU.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <set>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "graph_common.cuh"
+#include "host_common.h"
+
+static_assert(sizeof(apgar_b200_compiled_header_v1) == 112, "DeviceCompiledHeaderV1 layout");
+static_assert(sizeof(apgar_b200_layer_range_v1) == 48, "DeviceLayerRangeV1 layout");
+static_assert(sizeof(apgar_b200_node_v1) == 56, "DeviceNodeV1 layout");
+static_assert(sizeof(apgar_b200_run_v1) == 12, "DeviceRunV1 layout");
+static_assert(sizeof(apgar_b200_policy_edge_v1) == 16, "DeviceCandidatePolicyEdgeV1 layout");
+static_assert(sizeof(apgar_b200_batch_query_v1) == 120, "DeviceCandidateBatchQueryV1 layout");
+static_assert(sizeof(apgar_b200_batch_result_v1) == 120, "DeviceCandidateBatchResultV1 layout");
+static_assert(sizeof(apgar_b200_compact_path_v1) == 32, "DeviceCandidateCompactPathV1 layout");
+static_assert(sizeof(apgar_b200_route_result_header_v1) == 64, "DeviceRouteResultHeaderV1 layout");
+
+namespace apgar_b200 {
+
+cudaError_t launch_graph_search(const GraphLaunch& launch, cudaStream_t stream);
+cudaError_t launch_graph_pack(apgar_b200_compact_path_v1* compact, uint32_t count,
+                              uint64_t states_per_query, const uint32_t* stage, uint32_t* packed,
+                              unsigned long long* total, int sm_count, cudaStream_t stream);
+
+namespace {
+
+using U128 = unsigned __int128;
+constexpr uint64_t kMaximumRepresentedNodes = 10'000'000;  // compiled_board.h:21
+constexpr uint64_t kMaximumPolicyEntries = 1'000'000;      // candidate_policy.h:18
+constexpr int kDx[8] = {1, 1, 0, -1, -1, -1, 0, 1};
+constexpr int kDy[8] = {0, 1, 1, 1, 0, -1, -1, -1};
+
+int invariant(const std::string& detail) { return set_error(APGAR_B200_INTERNAL_INVARIANT, detail); }
+
+// One execution at a time per view, from execute until release (the
+// reference's prepared-view execution lease), independent of the thread.
+struct Lease {
+  std::mutex m;
+  std::condition_variable cv;
+  bool busy = false;
+  void acquire() {
+    std::unique_lock<std::mutex> lock(m);
+    cv.wait(lock, [&] { return !busy; });
+    busy = true;
+  }
+  void release() {
+    {
+      std::lock_guard<std::mutex> lock(m);
+      busy = false;
+    }
+    cv.notify_one();
+  }
+};
+
+struct Workspace {
+  DeviceBuffer<apgar_b200_batch_query_v1> queries;
+  DeviceBuffer<apgar_b200_policy_edge_v1> policy;
+  DeviceBuffer<apgar_b200_batch_result_v1> results;
+  DeviceBuffer<apgar_b200_compact_path_v1> compact;
+  DeviceBuffer<uint64_t> labels;
+  DeviceBuffer<uint32_t> queues;
+  DeviceBuffer<uint32_t> stamps;
+  DeviceBuffer<uint32_t> stage;  // compact: staged paths; workspace: predecessors
+  DeviceBuffer<uint64_t> owners;
+  DeviceBuffer<uint64_t> pred_owners;
+  DeviceBuffer<unsigned long long> counters;
+  uint64_t bytes() const {
+    return queries.bytes() + policy.bytes() + results.bytes() + compact.bytes() + labels.bytes() +
+           queues.bytes() + stamps.bytes() + stage.bytes() + owners.bytes() + pred_owners.bytes() +
+           counters.bytes();
+  }
+};
+
+struct ViewObject {
+  int device = -1;
+  int sm_count = 0;
+  apgar_b200_compiled_header_v1 header{};
+  std::vector<uint8_t> legal;  // host copy for policy-edge admission
+  uint64_t persistent_bytes = 0;
+  DeviceBuffer<uint32_t> neighbors;
+  DeviceBuffer<uint8_t> legal_dev;
+  Lease lease;
+  Workspace ws;
+  uint32_t* cancel_host = nullptr;
+  uint32_t* cancel_dev = nullptr;
+  ~ViewObject() {
+    if (cancel_host != nullptr) cudaFreeHost(cancel_host);
+  }
+  GraphDeviceView device_view() const {
+    GraphDeviceView g{};
+    g.neighbors = neighbors.get();
+    g.legal = legal_dev.get();
+    g.node_count = static_cast<uint32_t>(legal.size());
+    g.orth = header.orthogonal_step;
+    g.diag = header.diagonal_step;
+    g.bend = header.bend;
+    g.compiler_version = header.compiler_version;
+    g.source_board_content_hash = header.source_board_content_hash;
+    g.compiler_profile_fingerprint = header.compiler_profile_fingerprint;
+    g.rule_bucket_identity = header.rule_bucket_identity;
+    g.device_view_fingerprint = header.device_view_fingerprint;
+    return g;
+  }
+};
+
+struct PendingBatch {
+  ViewObject* view = nullptr;
+  bool leased = false;
+  bool workspace_mode = false;
+  uint32_t query_count = 0;
+  uint64_t states = 0;
+  uint64_t batch_bytes = 0;
+  float kernel_ms = 0.0f;
+  uint64_t launches = 0;
+  ~PendingBatch() {
+    if (leased && view != nullptr) view->lease.release();
+  }
+};
+
+struct PendingRoute {
+  std::unique_ptr<PendingBatch> batch;
+  apgar_b200_route_result_header_v1 header{};
+};
+
+int check_device(int expected) {
+  int current = -1;
+  APGAR_B200_CUDA("cudaGetDevice", cudaGetDevice(&current));
+  if (current != expected) {
+    return set_error(APGAR_B200_BACKEND_FAILURE,
+                     "current CUDA device differs from the device the view was uploaded on");
+  }
+  return APGAR_B200_OK;
+}
+
+// Memory-safety and cost-domain checks of the reference upload validation
+// (gpu/cuda/planar_router.cu:1256-1451).  The FNV view fingerprint is not
+// recomputed here; the C++ adapter recomputes it with the reference routine.
+int validate_view(const apgar_b200_compiled_header_v1& h, const apgar_b200_layer_range_v1* layers,
+                  uint64_t layer_count, const apgar_b200_node_v1* nodes, uint64_t n,
+                  const apgar_b200_run_v1* runs, uint64_t run_count, const uint32_t* run_nodes,
+                  uint64_t run_node_count) {
+  if (h.schema_version != 1u || n == 0 || n > kMaximumRepresentedNodes || n >= 0xFFFFFFFFull ||
+      h.represented_nodes != n || 9ull * n >= 0xFFFFFFFFull || h.represented_states != 9ull * n) {
+    return invariant("upload rejected inconsistent schema or node/state count bounds");
+  }
+  if (h.lattice_step <= 0 || h.orthogonal_step == 0 || h.diagonal_step == 0 ||
+      h.heading_mask == 0 || (h.heading_mask & ~0x7u) != 0 ||
+      std::any_of(h.reserved, h.reserved + 7, [](uint8_t b) { return b != 0; })) {
+    return invariant("upload rejected invalid lattice, cost, heading-mask or reserved header fields");
+  }
+  const U128 max_transition =
+      static_cast<U128>(std::max(h.orthogonal_step, h.diagonal_step)) + h.bend;
+  if (max_transition * n * 8u >= static_cast<U128>(~0ull)) {
+    return invariant("upload rejected costs that exceed or collide with the finite route-cost bound");
+  }
+  if (layer_count == 0 || layers == nullptr) return invariant("upload rejected an empty layer partition");
+  uint64_t expected = 0;
+  for (uint64_t li = 0; li < layer_count; ++li) {
+    const apgar_b200_layer_range_v1& L = layers[li];
+    const uint64_t end = static_cast<uint64_t>(L.node_offset) + L.node_count;
+    if (L.node_count == 0 || L.node_offset != expected || end > n ||
+        L.minimum_lattice_x > L.maximum_lattice_x || L.minimum_lattice_y > L.maximum_lattice_y ||
+        (li != 0 && layers[li - 1].layer >= L.layer)) {
+      return invariant("upload rejected an invalid or non-canonical layer range");
+    }
+    int64_t mnx = nodes[L.node_offset].lattice_x, mxx = mnx;
+    int64_t mny = nodes[L.node_offset].lattice_y, mxy = mny;
+    for (uint64_t i = L.node_offset; i < end; ++i) {
+      if (nodes[i].layer != L.layer) return invariant("upload rejected a node outside its layer range");
+      mnx = std::min(mnx, nodes[i].lattice_x);
+      mxx = std::max(mxx, nodes[i].lattice_x);
+      mny = std::min(mny, nodes[i].lattice_y);
+      mxy = std::max(mxy, nodes[i].lattice_y);
+    }
+    if (mnx != L.minimum_lattice_x || mxx != L.maximum_lattice_x || mny != L.minimum_lattice_y ||
+        mxy != L.maximum_lattice_y) {
+      return invariant("upload rejected inexact layer bounds");
+    }
+    expected = end;
+  }
+  if (expected != n) return invariant("upload rejected a layer partition that does not cover all nodes");
+  for (uint64_t i = 0; i < n; ++i) {
+    const apgar_b200_node_v1& node = nodes[i];
+    if (node.reserved[0] | node.reserved[1] | node.reserved[2]) {
+      return invariant("upload rejected nonzero reserved node fields");
+    }
+    for (int d = 0; d < 8; ++d) {
+      const bool legal = (node.legal_edges >> d) & 1u;
+      const uint32_t nb = node.neighbors[d];
+      const uint8_t heading = d % 4 == 0 ? 1u : (d % 4 == 2 ? 2u : 4u);  // H, V, 45
+      if (legal != (nb != 0xFFFFFFFFu) || (legal && ((h.heading_mask & heading) == 0 || nb >= n))) {
+        return invariant("upload rejected a legal mask and neighbor-index disagreement");
+      }
+      if (!legal) continue;
+      const apgar_b200_node_v1& other = nodes[nb];
+      if (other.layer != node.layer || other.lattice_x != node.lattice_x + kDx[d] ||
+          other.lattice_y != node.lattice_y + kDy[d]) {
+        return invariant("upload rejected a non-adjacent neighbor index");
+      }
+      const int od = (d + 4) % 8;
+      if (((other.legal_edges >> od) & 1u) == 0 || other.neighbors[od] != i) {
+        return invariant("upload rejected an edge without its exact reverse edge");
+      }
+    }
+  }
+  // directional runs: bounds, direction, and exact coverage of legal edges
+  std::vector<uint8_t> covered(n, 0);
+  uint64_t run_offset = 0;
+  for (uint64_t ri = 0; ri < run_count; ++ri) {
+    const apgar_b200_run_v1& r = runs[ri];
+    const uint64_t end = static_cast<uint64_t>(r.node_offset) + r.node_count;
+    if (r.direction >= 8 || r.node_count < 2 || r.node_offset != run_offset || end > run_node_count ||
+        r.reserved[0] | r.reserved[1] | r.reserved[2]) {
+      return invariant("upload rejected invalid directional-run bounds or direction");
+    }
+    for (uint64_t k = r.node_offset; k + 1 < end; ++k) {
+      const uint32_t a = run_nodes[k], b = run_nodes[k + 1];
+      if (a >= n || b >= n || nodes[a].neighbors[r.direction] != b) {
+        return invariant("upload rejected an invalid directed run edge");
+      }
+      if (covered[a] & (1u << r.direction)) return invariant("upload rejected a duplicated run edge");
+      covered[a] |= static_cast<uint8_t>(1u << r.direction);
+    }
+    run_offset = end;
+  }
+  if (run_offset != run_node_count) return invariant("upload rejected unowned run-node storage");
+  for (uint64_t i = 0; i < n; ++i) {
+    if (covered[i] != nodes[i].legal_edges) {
+      return invariant("upload rejected incomplete directional-run edge coverage");
+    }
+  }
+  const U128 bytes = 112u + static_cast<U128>(layer_count) * 48u + static_cast<U128>(n) * 56u +
+                     static_cast<U128>(run_count) * 12u + static_cast<U128>(run_node_count) * 4u;
+  if (bytes != h.estimated_persistent_device_bytes) {
+    return invariant("upload rejected inconsistent persistent-memory accounting");
+  }
+  return APGAR_B200_OK;
+}
+
+// Candidate-batch admission (gpu/cuda/planar_router.cu:1731-1909): ordering,
+// ownership, associations, workspace bounds, policy encoding and the
+// cost-sentinel bound.
+int validate_batch(const ViewObject& v, const apgar_b200_batch_request& req,
+                   const apgar_b200_batch_query_v1* queries, uint32_t count,
+                   const apgar_b200_policy_edge_v1* edges, uint64_t edge_count) {
+  const uint64_t n = v.legal.size();
+  const uint64_t S = 9ull * n;
+  if (req.schema_version != 1u || req.batch_id == 0 || count == 0 ||
+      edge_count > kMaximumPolicyEntries || req.maximum_rounds == 0 || req.generator > 2) {
+    return invariant("candidate batch has invalid schema, identity, policy size, generator or rounds");
+  }
+  if (req.maximum_workspace_states_per_query < S) {
+    return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "batch exceeds the per-query workspace-state capacity");
+  }
+  const bool frontier = req.generator == APGAR_B200_GENERATOR_BUCKETED_FRONTIER;
+  if (frontier && req.maximum_frontier_states_per_query < S) {
+    return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "batch exceeds the per-query frontier-state capacity");
+  }
+  if (static_cast<U128>(S) * count > static_cast<U128>(1ull << 40)) {
+    return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "batch query-major state space is too large");
+  }
+  std::set<uint64_t> owners;
+  uint64_t expected_policy = 0;
+  for (uint32_t i = 0; i < count; ++i) {
+    const apgar_b200_batch_query_v1& q = queries[i];
+    const uint64_t pend = static_cast<uint64_t>(q.policy_offset) + q.policy_count;
+    if (q.schema_version != 1u || q.batch_id != req.batch_id || q.query_id == 0 ||
+        q.workspace_owner == 0 || q.generator != req.generator ||
+        q.maximum_rounds != req.maximum_rounds || q.start_node >= n || q.goal_node >= n ||
+        q.start_node == q.goal_node || q.workspace_offset != i * S || q.workspace_state_count != S ||
+        q.frontier_state_capacity != (frontier ? S : 0) || q.policy_offset != expected_policy ||
+        pend > 0xFFFFFFFFull || pend > edge_count || (q.reserved[0] | q.reserved[1] | q.reserved[2]) ||
+        (i != 0 && queries[i - 1].query_id >= q.query_id) || !owners.insert(q.workspace_owner).second) {
+      return invariant("candidate batch query ordering, ownership, association, endpoint, policy or "
+                       "workspace bounds are invalid");
+    }
+    uint64_t max_penalty = 0;
+    for (uint64_t e = q.policy_offset; e < pend; ++e) {
+      const apgar_b200_policy_edge_v1& pe = edges[e];
+      const uint32_t node = pe.physical_edge_index / 8u, dir = pe.physical_edge_index % 8u;
+      if (pe.reserved != 0 || node >= n || dir >= 4 || ((v.legal[node] >> dir) & 1u) == 0 ||
+          (e != q.policy_offset && edges[e - 1].physical_edge_index >= pe.physical_edge_index)) {
+        return invariant("candidate batch policy edge encoding is invalid or non-canonical");
+      }
+      if (pe.adjustment != ~0ull) max_penalty = std::max(max_penalty, pe.adjustment);
+    }
+    const U128 orth = static_cast<U128>(v.header.orthogonal_step) + q.orthogonal_step_surcharge;
+    const U128 diag = static_cast<U128>(v.header.diagonal_step) + q.diagonal_step_surcharge;
+    const U128 bend = static_cast<U128>(v.header.bend) + q.bend_surcharge;
+    const U128 max_t = std::max(orth, diag) + bend + max_penalty;
+    const U128 inf = static_cast<U128>(~0ull);
+    if (orth >= inf || diag >= inf || bend >= inf || max_t * n * 8u >= inf) {
+      return invariant("candidate batch policy cost bound collides with the unreachable sentinel");
+    }
+    expected_policy = pend;
+  }
+  if (expected_policy != edge_count) return invariant("candidate batch contains unowned policy-edge storage");
+  return APGAR_B200_OK;
+}
+
+int run_batch(ViewObject* v, const apgar_b200_batch_request& req,
+              const apgar_b200_batch_query_v1* queries, uint32_t count,
+              const apgar_b200_policy_edge_v1* edges, uint64_t edge_count,
+              const volatile uint8_t* cancel, PendingBatch* pending) {
+  const uint64_t n = v->legal.size();
+  const uint64_t S = 9ull * n;
+  const bool workspace_mode = req.generator == APGAR_B200_GENERATOR_BUCKETED_FRONTIER;
+  Workspace& w = v->ws;
+  const uint64_t Q = count;
+  // deterministic workspace bytes for this batch (checked against the budget
+  // before allocating)
+  const U128 need = static_cast<U128>(Q) * (120u + 120u + 32u) + static_cast<U128>(edge_count) * 16u +
+                    static_cast<U128>(Q) * S * 8u + static_cast<U128>(Q) * n * 12u +
+                    static_cast<U128>(Q) * S * 4u +
+                    (workspace_mode ? static_cast<U128>(Q) * S * 16u : 0u) + 16u;
+  if (v->persistent_bytes > req.maximum_device_bytes ||
+      need > static_cast<U128>(req.maximum_device_bytes - v->persistent_bytes)) {
+    return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "batch exceeds the device-memory budget");
+  }
+  APGAR_B200_CUDA("cudaMalloc(queries)", w.queries.ensure(Q));
+  APGAR_B200_CUDA("cudaMalloc(policy)", w.policy.ensure(std::max<uint64_t>(edge_count, 1)));
+  APGAR_B200_CUDA("cudaMalloc(results)", w.results.ensure(Q));
+  APGAR_B200_CUDA("cudaMalloc(compact)", w.compact.ensure(Q));
+  APGAR_B200_CUDA("cudaMalloc(labels)", w.labels.ensure(Q * S));
+  APGAR_B200_CUDA("cudaMalloc(queues)", w.queues.ensure(Q * 2 * n));
+  APGAR_B200_CUDA("cudaMalloc(stamps)", w.stamps.ensure(Q * n));
+  APGAR_B200_CUDA("cudaMalloc(stage)", w.stage.ensure(Q * S));
+  if (workspace_mode) {
+    APGAR_B200_CUDA("cudaMalloc(owners)", w.owners.ensure(Q * S));
+    APGAR_B200_CUDA("cudaMalloc(pred owners)", w.pred_owners.ensure(Q * S));
+  }
+  APGAR_B200_CUDA("cudaMalloc(counters)", w.counters.ensure(2));
+  APGAR_B200_CUDA("cudaMemcpy(queries)",
+                  cudaMemcpy(w.queries.get(), queries, Q * sizeof(*queries), cudaMemcpyHostToDevice));
+  if (edge_count > 0) {
+    APGAR_B200_CUDA("cudaMemcpy(policy)", cudaMemcpy(w.policy.get(), edges, edge_count * sizeof(*edges),
+                                                     cudaMemcpyHostToDevice));
+  }
+  if (v->cancel_host == nullptr) {
+    void* h = nullptr;
+    APGAR_B200_CUDA("cudaHostAlloc(cancel flag)", cudaHostAlloc(&h, sizeof(uint32_t), cudaHostAllocMapped));
+    v->cancel_host = static_cast<uint32_t*>(h);
+    void* d = nullptr;
+    APGAR_B200_CUDA("cudaHostGetDevicePointer(cancel flag)", cudaHostGetDevicePointer(&d, h, 0));
+    v->cancel_dev = static_cast<uint32_t*>(d);
+  }
+  *reinterpret_cast<volatile uint32_t*>(v->cancel_host) = 0u;
+
+  GraphLaunch L{};
+  L.g = v->device_view();
+  L.queries = w.queries.get();
+  L.query_count = count;
+  L.policy = w.policy.get();
+  L.labels = w.labels.get();
+  L.queues = w.queues.get();
+  L.stamps = w.stamps.get();
+  L.results = w.results.get();
+  L.compact = w.compact.get();
+  L.path_stage = w.stage.get();
+  L.predecessors = w.stage.get();
+  L.state_owners = w.owners.get();
+  L.predecessor_owners = w.pred_owners.get();
+  L.maximum_rounds = req.maximum_rounds;
+  L.generator = req.generator;
+  L.workspace_mode = workspace_mode ? 1 : 0;
+  L.cancel = v->cancel_dev;
+
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  APGAR_B200_CUDA("cudaEventCreate", cudaEventCreate(&t0));
+  APGAR_B200_CUDA("cudaEventCreate", cudaEventCreate(&t1));
+  std::unique_ptr<CUevent_st, decltype(&cudaEventDestroy)> g0(t0, cudaEventDestroy);
+  std::unique_ptr<CUevent_st, decltype(&cudaEventDestroy)> g1(t1, cudaEventDestroy);
+  APGAR_B200_CUDA("cudaEventRecord", cudaEventRecord(t0, nullptr));
+  APGAR_B200_CUDA("graph search launch", launch_graph_search(L, nullptr));
+  uint64_t launches = 1;
+  if (!workspace_mode) {
+    // packed states reuse the label slab, dead once every path is staged
+    APGAR_B200_CUDA("graph pack launch",
+                    launch_graph_pack(w.compact.get(), count, S, w.stage.get(),
+                                      reinterpret_cast<uint32_t*>(w.labels.get()),
+                                      w.counters.get(), v->sm_count, nullptr));
+    launches += 2;
+  }
+  APGAR_B200_CUDA("cudaEventRecord", cudaEventRecord(t1, nullptr));
+  // The caller's flag is sampled here and forwarded through the view's
+  // mapped flag, which the kernel polls once per round.
+  for (;;) {
+    const cudaError_t q = cudaEventQuery(t1);
+    if (q == cudaSuccess) break;
+    if (q != cudaErrorNotReady) return cuda_failure("graph search", q);
+    if (cancel != nullptr && *cancel != 0u) *reinterpret_cast<volatile uint32_t*>(v->cancel_host) = 1u;
+    std::this_thread::yield();
+  }
+  float ms = 0.0f;
+  APGAR_B200_CUDA("cudaEventElapsedTime", cudaEventElapsedTime(&ms, t0, t1));
+  pending->view = v;
+  pending->workspace_mode = workspace_mode;
+  pending->query_count = count;
+  pending->states = S;
+  pending->batch_bytes = static_cast<uint64_t>(need);
+  pending->kernel_ms = ms;
+  pending->launches = launches;
+  return APGAR_B200_OK;
+}
+
+void fill_telemetry(const PendingBatch& p, uint64_t readback_bytes, uint32_t max_rounds,
+                    apgar_b200_batch_telemetry* t) {
+  if (t == nullptr) return;
+  std::memset(t, 0, sizeof(*t));
+  t->persistent_device_bytes = p.view->persistent_bytes;
+  t->batch_device_bytes = p.batch_bytes;
+  t->workspace_capacity_device_bytes = std::max<uint64_t>(p.view->ws.bytes(), p.batch_bytes);
+  t->peak_device_bytes = t->persistent_device_bytes + t->workspace_capacity_device_bytes;
+  t->device_to_host_readback_bytes = readback_bytes;
+  t->kernel_launch_count = p.launches;
+  t->blocking_status_readback_count = 0;  // no host round trip during the search
+  t->dispatched_rounds = max_rounds;
+  t->finalization_launch_count = 0;
+  t->kernel_milliseconds = p.kernel_ms;
+}
+
+}  // namespace
+}  // namespace apgar_b200
+
+using namespace apgar_b200;
+
+extern "C" int apgar_b200_view_upload(const apgar_b200_compiled_header_v1* header,
+                                      const apgar_b200_layer_range_v1* layers, uint64_t layer_count,
+                                      const apgar_b200_node_v1* nodes, uint64_t node_count,
+                                      const apgar_b200_run_v1* runs, uint64_t run_count,
+                                      const uint32_t* run_nodes, uint64_t run_node_count,
+                                      void** out_view) {
+  if (header == nullptr || nodes == nullptr || out_view == nullptr ||
+      (run_count > 0 && runs == nullptr) || (run_node_count > 0 && run_nodes == nullptr)) {
+    return invariant("view upload received a null argument");
+  }
+  try {
+    if (int rc = validate_view(*header, layers, layer_count, nodes, node_count, runs, run_count,
+                               run_nodes, run_node_count);
+        rc != APGAR_B200_OK) {
+      return rc;
+    }
+    auto v = std::make_unique<ViewObject>();
+    APGAR_B200_CUDA("cudaGetDevice", cudaGetDevice(&v->device));
+    APGAR_B200_CUDA("cudaDeviceGetAttribute",
+                    cudaDeviceGetAttribute(&v->sm_count, cudaDevAttrMultiProcessorCount, v->device));
+    v->header = *header;
+    v->persistent_bytes = header->estimated_persistent_device_bytes;
+    v->legal.resize(node_count);
+    std::vector<uint32_t> soa(8 * node_count);
+    for (uint64_t i = 0; i < node_count; ++i) {
+      v->legal[i] = nodes[i].legal_edges;
+      for (int d = 0; d < 8; ++d) soa[static_cast<uint64_t>(d) * node_count + i] = nodes[i].neighbors[d];
+    }
+    APGAR_B200_CUDA("cudaMalloc(neighbors)", v->neighbors.ensure(soa.size()));
+    APGAR_B200_CUDA("cudaMemcpy(neighbors)", cudaMemcpy(v->neighbors.get(), soa.data(),
+                                                        soa.size() * 4, cudaMemcpyHostToDevice));
+    APGAR_B200_CUDA("cudaMalloc(legal)", v->legal_dev.ensure(node_count));
+    APGAR_B200_CUDA("cudaMemcpy(legal)", cudaMemcpy(v->legal_dev.get(), v->legal.data(), node_count,
+                                                    cudaMemcpyHostToDevice));
+    *out_view = v.release();
+    clear_error();
+    return APGAR_B200_OK;
+  } catch (const std::bad_alloc&) {
+    return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "host allocation failed during upload");
+  }
+}
+
+extern "C" int apgar_b200_view_release(void* view) {
+  delete static_cast<ViewObject*>(view);
+  return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_execute_batch(void* view, const apgar_b200_batch_request* request,
+                                        const apgar_b200_batch_query_v1* queries,
+                                        uint32_t query_count,
+                                        const apgar_b200_policy_edge_v1* policy_edges,
+                                        uint64_t policy_edge_count, const volatile uint8_t* cancel,
+                                        void** out_pending) {
+  if (view == nullptr || request == nullptr || out_pending == nullptr ||
+      (query_count > 0 && queries == nullptr) || (policy_edge_count > 0 && policy_edges == nullptr)) {
+    return invariant("candidate batch received a null argument");
+  }
+  auto* v = static_cast<ViewObject*>(view);
+  if (int rc = check_device(v->device); rc != APGAR_B200_OK) return rc;
+  try {
+    auto pending = std::make_unique<PendingBatch>();
+    v->lease.acquire();
+    pending->view = v;
+    pending->leased = true;
+    if (int rc = validate_batch(*v, *request, queries, query_count, policy_edges, policy_edge_count);
+        rc != APGAR_B200_OK) {
+      return rc;
+    }
+    if (int rc = run_batch(v, *request, queries, query_count, policy_edges, policy_edge_count, cancel,
+                           pending.get());
+        rc != APGAR_B200_OK) {
+      return rc;
+    }
+    *out_pending = pending.release();
+    clear_error();
+    return APGAR_B200_OK;
+  } catch (const std::bad_alloc&) {
+    return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "host allocation failed during execution");
+  }
+}
+
+extern "C" int apgar_b200_readback_batch(void* pending, apgar_b200_batch_result_v1* results,
+                                         apgar_b200_compact_path_v1* compact_paths,
+                                         uint32_t* path_states, uint64_t path_capacity,
+                                         uint64_t* path_state_count,
+                                         apgar_b200_batch_telemetry* telemetry) {
+  if (pending == nullptr || results == nullptr) return invariant("readback received a null argument");
+  auto* p = static_cast<PendingBatch*>(pending);
+  if (int rc = check_device(p->view->device); rc != APGAR_B200_OK) return rc;
+  Workspace& w = p->view->ws;
+  const uint64_t Q = p->query_count;
+  APGAR_B200_CUDA("cudaMemcpy(results)", cudaMemcpy(results, w.results.get(), Q * sizeof(*results),
+                                                    cudaMemcpyDeviceToHost));
+  uint64_t bytes = Q * sizeof(*results);
+  uint32_t max_rounds = 0;
+  for (uint64_t i = 0; i < Q; ++i) max_rounds = std::max(max_rounds, results[i].rounds);
+  uint64_t total = 0;
+  if (!p->workspace_mode) {
+    unsigned long long t = 0;
+    APGAR_B200_CUDA("cudaMemcpy(path total)", cudaMemcpy(&t, w.counters.get(), sizeof(t), cudaMemcpyDeviceToHost));
+    total = t;
+    if (compact_paths != nullptr) {
+      APGAR_B200_CUDA("cudaMemcpy(compact paths)",
+                      cudaMemcpy(compact_paths, w.compact.get(), Q * sizeof(*compact_paths),
+                                 cudaMemcpyDeviceToHost));
+      bytes += Q * sizeof(*compact_paths);
+    }
+    if (path_states != nullptr && total > 0) {
+      if (total > path_capacity) {
+        return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "compact path buffer is too small");
+      }
+      APGAR_B200_CUDA("cudaMemcpy(path states)",
+                      cudaMemcpy(path_states, w.labels.get(), total * 4, cudaMemcpyDeviceToHost));
+      bytes += total * 4;
+    }
+  }
+  if (path_state_count != nullptr) *path_state_count = total;
+  fill_telemetry(*p, bytes, max_rounds, telemetry);
+  clear_error();
+  return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_readback_batch_workspace(void* pending, uint64_t* labels,
+                                                   uint32_t* predecessors, uint64_t* state_owners,
+                                                   uint64_t* predecessor_owners) {
+  if (pending == nullptr) return invariant("workspace readback received a null pending batch");
+  auto* p = static_cast<PendingBatch*>(pending);
+  if (!p->workspace_mode) {
+    return set_error(APGAR_B200_UNSUPPORTED, "this batch ran in compact-path form");
+  }
+  if (int rc = check_device(p->view->device); rc != APGAR_B200_OK) return rc;
+  Workspace& w = p->view->ws;
+  const uint64_t total = static_cast<uint64_t>(p->query_count) * p->states;
+  if (labels) APGAR_B200_CUDA("cudaMemcpy(labels)", cudaMemcpy(labels, w.labels.get(), total * 8, cudaMemcpyDeviceToHost));
+  if (predecessors) APGAR_B200_CUDA("cudaMemcpy(predecessors)", cudaMemcpy(predecessors, w.stage.get(), total * 4, cudaMemcpyDeviceToHost));
+  if (state_owners) APGAR_B200_CUDA("cudaMemcpy(owners)", cudaMemcpy(state_owners, w.owners.get(), total * 8, cudaMemcpyDeviceToHost));
+  if (predecessor_owners) APGAR_B200_CUDA("cudaMemcpy(pred owners)", cudaMemcpy(predecessor_owners, w.pred_owners.get(), total * 8, cudaMemcpyDeviceToHost));
+  clear_error();
+  return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_release_batch(void* pending) {
+  delete static_cast<PendingBatch*>(pending);
+  return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_execute_route(void* view, uint8_t generator, uint32_t start_node,
+                                        uint32_t goal_node, uint64_t routing_profile_fingerprint,
+                                        uint32_t maximum_rounds, uint64_t maximum_device_bytes,
+                                        const volatile uint8_t* cancel, void** out_pending) {
+  if (view == nullptr || out_pending == nullptr) return invariant("route received a null argument");
+  auto* v = static_cast<ViewObject*>(view);
+  const uint64_t n = v->legal.size();
+  if (start_node >= n || goal_node >= n || maximum_rounds == 0 || start_node == goal_node ||
+      generator > 2) {
+    return invariant("route received invalid endpoint, generator or budget bounds");
+  }
+  if (int rc = check_device(v->device); rc != APGAR_B200_OK) return rc;
+  try {
+    auto route = std::make_unique<PendingRoute>();
+    route->batch = std::make_unique<PendingBatch>();
+    v->lease.acquire();
+    route->batch->view = v;
+    route->batch->leased = true;
+    apgar_b200_batch_request req{};
+    req.schema_version = 1;
+    req.generator = APGAR_B200_GENERATOR_BUCKETED_FRONTIER;  // full labels + predecessors
+    req.batch_id = 1;
+    req.maximum_rounds = maximum_rounds;
+    req.maximum_workspace_states_per_query = ~0ull;
+    req.maximum_frontier_states_per_query = ~0ull;
+    req.maximum_device_bytes = maximum_device_bytes;
+    req.maximum_host_bytes = ~0ull;
+    apgar_b200_batch_query_v1 q{};
+    q.schema_version = 1;
+    q.batch_id = 1;
+    q.query_id = 1;
+    q.workspace_owner = 1;
+    q.routing_profile_fingerprint = routing_profile_fingerprint;
+    q.start_node = start_node;
+    q.goal_node = goal_node;
+    q.workspace_state_count = 9ull * n;
+    q.frontier_state_capacity = 9ull * n;
+    q.maximum_rounds = maximum_rounds;
+    q.generator = APGAR_B200_GENERATOR_BUCKETED_FRONTIER;
+    if (int rc = run_batch(v, req, &q, 1, nullptr, 0, cancel, route->batch.get()); rc != APGAR_B200_OK) {
+      return rc;
+    }
+    apgar_b200_route_result_header_v1& h = route->header;
+    h.schema_version = 1;
+    h.compiler_version = v->header.compiler_version;
+    h.start_node = start_node;
+    h.goal_node = goal_node;
+    h.source_board_content_hash = v->header.source_board_content_hash;
+    h.compiler_profile_fingerprint = v->header.compiler_profile_fingerprint;
+    h.routing_profile_fingerprint = routing_profile_fingerprint;
+    h.rule_bucket_identity = v->header.rule_bucket_identity;
+    h.device_view_fingerprint = v->header.device_view_fingerprint;
+    h.generator = generator;
+    *out_pending = route.release();
+    clear_error();
+    return APGAR_B200_OK;
+  } catch (const std::bad_alloc&) {
+    return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "host allocation failed during route execution");
+  }
+}
+
+extern "C" int apgar_b200_readback_route(void* pending, apgar_b200_route_result_header_v1* header,
+                                         uint8_t* completion, uint32_t* goal_state,
+                                         uint64_t* labels, uint32_t* predecessors,
+                                         apgar_b200_batch_telemetry* telemetry) {
+  if (pending == nullptr) return invariant("route readback received a null argument");
+  auto* r = static_cast<PendingRoute*>(pending);
+  apgar_b200_batch_result_v1 res{};
+  if (int rc = apgar_b200_readback_batch(r->batch.get(), &res, nullptr, nullptr, 0, nullptr, telemetry);
+      rc != APGAR_B200_OK) {
+    return rc;
+  }
+  if (int rc = apgar_b200_readback_batch_workspace(r->batch.get(), labels, predecessors, nullptr, nullptr);
+      rc != APGAR_B200_OK) {
+    return rc;
+  }
+  if (header != nullptr) *header = r->header;
+  if (completion != nullptr) *completion = res.completion;
+  if (goal_state != nullptr) *goal_state = res.goal_state;
+  if (telemetry != nullptr) {
+    telemetry->device_to_host_readback_bytes =
+        sizeof(apgar_b200_route_result_header_v1) + r->batch->states * 12u;
+  }
+  clear_error();
+  return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_release_route(void* pending) {
+  delete static_cast<PendingRoute*>(pending);
+  return APGAR_B200_OK;
+}

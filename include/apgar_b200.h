@@ -83,6 +83,191 @@ typedef struct apgar_b200_metadata {
 
 APGAR_B200_API int apgar_b200_query_metadata(apgar_b200_metadata* out);
 
+/* =================== A. drop-in seam (reference V1 records) =================== */
+
+/* Generator values of PlanarGenerator (planar_router.h:42-45) plus the value
+ * this backend adds for its own persistent engine; the descriptor of the new
+ * value is described in INTEGRATION.md. */
+enum {
+  APGAR_B200_GENERATOR_BUCKETED_FRONTIER = 0, /* PlanarGenerator::kBucketedFrontier */
+  APGAR_B200_GENERATOR_HEADING_SWEEP = 1,     /* PlanarGenerator::kHeadingAwareSweep */
+  APGAR_B200_GENERATOR_B200_PERSISTENT = 2    /* added: one fused launch per batch */
+};
+
+/* DeviceCompiledHeaderV1 (planar_router.h:170-188), 112 bytes. */
+typedef struct apgar_b200_compiled_header_v1 {
+  uint32_t schema_version;
+  uint32_t compiler_version;
+  uint64_t source_board_content_hash;
+  uint64_t compiler_profile_fingerprint;
+  uint64_t rule_bucket_identity;
+  uint64_t device_view_fingerprint;
+  uint64_t represented_nodes;
+  uint64_t represented_states;
+  uint64_t estimated_persistent_device_bytes;
+  int64_t lattice_origin_x, lattice_origin_y;
+  int64_t lattice_step;
+  uint32_t orthogonal_step, diagonal_step, bend; /* DeterministicCosts */
+  uint8_t heading_mask;
+  uint8_t reserved[7];
+  uint8_t padding[4];
+} apgar_b200_compiled_header_v1;
+
+/* DeviceLayerRangeV1 (planar_router.h:190-201), 48 bytes. */
+typedef struct apgar_b200_layer_range_v1 {
+  uint32_t layer, node_offset, node_count, padding;
+  int64_t minimum_lattice_x, maximum_lattice_x, minimum_lattice_y, maximum_lattice_y;
+} apgar_b200_layer_range_v1;
+
+/* DeviceNodeV1 (planar_router.h:203-213), 56 bytes. */
+typedef struct apgar_b200_node_v1 {
+  int64_t lattice_x, lattice_y;
+  uint32_t layer;
+  uint8_t legal_edges;
+  uint8_t reserved[3];
+  uint32_t neighbors[8];
+} apgar_b200_node_v1;
+
+/* DeviceRunV1 (planar_router.h:215-223), 12 bytes. */
+typedef struct apgar_b200_run_v1 {
+  uint32_t node_offset, node_count;
+  uint8_t direction;
+  uint8_t reserved[3];
+} apgar_b200_run_v1;
+
+/* DeviceCandidatePolicyEdgeV1 (planar_router.h:340-348), 16 bytes. */
+typedef struct apgar_b200_policy_edge_v1 {
+  uint32_t physical_edge_index;
+  uint32_t reserved;
+  uint64_t adjustment; /* UINT64_MAX = banned */
+} apgar_b200_policy_edge_v1;
+
+/* DeviceCandidateBatchQueryV1 (planar_router.h:352-377), 120 bytes. */
+typedef struct apgar_b200_batch_query_v1 {
+  uint32_t schema_version, input_ordinal;
+  uint64_t batch_id, query_id, workspace_owner, policy_identity, routing_profile_fingerprint;
+  uint32_t start_node, goal_node, policy_offset, policy_count;
+  uint64_t workspace_offset, workspace_state_count, frontier_state_capacity;
+  uint64_t orthogonal_step_surcharge, diagonal_step_surcharge, bend_surcharge;
+  uint32_t maximum_rounds;
+  uint8_t generator;
+  uint8_t reserved[3];
+} apgar_b200_batch_query_v1;
+
+/* DeviceCandidateBatchResultV1 (planar_router.h:381-407), 120 bytes. */
+typedef struct apgar_b200_batch_result_v1 {
+  uint32_t schema_version, compiler_version, input_ordinal, start_node, goal_node, goal_state, rounds;
+  uint8_t generator, completion; /* completion: APGAR_B200_COMPLETION_* (0..3) */
+  uint8_t reserved[2];
+  uint64_t batch_id, query_id, workspace_owner, policy_identity, routing_profile_fingerprint;
+  uint64_t source_board_content_hash, compiler_profile_fingerprint, rule_bucket_identity;
+  uint64_t device_view_fingerprint, examined_work, heading_turn_relaxations;
+} apgar_b200_batch_result_v1;
+
+/* DeviceCandidateCompactPathV1 (planar_router.h:413-423), 32 bytes. */
+typedef struct apgar_b200_compact_path_v1 {
+  uint32_t schema_version, state_count;
+  uint64_t query_id, workspace_owner, state_offset;
+} apgar_b200_compact_path_v1;
+
+/* DeviceRouteResultHeaderV1 (planar_router.h:225-241), 64 bytes. */
+typedef struct apgar_b200_route_result_header_v1 {
+  uint32_t schema_version, compiler_version, start_node, goal_node;
+  uint64_t source_board_content_hash, compiler_profile_fingerprint, routing_profile_fingerprint;
+  uint64_t rule_bucket_identity, device_view_fingerprint;
+  uint8_t generator;
+  uint8_t reserved[7];
+} apgar_b200_route_result_header_v1;
+
+/* The non-vector fields of BackendCandidateBatchExecutionRequest
+ * (planar_router.h:425-437). */
+typedef struct apgar_b200_batch_request {
+  uint32_t schema_version;
+  uint8_t generator;
+  uint8_t reserved[3];
+  uint64_t batch_id;
+  uint32_t maximum_rounds;
+  uint32_t padding;
+  uint64_t maximum_workspace_states_per_query;
+  uint64_t maximum_frontier_states_per_query;
+  uint64_t maximum_device_bytes;
+  uint64_t maximum_host_bytes;
+} apgar_b200_batch_request;
+
+/* CandidateBatchTelemetry (planar_router.h:127-147) as produced by this
+ * backend: launches and readbacks are this engine's own counts. */
+typedef struct apgar_b200_batch_telemetry {
+  uint64_t persistent_device_bytes;
+  uint64_t batch_device_bytes;
+  uint64_t workspace_capacity_device_bytes;
+  uint64_t peak_device_bytes;
+  uint64_t device_to_host_readback_bytes;
+  uint64_t kernel_launch_count;
+  uint64_t blocking_status_readback_count;
+  uint32_t dispatched_rounds;
+  uint32_t finalization_launch_count;
+  double kernel_milliseconds;
+} apgar_b200_batch_telemetry;
+
+/* UploadCompiledView (planar_router.h:548; gpu/cuda/planar_router.cu:1951-2003):
+ * validates the flattened view (the checks of planar_router.cu:1256-1451 that
+ * guard device memory safety and the cost bound) and uploads it to the
+ * current device. */
+APGAR_B200_API int apgar_b200_view_upload(const apgar_b200_compiled_header_v1* header,
+                                          const apgar_b200_layer_range_v1* layers,
+                                          uint64_t layer_count,
+                                          const apgar_b200_node_v1* nodes, uint64_t node_count,
+                                          const apgar_b200_run_v1* runs, uint64_t run_count,
+                                          const uint32_t* run_nodes, uint64_t run_node_count,
+                                          void** out_view);
+APGAR_B200_API int apgar_b200_view_release(void* view);
+
+/* ExecuteCandidateBatch (planar_router.h:556-557; planar_router.cu:2183-2625):
+ * validates the batch (ordering, ownership, workspace and policy bounds, the
+ * cost-sentinel bound of planar_router.cu:1731-1909), then searches every
+ * query on the device.  `cancel` (optional, host memory) is sampled on the
+ * host while the batch runs. */
+APGAR_B200_API int apgar_b200_execute_batch(void* view, const apgar_b200_batch_request* request,
+                                            const apgar_b200_batch_query_v1* queries,
+                                            uint32_t query_count,
+                                            const apgar_b200_policy_edge_v1* policy_edges,
+                                            uint64_t policy_edge_count,
+                                            const volatile uint8_t* cancel, void** out_pending);
+
+/* ReadbackCandidateBatch (planar_router.h:558-559; planar_router.cu:2627-2792),
+ * compact form: result headers, compact path headers and the packed reverse
+ * state paths (state = node*9 + incoming heading, goal first). */
+APGAR_B200_API int apgar_b200_readback_batch(void* pending, apgar_b200_batch_result_v1* results,
+                                             apgar_b200_compact_path_v1* compact_paths,
+                                             uint32_t* path_states, uint64_t path_capacity,
+                                             uint64_t* path_state_count,
+                                             apgar_b200_batch_telemetry* telemetry);
+
+/* Full-workspace form (the frontier generator's readback): query-major labels
+ * (uint64, UINT64_MAX unreachable), canonical predecessors (UINT32_MAX none)
+ * and the owner stamps of every state.  Arrays hold query_count * 9 * nodes. */
+APGAR_B200_API int apgar_b200_readback_batch_workspace(void* pending, uint64_t* labels,
+                                                       uint32_t* predecessors,
+                                                       uint64_t* state_owners,
+                                                       uint64_t* predecessor_owners);
+APGAR_B200_API int apgar_b200_release_batch(void* pending);
+
+/* ExecuteRoute / ReadbackRoute (planar_router.h:549-551; planar_router.cu:2049-2181,
+ * :2794-2853): one query without a policy; readback returns the result header,
+ * completion, goal state and the full label / predecessor arrays (9 * nodes). */
+APGAR_B200_API int apgar_b200_execute_route(void* view, uint8_t generator, uint32_t start_node,
+                                            uint32_t goal_node,
+                                            uint64_t routing_profile_fingerprint,
+                                            uint32_t maximum_rounds,
+                                            uint64_t maximum_device_bytes,
+                                            const volatile uint8_t* cancel, void** out_pending);
+APGAR_B200_API int apgar_b200_readback_route(void* pending,
+                                             apgar_b200_route_result_header_v1* header,
+                                             uint8_t* completion, uint32_t* goal_state,
+                                             uint64_t* labels, uint32_t* predecessors,
+                                             apgar_b200_batch_telemetry* telemetry);
+APGAR_B200_API int apgar_b200_release_route(void* pending);
+
 /* ======================= B. lattice mode ======================= */
 
 typedef struct apgar_b200_lattice_desc {

@@ -193,3 +193,44 @@ def sweep_one(lat, net_row, max_sweeps=100000):
     cost = L.lo_sweep_schedule(ctypes.byref(ref.c), _net_ptr(net), ctypes.c_uint32(max_sweeps),
                                _ptr(dist), ctypes.byref(st))
     return cost, dist, st
+
+
+def graph_search(nodes, costs, start, goal, orth_s=0, diag_s=0, bend_s=0, policy=None,
+                 want_labels=False, path_cap=None):
+    """Exact heading-state search over DeviceCompiledBoardV1 node records.
+
+    Returns (reached, goal_cost, goal_state, reverse compact path, labels)."""
+    L = lib()
+    nodes = np.ascontiguousarray(nodes)
+    n = len(nodes)
+    labels = np.empty(9 * n, dtype=np.uint64) if want_labels else None
+    cap = path_cap or 9 * n
+    path = np.empty(cap, dtype=np.uint32)
+    pol = np.ascontiguousarray(policy) if policy is not None and len(policy) else None
+    q = GoQuery(start, goal, orth_s, diag_s, bend_s,
+                pol.ctypes.data_as(ctypes.c_void_p) if pol is not None else None,
+                len(pol) if pol is not None else 0)
+    gc = ctypes.c_uint64(0)
+    gs = ctypes.c_uint32(0)
+    plen = ctypes.c_uint32(0)
+    reached = L.go_search(nodes.ctypes.data_as(ctypes.c_void_p), ctypes.c_uint32(n),
+                          GoCosts(*costs), ctypes.byref(q),
+                          labels.ctypes.data_as(U64P) if labels is not None else U64P(),
+                          ctypes.byref(gc), ctypes.byref(gs), _ptr(path), ctypes.c_uint32(cap),
+                          ctypes.byref(plen))
+    return bool(reached), gc.value, gs.value, path[: plen.value].copy(), labels
+
+
+def graph_predecessors(nodes, costs, start, labels, orth_s=0, diag_s=0, bend_s=0, policy=None):
+    """Canonical predecessor of every state from exact labels."""
+    L = lib()
+    nodes = np.ascontiguousarray(nodes)
+    labels = np.ascontiguousarray(labels, dtype=np.uint64)
+    pol = np.ascontiguousarray(policy) if policy is not None and len(policy) else None
+    q = GoQuery(start, 0, orth_s, diag_s, bend_s,
+                pol.ctypes.data_as(ctypes.c_void_p) if pol is not None else None,
+                len(pol) if pol is not None else 0)
+    preds = np.empty(len(labels), dtype=np.uint32)
+    L.go_predecessors(nodes.ctypes.data_as(ctypes.c_void_p), ctypes.c_uint32(len(nodes)),
+                      GoCosts(*costs), ctypes.byref(q), labels.ctypes.data_as(U64P), _ptr(preds))
+    return preds

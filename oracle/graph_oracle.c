@@ -188,3 +188,29 @@ int go_search(const go_node* nodes, uint32_t node_count, go_costs costs, const g
   if (!labels_out) free(labels);
   return reached;
 }
+
+/* Canonical predecessor of every state from exact labels (the reference's
+ * SelectCandidateBatchPredecessors rule, planar_router.cu:1021-1079): the
+ * smallest predecessor state whose label plus the move cost equals the
+ * state's label; UINT32_MAX for the start state, unreachable states and
+ * heading-8 states. */
+void go_predecessors(const go_node* nodes, uint32_t node_count, go_costs costs, const go_query* q,
+                     const uint64_t* labels, uint32_t* preds) {
+  const uint32_t states = node_count * 9u;
+  for (uint32_t s = 0; s < states; ++s) {
+    preds[s] = GO_INVALID;
+    const uint32_t node = s / 9u, h = s % 9u;
+    if (h == 8u || labels[s] == GO_INF) continue;
+    const uint32_t pred = nodes[node].neighbors[(h + 4u) % 8u];
+    if (pred == GO_INVALID) continue;
+    for (uint32_t ph = 0; ph < 9u; ++ph) {
+      if (ph == 8u && pred != q->start_node) continue;
+      uint64_t t, c;
+      if (!transition(nodes, costs, q, pred, h, ph, &t)) continue;
+      if (checked_add(labels[pred * 9u + ph], t, &c) && c == labels[s]) {
+        preds[s] = pred * 9u + ph;
+        break;
+      }
+    }
+  }
+}

@@ -128,6 +128,10 @@ int go_search(const go_node* nodes, uint32_t node_count, go_costs costs, const g
               uint64_t* labels, uint64_t* goal_cost, uint32_t* goal_state, uint32_t* path,
               uint32_t path_cap, uint32_t* path_len);
 
+/* Canonical predecessor of every state from exact labels. */
+void go_predecessors(const go_node* nodes, uint32_t node_count, go_costs costs,
+                     const go_query* query, const uint64_t* labels, uint32_t* preds);
+
 /* ---------------- congestion prices (integer, checked) ---------------- */
 
 /* Allocator epoch update (negotiated_regeneration_plan.cc:676-760):

@@ -1,0 +1,120 @@
+"""Reader for tests/golden/ref_corpus/*.bin (written by oracle/ref_fixtures.cc).
+
+Layout (little endian): u64 magic "AGRFTIX1"; DeviceCompiledHeaderV1 (112 B);
+then u64-counted arrays of DeviceLayerRangeV1 (48 B), DeviceNodeV1 (56 B),
+DeviceRunV1 (12 B) and run-node u32; then u64 query count and per query:
+u32 start node, u32 goal node, u64 orthogonal / diagonal / bend surcharges,
+u64 policy identity, u32 CPU status (0 reached, 1 disconnected, 2 failed),
+u32 pad, u64 CPU A* cost, u64-counted DeviceCandidatePolicyEdgeV1 (16 B).
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import glob
+import json
+import os
+
+import numpy as np
+
+HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_corpus")
+
+HEADER_DTYPE = np.dtype([
+    ("schema_version", "<u4"), ("compiler_version", "<u4"),
+    ("source_board_content_hash", "<u8"), ("compiler_profile_fingerprint", "<u8"),
+    ("rule_bucket_identity", "<u8"), ("device_view_fingerprint", "<u8"),
+    ("represented_nodes", "<u8"), ("represented_states", "<u8"),
+    ("estimated_persistent_device_bytes", "<u8"),
+    ("lattice_origin_x", "<i8"), ("lattice_origin_y", "<i8"), ("lattice_step", "<i8"),
+    ("orthogonal_step", "<u4"), ("diagonal_step", "<u4"), ("bend", "<u4"),
+    ("heading_mask", "u1"), ("reserved", "u1", (7,)), ("padding", "u1", (4,)),
+])
+LAYER_DTYPE = np.dtype([("layer", "<u4"), ("node_offset", "<u4"), ("node_count", "<u4"),
+                        ("padding", "<u4"), ("minimum_lattice_x", "<i8"), ("maximum_lattice_x", "<i8"),
+                        ("minimum_lattice_y", "<i8"), ("maximum_lattice_y", "<i8")])
+NODE_DTYPE = np.dtype([("lattice_x", "<i8"), ("lattice_y", "<i8"), ("layer", "<u4"),
+                       ("legal_edges", "u1"), ("reserved", "u1", (3,)), ("neighbors", "<u4", (8,))])
+RUN_DTYPE = np.dtype([("node_offset", "<u4"), ("node_count", "<u4"), ("direction", "u1"),
+                      ("reserved", "u1", (3,))])
+POLICY_EDGE_DTYPE = np.dtype([("physical_edge_index", "<u4"), ("reserved", "<u4"), ("adjustment", "<u8")])
+assert HEADER_DTYPE.itemsize == 112 and LAYER_DTYPE.itemsize == 48
+assert NODE_DTYPE.itemsize == 56 and RUN_DTYPE.itemsize == 12 and POLICY_EDGE_DTYPE.itemsize == 16
+
+
+@dataclasses.dataclass
+class Query:
+    start_node: int
+    goal_node: int
+    orthogonal_surcharge: int
+    diagonal_surcharge: int
+    bend_surcharge: int
+    policy_identity: int
+    cpu_status: int
+    cpu_cost: int
+    policy: np.ndarray
+
+
+@dataclasses.dataclass
+class Case:
+    name: str
+    header: np.ndarray
+    layers: np.ndarray
+    nodes: np.ndarray
+    runs: np.ndarray
+    run_nodes: np.ndarray
+    queries: list
+
+    @property
+    def costs(self):
+        h = self.header[0]
+        return int(h["orthogonal_step"]), int(h["diagonal_step"]), int(h["bend"])
+
+
+class _Reader:
+    def __init__(self, data: bytes):
+        self.data = data
+        self.pos = 0
+
+    def take(self, n: int) -> bytes:
+        b = self.data[self.pos:self.pos + n]
+        self.pos += n
+        return b
+
+    def u32(self) -> int:
+        return int(np.frombuffer(self.take(4), "<u4")[0])
+
+    def u64(self) -> int:
+        return int(np.frombuffer(self.take(8), "<u8")[0])
+
+    def array(self, dtype) -> np.ndarray:
+        n = self.u64()
+        return np.frombuffer(self.take(n * np.dtype(dtype).itemsize), dtype).copy()
+
+
+def load_case(path: str) -> Case:
+    r = _Reader(open(path, "rb").read())
+    assert r.u64() == 0x3158495446524741, "bad fixture magic"
+    header = np.frombuffer(r.take(112), HEADER_DTYPE).copy()
+    layers = r.array(LAYER_DTYPE)
+    nodes = r.array(NODE_DTYPE)
+    runs = r.array(RUN_DTYPE)
+    run_nodes = r.array("<u4")
+    queries = []
+    for _ in range(r.u64()):
+        s, g = r.u32(), r.u32()
+        o, d, b, ident = r.u64(), r.u64(), r.u64(), r.u64()
+        status = r.u32()
+        r.u32()
+        cost = r.u64()
+        policy = r.array(POLICY_EDGE_DTYPE)
+        queries.append(Query(s, g, o, d, b, ident, status, cost, policy))
+    return Case(os.path.basename(path)[:-4], header, layers, nodes, runs, run_nodes, queries)
+
+
+def load_all() -> list:
+    return [load_case(p) for p in sorted(glob.glob(os.path.join(HERE, "*.bin")))]
+
+
+def manifest() -> dict:
+    with open(os.path.join(HERE, "manifest.json")) as f:
+        return json.load(f)

@@ -52,3 +52,20 @@ def test_python_mirror_never_imports_the_oracle():
     for path in glob.glob(os.path.join(ROOT, "apgar_b200", "**", "*.py"), recursive=True):
         text = open(path).read()
         assert "import oracle" not in text and "from oracle" not in text, path
+
+
+def test_view_upload_rejects_corrupt_views_without_gpu():
+    """Upload validation runs on the host before any device call."""
+    from apgar_b200 import dropin
+    from tests.golden import ref_corpus
+
+    case = ref_corpus.load_case(ref_corpus.HERE + "/dense_corridors.bin")
+    nodes = case.nodes.copy()
+    nodes["neighbors"][0][0], nodes["neighbors"][0][1] = nodes["neighbors"][0][1], nodes["neighbors"][0][0]
+    nodes["legal_edges"][0] |= 0x3
+    try:
+        dropin.View(case.header, case.layers, nodes, case.runs, case.run_nodes)
+    except apgar_b200.BackendError as e:
+        assert e.code == 4 and "upload rejected" in e.detail
+    else:
+        raise AssertionError("corrupt view accepted")

@@ -1,0 +1,74 @@
+"""CPU pin of the graph-mode oracle: on every query of the reference's own
+corpus, the oracle's exact heading-state search reproduces the reference CPU
+A* outcome (cost, or disconnected) bit for bit, and its canonical compact
+path is a legal, cost-consistent reverse path."""
+
+import numpy as np
+import pytest
+
+import oracle
+from tests.golden import ref_corpus
+
+CASES = ref_corpus.load_all()
+U64_MAX = (1 << 64) - 1
+
+
+def test_fixture_set_is_complete():
+    names = {c.name for c in CASES}
+    assert {"dense_corridors", "sparse_regions", "fragmented_runs", "high_turn_maze",
+            "cross_tile_edges", "negative_coordinates", "disconnected_fields",
+            "kicad_fixture"} <= names
+    # the reference's published Phase-2 costs (base policy, forward request)
+    published = {"dense_corridors": 140, "sparse_regions": 149, "fragmented_runs": 454,
+                 "high_turn_maze": 1148, "cross_tile_edges": 50, "negative_coordinates": 370,
+                 "kicad_fixture": 37168}
+    for c in CASES:
+        if c.name in published:
+            assert c.queries[0].cpu_status == 0 and c.queries[0].cpu_cost == published[c.name]
+        if c.name == "disconnected_fields":
+            assert c.queries[0].cpu_status == 1
+
+
+def _transition(nodes, costs, q, src, d, h_in):
+    """Reference DeviceBatchTransitionCost (planar_router.cu:557-583) in Python."""
+    orth, diag, bend = costs
+    if d < 4:
+        edge = src * 8 + d
+    else:
+        canon = int(nodes["neighbors"][src][d])
+        edge = canon * 8 + d - 4
+    adj = 0
+    idx = np.searchsorted(q.policy["physical_edge_index"], edge) if len(q.policy) else 0
+    if len(q.policy) and idx < len(q.policy) and q.policy["physical_edge_index"][idx] == edge:
+        adj = int(q.policy["adjustment"][idx])
+    if adj == U64_MAX:
+        return None
+    v = (diag + q.diagonal_surcharge) if d & 1 else (orth + q.orthogonal_surcharge)
+    if h_in != 8 and h_in != d:
+        v += bend + q.bend_surcharge
+    v += adj
+    return v if v < U64_MAX else None
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c.name for c in CASES])
+def test_graph_oracle_matches_reference_cpu_astar(case):
+    costs = case.costs
+    for qi, q in enumerate(case.queries):
+        reached, cost, goal_state, path, _ = oracle.graph_search(
+            case.nodes, costs, q.start_node, q.goal_node, q.orthogonal_surcharge,
+            q.diagonal_surcharge, q.bend_surcharge, q.policy)
+        if q.cpu_status == 0:
+            assert reached and cost == q.cpu_cost, (qi, cost, q.cpu_cost)
+            # reverse path: goal state first, start state (heading 8) last
+            assert path[0] == goal_state and path[-1] == q.start_node * 9 + 8
+            total = 0
+            for a, b in zip(path[::-1][:-1], path[::-1][1:]):
+                node_a, h_a = divmod(int(a), 9)
+                node_b, h_b = divmod(int(b), 9)
+                assert int(case.nodes["neighbors"][node_a][h_b]) == node_b
+                t = _transition(case.nodes, costs, q, node_a, h_b, h_a)
+                assert t is not None
+                total += t
+            assert total == cost
+        elif q.cpu_status == 1:
+            assert not reached, qi
