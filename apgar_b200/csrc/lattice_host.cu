@@ -22,6 +22,9 @@ int lattice_cells_per_lane(int layers);
 size_t lattice_sweep_smem_bytes(int layers, int warps_per_net, int max_rows);
 cudaError_t launch_lattice_sweep(int layers, int warps_per_net, const SweepLaunch& launch,
                                  int max_rows, cudaStream_t stream);
+cudaError_t launch_accumulate_cells(const apgar_b200_lattice_result* results, uint32_t count,
+                                    const uint32_t* paths, uint32_t* usage, uint64_t cell_count,
+                                    int sm_count, cudaStream_t stream);
 cudaError_t launch_lattice_pack(apgar_b200_lattice_result* results, uint32_t count,
                                 unsigned long long* total, const uint32_t* arena, uint32_t* paths,
                                 int sm_count, cudaStream_t stream);
@@ -550,4 +553,18 @@ extern "C" int apgar_b200_lattice_route(void* lattice, const apgar_b200_lattice_
   } catch (const std::bad_alloc&) {
     return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "host allocation failed during routing");
   }
+}
+
+extern "C" int apgar_b200_lattice_accumulate_usage(void* plan, uint32_t* usage, uint64_t cell_count,
+                                                   void* stream) {
+  if (plan == nullptr || usage == nullptr) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "usage accumulation received a null argument");
+  }
+  auto* p = static_cast<PlanObject*>(plan);
+  if (int rc = check_device(p->device); rc != APGAR_B200_OK) return rc;
+  APGAR_B200_CUDA("usage accumulation launch",
+                  launch_accumulate_cells(p->results.get(), p->count, p->paths.get(), usage,
+                                          cell_count, p->sm_count, static_cast<cudaStream_t>(stream)));
+  clear_error();
+  return APGAR_B200_OK;
 }

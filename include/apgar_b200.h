@@ -334,6 +334,52 @@ typedef struct apgar_b200_plan_info {
 APGAR_B200_API int apgar_b200_lattice_plan_info(void* plan, apgar_b200_plan_info* out);
 APGAR_B200_API int apgar_b200_lattice_plan_release(void* plan);
 
+/* ======================= C. congestion prices ======================= */
+
+/* Integer negotiated-congestion price schedule.  Combines the allocator epoch
+ * update (NegotiatedPriceUpdatePolicyV1 and the per-resource update of
+ * src/allocator/negotiated_regeneration_plan.cc:430-442, :676-760) with the
+ * CS-RR-v1 history update and next-pass query snapshot cost
+ * (src/allocator/cpu_sequential_negotiated_routing.cc:299-505, :1300-1330);
+ * overuse = max(0, usage - capacity) as in resource_accounting.cc:212-213. */
+typedef struct apgar_b200_price_policy {
+  uint64_t initial_present_factor;     /* 100 in the reference default */
+  uint64_t present_factor_increment;   /* 100 */
+  uint64_t historical_price_increment; /* 10 */
+  uint64_t capacity;                   /* capacity units per resource */
+  uint64_t maximum_value;              /* bound on histories and snapshot costs */
+} apgar_b200_price_policy;
+
+/* status bits written by the price update */
+enum { APGAR_B200_PRICE_OVERFLOW = 1u, APGAR_B200_PRICE_BOUND = 2u };
+
+/* One fused pass over `count` resources with usage counts `usage`, for price
+ * epoch `epoch` (factor = initial + epoch * increment):
+ *   overuse > 0:  present = factor * overuse, history += increment * overuse,
+ *   otherwise:    present = 0, history unchanged;
+ *   total = present + history;
+ *   next_cost (optional) = history + factor(epoch + 1) * max(0, usage + 1 - capacity),
+ * the CS-RR snapshot cost a query pays in the next pass.  All arithmetic is
+ * checked uint64; *status receives APGAR_B200_PRICE_* bits (0 = clean).
+ * Device pointers, stream-ordered; `status` is a device word. */
+APGAR_B200_API int apgar_b200_price_update_device(uint32_t count, const uint32_t* usage,
+                                                  const apgar_b200_price_policy* policy,
+                                                  uint64_t epoch, uint64_t* present,
+                                                  uint64_t* history, uint64_t* total,
+                                                  uint64_t* next_cost, uint32_t* status,
+                                                  void* stream);
+/* Same on host arrays (copies in, runs on the current device, copies out). */
+APGAR_B200_API int apgar_b200_price_update(uint32_t count, const uint32_t* usage,
+                                           const apgar_b200_price_policy* policy, uint64_t epoch,
+                                           uint64_t* present, uint64_t* history, uint64_t* total,
+                                           uint64_t* next_cost, uint32_t* status);
+
+/* Adds one usage unit per path cell of a lattice plan's packed paths
+ * (cell resources, usage indexed by global cell id; `cell_count` bounds the
+ * array).  Device pointer, stream-ordered. */
+APGAR_B200_API int apgar_b200_lattice_accumulate_usage(void* plan, uint32_t* usage,
+                                                       uint64_t cell_count, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -234,3 +234,43 @@ def graph_predecessors(nodes, costs, start, labels, orth_s=0, diag_s=0, bend_s=0
     L.go_predecessors(nodes.ctypes.data_as(ctypes.c_void_p), ctypes.c_uint32(len(nodes)),
                       GoCosts(*costs), ctypes.byref(q), labels.ctypes.data_as(U64P), _ptr(preds))
     return preds
+
+
+def price_epoch_update(usage, history, capacity, epoch, init=100, inc=100, hinc=10):
+    """Allocator epoch prices (checked). Returns (rc, present, history', total)."""
+    L = lib()
+    usage = np.ascontiguousarray(usage, dtype=np.uint64)
+    hist = np.ascontiguousarray(history, dtype=np.uint64).copy()
+    n = len(usage)
+    present = np.zeros(n, np.uint64)
+    total = np.zeros(n, np.uint64)
+    rc = L.po_epoch_update(ctypes.c_uint32(n), usage.ctypes.data_as(U64P), ctypes.c_uint64(capacity),
+                           ctypes.c_uint64(epoch), ctypes.c_uint64(init), ctypes.c_uint64(inc),
+                           ctypes.c_uint64(hinc), present.ctypes.data_as(U64P),
+                           hist.ctypes.data_as(U64P), total.ctypes.data_as(U64P))
+    return rc, present, hist, total
+
+
+def price_snapshot(usage, history, capacity, pass_index, init, inc, max_value):
+    """CS-RR-v1 snapshot costs. Returns (rc, costs)."""
+    L = lib()
+    usage = np.ascontiguousarray(usage, dtype=np.uint64)
+    hist = np.ascontiguousarray(history, dtype=np.uint64)
+    cost = np.zeros(len(usage), np.uint64)
+    rc = L.po_snapshot_costs(ctypes.c_uint32(len(usage)), usage.ctypes.data_as(U64P),
+                             hist.ctypes.data_as(U64P), ctypes.c_uint64(capacity),
+                             ctypes.c_uint32(pass_index), ctypes.c_uint64(init),
+                             ctypes.c_uint64(inc), ctypes.c_uint64(max_value),
+                             cost.ctypes.data_as(U64P))
+    return rc, cost
+
+
+def accumulate_cells(offsets, lengths, cells, cell_count):
+    L = lib()
+    offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+    lengths = np.ascontiguousarray(lengths, dtype=np.uint32)
+    cells = np.ascontiguousarray(cells, dtype=np.uint32)
+    usage = np.zeros(cell_count, np.uint32)
+    L.po_accumulate_cells(ctypes.c_uint32(len(lengths)), offsets.ctypes.data_as(U64P), _ptr(lengths),
+                          _ptr(cells), ctypes.c_uint32(cell_count), _ptr(usage))
+    return usage
