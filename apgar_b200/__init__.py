@@ -33,6 +33,8 @@ COMPLETION_BUDGET_EXHAUSTED = 2
 COMPLETION_CANCELLED = 3
 COMPLETION_REJECTED = 4
 UNREACHABLE = 0xFFFFFFFF
+NOALLOC_SCRATCH_BYTES = 32 * 1024 * 1024  # APGAR_B200_NOALLOC_SCRATCH_BYTES
+NOALLOC_MAX_NETS = 4096  # APGAR_B200_NOALLOC_MAX_NETS
 
 
 class BackendError(RuntimeError):
@@ -181,6 +183,30 @@ class DeviceLattice:
             _vp(cancel), _vp(results), _vp(paths) if want_paths else None,
             ctypes.c_uint64(paths.size if want_paths else 0), ctypes.byref(total)))
         return results, (paths[: total.value] if want_paths else None)
+
+    def route_noalloc(self, nets: np.ndarray, max_sweeps: int = 4096, stream: int = 0,
+                      out=None):
+        """``route`` without device allocation: the library's fixed scratch
+        (``NOALLOC_SCRATCH_BYTES`` per device, at most ``NOALLOC_MAX_NETS``
+        nets) holds the workspace, and work goes to ``stream``.  Calls that
+        overlap in time share that scratch and must be serialised by the
+        caller.  ``out`` may supply preallocated (results, paths) host arrays
+        so that the call allocates nothing in Python either."""
+        nets = np.ascontiguousarray(nets)
+        count = len(nets)
+        if out is not None:
+            results, paths = out
+        else:
+            results = np.empty(count, dtype=RESULT_DTYPE)
+            cap = int(8 * (nets["win_w"].astype(np.int64) + nets["win_h"].astype(np.int64)).sum()
+                      + 64 * self.layers * count + 64)
+            paths = np.empty(cap, dtype=np.uint32)
+        total = ctypes.c_uint64(0)
+        _check(lib().apgar_b200_lattice_route_noalloc(
+            self.handle, _vp(nets), ctypes.c_uint32(count), ctypes.c_uint32(max_sweeps),
+            ctypes.c_void_p(stream), _vp(results), _vp(paths), ctypes.c_uint64(paths.size),
+            ctypes.byref(total)))
+        return results, paths[: total.value]
 
     def plan(self, nets: np.ndarray, max_sweeps: int = 4096) -> "Plan":
         return Plan(self, nets, max_sweeps)

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -567,4 +568,260 @@ extern "C" int apgar_b200_lattice_accumulate_usage(void* plan, uint32_t* usage, 
                                           cell_count, p->sm_count, static_cast<cudaStream_t>(stream)));
   clear_error();
   return APGAR_B200_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free routing (apgar_b200_lattice_route_noalloc).
+//
+// Some callers must not allocate device memory while they route: a process
+// whose device memory is already held by another allocator (a caching
+// allocator, a fixed serving budget) gets out-of-memory from cudaMalloc, and a
+// router that shares the GPU with work on other streams cannot take the
+// device-wide synchronisation that cudaMalloc and cudaFree imply.  This entry
+// point serves them from one file-scope device array per device and per
+// process, carved into the same buffers a plan owns, and stages its host-side
+// plan in fixed file-scope host arrays.  It creates no stream, event or pinned
+// buffer; every copy and launch goes to the caller's stream.
+//
+// The scratch is shared by every call on a device: two calls whose work
+// overlaps in time (two host threads, or calls on different streams) race on
+// it and on the host staging arrays, and corrupt each other's results.
+// Callers serialise them.
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[APGAR_B200_NOALLOC_SCRATCH_BYTES];
+
+namespace apgar_b200 {
+namespace {
+
+constexpr int kNoallocMaxDevices = 64;
+constexpr uint64_t kNoallocAlign = 256;
+
+// Device address of g_noalloc_scratch per device ordinal; 0 until the first
+// call on that device looks it up (with that device current).
+std::atomic<uintptr_t> g_noalloc_base[kNoallocMaxDevices];
+
+struct NoallocStaging {
+  NetPlan plans[APGAR_B200_NOALLOC_MAX_NETS];
+  apgar_b200_lattice_result init[APGAR_B200_NOALLOC_MAX_NETS];
+  uint32_t order[APGAR_B200_NOALLOC_MAX_NETS];
+  int8_t width_class[APGAR_B200_NOALLOC_MAX_NETS];
+};
+NoallocStaging g_noalloc_host;
+
+int noalloc_scratch(int device, unsigned char** out) {
+  if (device < 0 || device >= kNoallocMaxDevices) {
+    return set_error(APGAR_B200_UNSUPPORTED,
+                     "allocation-free route supports device ordinals below 64");
+  }
+  uintptr_t base = g_noalloc_base[device].load(std::memory_order_acquire);
+  if (base == 0) {
+    void* ptr = nullptr;
+    APGAR_B200_CUDA("cudaGetSymbolAddress(allocation-free scratch)",
+                    cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+    base = reinterpret_cast<uintptr_t>(ptr);
+    g_noalloc_base[device].store(base, std::memory_order_release);
+  }
+  *out = reinterpret_cast<unsigned char*>(base);
+  return APGAR_B200_OK;
+}
+
+uint64_t noalloc_take(uint64_t* cursor, uint64_t bytes) {
+  const uint64_t at = *cursor;
+  *cursor = (at + bytes + kNoallocAlign - 1) & ~(kNoallocAlign - 1);
+  return at;
+}
+
+int route_noalloc(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint32_t count,
+                  uint32_t max_sweeps, cudaStream_t stream, apgar_b200_lattice_result* results,
+                  uint32_t* paths, uint64_t path_capacity, uint64_t* path_total) {
+  if (count > APGAR_B200_NOALLOC_MAX_NETS) {
+    return set_error(APGAR_B200_RESOURCE_EXHAUSTED,
+                     "allocation-free route takes at most " +
+                         std::to_string(APGAR_B200_NOALLOC_MAX_NETS) +
+                         " nets per call; split the batch or use apgar_b200_lattice_route");
+  }
+  const LatticeDeviceView& v = lat->view;
+  const uint64_t max_move = std::max(v.orth, std::max(v.diag, v.via));
+  NoallocStaging& h = g_noalloc_host;
+
+  // Admission and width classes: the same rules as a plan.
+  for (uint32_t i = 0; i < count; ++i) {
+    const apgar_b200_lattice_net& n = host_nets[i];
+    apgar_b200_lattice_result& r = h.init[i];
+    std::memset(&r, 0, sizeof(r));
+    r.cost = APGAR_B200_UNREACHABLE;
+    r.completion = APGAR_B200_COMPLETION_REJECTED;
+    h.width_class[i] = -1;
+    const bool in_lattice =
+        n.start_layer < static_cast<uint32_t>(v.layers) &&
+        n.goal_layer < static_cast<uint32_t>(v.layers) && n.win_w > 0 && n.win_h > 0 &&
+        static_cast<uint64_t>(n.win_x0) + n.win_w <= static_cast<uint64_t>(v.width) &&
+        static_cast<uint64_t>(n.win_y0) + n.win_h <= static_cast<uint64_t>(v.height) &&
+        n.start_x >= n.win_x0 && n.start_x < n.win_x0 + n.win_w && n.start_y >= n.win_y0 &&
+        n.start_y < n.win_y0 + n.win_h && n.goal_x >= n.win_x0 && n.goal_x < n.win_x0 + n.win_w &&
+        n.goal_y >= n.win_y0 && n.goal_y < n.win_y0 + n.win_h;
+    if (!in_lattice) continue;
+    const uint64_t cells = static_cast<uint64_t>(v.layers) * n.win_w * n.win_h;
+    if (cells * max_move >= kLabelInf) continue;
+    const uint32_t frame_width = std::max(n.win_w, n.win_h);
+    const uint32_t frame_rows = std::min(n.win_w, n.win_h);
+    const int ci = class_for_width(frame_width, v.layers);
+    if (ci < 0 || frame_rows > 32000u) continue;
+    h.width_class[i] = static_cast<int8_t>(ci);
+  }
+
+  // Plan records, class by class, larger windows first (ties by net index).
+  ClassRange ranges[kClassCount];
+  int range_count = 0;
+  uint32_t planned = 0;
+  uint64_t dist_cells = 0, arena_cells = 0;
+  for (int ci = 0; ci < kClassCount; ++ci) {
+    uint32_t members = 0;
+    for (uint32_t i = 0; i < count; ++i) {
+      if (h.width_class[i] == ci) h.order[members++] = i;
+    }
+    if (members == 0) continue;
+    std::sort(h.order, h.order + members, [&](uint32_t a, uint32_t b) {
+      const uint64_t ca = static_cast<uint64_t>(host_nets[a].win_w) * host_nets[a].win_h;
+      const uint64_t cb = static_cast<uint64_t>(host_nets[b].win_w) * host_nets[b].win_h;
+      return ca != cb ? ca > cb : a < b;
+    });
+    ClassRange& range = ranges[range_count++];
+    range = ClassRange{};
+    range.warps_per_net = kGroupSizes[ci];
+    range.begin = planned;
+    range.count = members;
+    for (uint32_t k = 0; k < members; ++k) {
+      const uint32_t i = h.order[k];
+      const apgar_b200_lattice_net& n = host_nets[i];
+      NetPlan& np = h.plans[planned++];
+      np = NetPlan{};
+      np.net = i;
+      np.transposed = n.win_h > n.win_w ? 1u : 0u;
+      np.rows = np.transposed ? n.win_w : n.win_h;
+      np.width = np.transposed ? n.win_h : n.win_w;
+      np.pitch = (np.width + 3u) & ~3u;
+      np.dist_offset = dist_cells;
+      dist_cells += static_cast<uint64_t>(v.layers) * np.rows * np.pitch;
+      arena_cells += 8ull * (n.win_w + n.win_h) + 64ull * v.layers;
+      range.max_rows = std::max(range.max_rows, static_cast<int>(np.rows));
+    }
+    if (lattice_sweep_smem_bytes(v.layers, range.warps_per_net, range.max_rows) >
+        kMaxSmemPerBlock) {
+      return set_error(APGAR_B200_UNSUPPORTED, "window too tall for the shared-memory row map");
+    }
+  }
+  const uint64_t arena_capacity = std::max<uint64_t>(arena_cells, 64);
+
+  // Carve the scratch: the same buffers, in the same roles, as a plan's.
+  uint64_t cursor = 0;
+  const uint64_t nets_at = noalloc_take(&cursor, count * sizeof(apgar_b200_lattice_net));
+  const uint64_t plans_at = noalloc_take(&cursor, planned * sizeof(NetPlan));
+  const uint64_t results_at = noalloc_take(&cursor, count * sizeof(apgar_b200_lattice_result));
+  const uint64_t counters_at = noalloc_take(&cursor, 2 * sizeof(unsigned long long));
+  const uint64_t labels_at = noalloc_take(&cursor, dist_cells * sizeof(uint32_t));
+  const uint64_t arena_at = noalloc_take(&cursor, arena_capacity * sizeof(uint32_t));
+  const uint64_t paths_at = noalloc_take(&cursor, arena_capacity * sizeof(uint32_t));
+  if (cursor > APGAR_B200_NOALLOC_SCRATCH_BYTES) {
+    return set_error(APGAR_B200_RESOURCE_EXHAUSTED,
+                     "allocation-free route needs " + std::to_string(cursor) +
+                         " bytes of scratch for this batch; the fixed scratch holds " +
+                         std::to_string(static_cast<uint64_t>(APGAR_B200_NOALLOC_SCRATCH_BYTES)) +
+                         " bytes; split the batch or use apgar_b200_lattice_route");
+  }
+  unsigned char* base = nullptr;
+  if (int rc = noalloc_scratch(lat->device, &base); rc != APGAR_B200_OK) return rc;
+  auto* d_nets = reinterpret_cast<apgar_b200_lattice_net*>(base + nets_at);
+  auto* d_plans = reinterpret_cast<NetPlan*>(base + plans_at);
+  auto* d_results = reinterpret_cast<apgar_b200_lattice_result*>(base + results_at);
+  auto* d_counters = reinterpret_cast<unsigned long long*>(base + counters_at);
+  auto* d_labels = reinterpret_cast<uint32_t*>(base + labels_at);
+  auto* d_arena = reinterpret_cast<uint32_t*>(base + arena_at);
+  auto* d_paths = reinterpret_cast<uint32_t*>(base + paths_at);
+
+  int sm_count = 0;
+  APGAR_B200_CUDA("cudaDeviceGetAttribute",
+                  cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, lat->device));
+  // The pageable source copies return once the bytes are staged, so the host
+  // staging arrays may be reused by the next call.
+  if (count > 0) {
+    APGAR_B200_CUDA("cudaMemcpyAsync(nets)",
+                    cudaMemcpyAsync(d_nets, host_nets, count * sizeof(apgar_b200_lattice_net),
+                                    cudaMemcpyHostToDevice, stream));
+    APGAR_B200_CUDA("cudaMemcpyAsync(results init)",
+                    cudaMemcpyAsync(d_results, h.init, count * sizeof(apgar_b200_lattice_result),
+                                    cudaMemcpyHostToDevice, stream));
+  }
+  if (planned > 0) {
+    APGAR_B200_CUDA("cudaMemcpyAsync(plans)",
+                    cudaMemcpyAsync(d_plans, h.plans, planned * sizeof(NetPlan),
+                                    cudaMemcpyHostToDevice, stream));
+  }
+  // Arena cursor and packed total start at zero; label slabs are written by
+  // the kernels before they are read.
+  APGAR_B200_CUDA("cudaMemsetAsync(counters)",
+                  cudaMemsetAsync(d_counters, 0, 2 * sizeof(unsigned long long), stream));
+  SweepLaunch launch{};
+  launch.lat = v;
+  launch.nets = d_nets;
+  launch.max_sweeps = max_sweeps;
+  launch.dist_pool = d_labels;
+  launch.results = d_results;
+  launch.path_arena = d_arena;
+  launch.path_arena_capacity = arena_capacity;
+  launch.arena_cursor = d_counters;
+  launch.cancel = nullptr;
+  for (int k = 0; k < range_count; ++k) {
+    launch.plans = d_plans + ranges[k].begin;
+    launch.plan_count = ranges[k].count;
+    APGAR_B200_CUDA("lattice sweep launch",
+                    launch_lattice_sweep(v.layers, ranges[k].warps_per_net, launch,
+                                         ranges[k].max_rows, stream));
+  }
+  APGAR_B200_CUDA("lattice pack launch",
+                  launch_lattice_pack(d_results, count, d_counters + 1, d_arena, d_paths, sm_count,
+                                      stream));
+
+  // Device-to-pageable copies return when the bytes have arrived.
+  unsigned long long total = 0;
+  APGAR_B200_CUDA("cudaMemcpyAsync(path total)",
+                  cudaMemcpyAsync(&total, d_counters + 1, sizeof(total), cudaMemcpyDeviceToHost,
+                                  stream));
+  if (count > 0) {
+    APGAR_B200_CUDA("cudaMemcpyAsync(results)",
+                    cudaMemcpyAsync(results, d_results, count * sizeof(apgar_b200_lattice_result),
+                                    cudaMemcpyDeviceToHost, stream));
+  }
+  if (path_total != nullptr) *path_total = total;
+  if (paths != nullptr && total > 0) {
+    if (total > path_capacity) {
+      return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "path output buffer is too small");
+    }
+    APGAR_B200_CUDA("cudaMemcpyAsync(paths)",
+                    cudaMemcpyAsync(paths, d_paths, total * sizeof(uint32_t),
+                                    cudaMemcpyDeviceToHost, stream));
+  }
+  APGAR_B200_CUDA("cudaStreamSynchronize(route)", cudaStreamSynchronize(stream));
+  return APGAR_B200_OK;
+}
+
+}  // namespace
+}  // namespace apgar_b200
+
+extern "C" int apgar_b200_lattice_route_noalloc(void* lattice, const apgar_b200_lattice_net* nets,
+                                                uint32_t count, uint32_t max_sweeps, void* stream,
+                                                apgar_b200_lattice_result* results,
+                                                uint32_t* paths, uint64_t path_capacity,
+                                                uint64_t* path_total) {
+  if (lattice == nullptr || (count > 0 && (nets == nullptr || results == nullptr)) ||
+      max_sweeps == 0 || max_sweeps > 30000) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT,
+                     "allocation-free lattice route received invalid arguments");
+  }
+  auto* lat = static_cast<LatticeObject*>(lattice);
+  if (int rc = check_device(lat->device); rc != APGAR_B200_OK) return rc;
+  const int rc = route_noalloc(lat, nets, count, max_sweeps, static_cast<cudaStream_t>(stream),
+                               results, paths, path_capacity, path_total);
+  if (rc == APGAR_B200_OK) clear_error();
+  return rc;
 }

@@ -311,6 +311,40 @@ APGAR_B200_API int apgar_b200_lattice_route(void* lattice, const apgar_b200_latt
                              apgar_b200_lattice_result* results, uint32_t* paths,
                              uint64_t path_capacity, uint64_t* path_total);
 
+/* Allocation-free form of apgar_b200_lattice_route.  No counterpart in the
+ * reference: it is an addition for callers that must not allocate device
+ * memory while they route, such as a process whose device memory is already
+ * held by another allocator (a caching allocator or a fixed serving budget,
+ * where cudaMalloc fails), or a router sharing the GPU with work on other
+ * streams that cannot take the device-wide synchronisation cudaMalloc and
+ * cudaFree imply.
+ *
+ * Same admission, search, results and packed paths as
+ * apgar_b200_lattice_route, with these differences:
+ *  - Its label slabs, plan records, result records and path arena live in one
+ *    fixed device array of APGAR_B200_NOALLOC_SCRATCH_BYTES per device.  It
+ *    calls no cudaMalloc or cudaFree and creates no stream, event or pinned
+ *    buffer.  The host-side plan is staged in fixed arrays.
+ *  - A batch that needs more than the scratch holds, or has more than
+ *    APGAR_B200_NOALLOC_MAX_NETS nets, fails with
+ *    APGAR_B200_RESOURCE_EXHAUSTED and a message giving the bytes it needed.
+ *  - Its copies and launches go to `stream` (NULL: the legacy default
+ *    stream).  Width classes run one after another on that stream.  The call
+ *    synchronises only that stream before it returns.
+ *  - It takes no cancel flag.
+ *  - The first call on a device looks up the array's device address with that
+ *    device current.  That call should come before any stream capture on the
+ *    device.
+ *  - The scratch is shared: calls whose work overlaps in time race on it and
+ *    corrupt each other's results.  This includes two host threads, or calls
+ *    on different streams.  Callers serialise them. */
+#define APGAR_B200_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+#define APGAR_B200_NOALLOC_MAX_NETS 4096u
+APGAR_B200_API int apgar_b200_lattice_route_noalloc(void* lattice, const apgar_b200_lattice_net* nets,
+                                     uint32_t count, uint32_t max_sweeps, void* stream,
+                                     apgar_b200_lattice_result* results, uint32_t* paths,
+                                     uint64_t path_capacity, uint64_t* path_total);
+
 /* Resident form for repeated launches: plan once (host planning, workspace
  * allocation, nets copied to the device), then execute on a stream (launches
  * only; capturable in a CUDA graph), then read back. */
