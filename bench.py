@@ -49,8 +49,10 @@ def parse_args():
     ap.add_argument("--size", type=int, default=2048)
     ap.add_argument("--nets", type=int, default=4096)
     ap.add_argument("--seed", type=int, default=2)
-    ap.add_argument("--cpu-sample", type=int, default=512,
+    ap.add_argument("--cpu-sample", type=int, default=4096,
                     help="nets timed by the CPU baseline (bounded sample)")
+    ap.add_argument("--ref-sample", type=int, default=512,
+                    help="nets per step of the reference arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
 
@@ -181,7 +183,7 @@ def run_reference(args, rank, world):
 
     lat, nets = synth.config_medium(args.seed, nets=args.nets, size=args.size)
     threads = os.cpu_count() or 1
-    sample = np.ascontiguousarray(nets[: args.cpu_sample])
+    sample = np.ascontiguousarray(nets[: args.ref_sample])
     for _ in range(args.warmup):
         oracle.astar_batch(lat, sample[:64], threads=threads)
     t0 = time.perf_counter()
@@ -316,7 +318,7 @@ def main():
             "roofline": {
                 "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind,
-                "traffic": (traffic or {}).get("dram_bytes_per_launch"),
+                "traffic": (traffic or {}).get("dram_bytes_per_step"),
                 "bytes_alg_per_step": bytes_alg, "one_pass_bytes_per_step": one_pass,
             },
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
