@@ -24,9 +24,12 @@
  *
  * Parity pinning: graph mode is checked against golden fixtures produced by
  * the reference's own CPU A* and corpus builders (tests/golden/, generated by
- * oracle/ref_fixtures.cc compiled from the reference sources); lattice mode is
- * checked against the reference A* on single-layer lattices compiled through
- * the reference geometry compiler (same fixture generator).
+ * oracle/ref_fixtures.cc compiled from the reference sources).  Lattice mode
+ * is pinned through graph mode: on single-layer lattices expressed as node
+ * records with the lattice move rule, lo_dijkstra and go_search give the same
+ * costs and the same canonical reverse paths; vias, which the reference's
+ * planar search does not model, are covered by the agreement of the three
+ * lattice restatements.
  */
 #ifndef APGAR_B200_ORACLE_H_
 #define APGAR_B200_ORACLE_H_

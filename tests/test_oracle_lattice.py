@@ -113,3 +113,68 @@ def test_disconnected_by_wall():
     c = oracle.dijkstra(lat, net[0])[0]
     assert c != oracle.lo_inf()
     assert c == oracle.astar_batch(lat, net)[0] == oracle.sweep_batch(lat, net)[0][0]
+
+
+def _lattice_as_graph(dense):
+    """Single-layer lattice as DeviceCompiledBoardV1 node records (node id
+    y*W + x), with legal-edge masks from the lattice move rule: orthogonal moves
+    need both cells free, diagonal moves also both side cells."""
+    from tests.golden import ref_corpus
+
+    _, h, w = dense.shape
+    nodes = np.zeros(h * w, dtype=ref_corpus.NODE_DTYPE)
+    nodes["neighbors"] = 0xFFFFFFFF
+
+    def free(x, y):
+        return 0 <= x < w and 0 <= y < h and not dense[0, y, x]
+
+    for y in range(h):
+        for x in range(w):
+            n = nodes[y * w + x]
+            n["lattice_x"], n["lattice_y"] = x, y
+            legal = 0
+            for d in range(8):
+                nx, ny = x + DX[d], y + DY[d]
+                if not (0 <= nx < w and 0 <= ny < h):
+                    continue
+                n["neighbors"][d] = ny * w + nx
+                ok = free(x, y) and free(nx, ny)
+                if d & 1:
+                    ok = ok and free(x + DX[d], y) and free(x, y + DY[d])
+                if ok:
+                    legal |= 1 << d
+            n["legal_edges"] = legal
+    return nodes
+
+
+@pytest.mark.parametrize("seed", [3, 4])
+def test_pinned_to_reference_graph_oracle_on_single_layer(seed):
+    """Transitive pin: the graph oracle reproduces the reference CPU A* on
+    every fixture query (test_oracle_graph.py); on single-layer lattices
+    (no vias, bend 0) the lattice oracle must give the same costs and the same
+    canonical reverse paths as the graph oracle's compact heading-state path."""
+    rng = np.random.default_rng(seed)
+    h, w = 40, 64
+    dense = np.zeros((1, h, w), bool)
+    for _ in range(30):
+        x0, y0 = rng.integers(0, w - 4), rng.integers(0, h - 4)
+        dense[0, y0:y0 + rng.integers(2, 9), x0:x0 + rng.integers(2, 9)] = True
+    lat = synth.Lattice(1, h, w, synth.pack_bits(dense), None)
+    nodes = _lattice_as_graph(dense)
+    free = np.argwhere(~dense[0])
+    compared = reached = 0
+    for _ in range(40):
+        (sy, sx), (gy, gx) = free[rng.integers(len(free), size=2)]
+        net = np.array([(0, sx, sy, 0, gx, gy, 0, 0, w, h)], dtype=synth.NET_DTYPE)
+        cost, path, _ = oracle.dijkstra(lat, net[0])
+        ok, gcost, _, gpath, _ = oracle.graph_search(nodes, (10, 14, 0), int(sy * w + sx),
+                                                     int(gy * w + gx))
+        compared += 1
+        if cost == oracle.lo_inf():
+            assert not ok
+            continue
+        reached += 1
+        assert ok and gcost == cost
+        graph_cells = (gpath // 9).astype(np.uint32)  # node ids are y*W + x = cell ids
+        assert np.array_equal(graph_cells, path), (sx, sy, gx, gy)
+    assert compared == 40 and reached >= 20
