@@ -72,3 +72,26 @@ def test_graph_oracle_matches_reference_cpu_astar(case):
             assert total == cost
         elif q.cpu_status == 1:
             assert not reached, qi
+
+
+def test_fixtures_regenerate_from_the_reference(tmp_path):
+    """Where the reference sources are present and built (oracle/build_ref.sh),
+    its own corpus builders and CPU A* reproduce the committed fixtures byte
+    for byte."""
+    import filecmp
+    import os
+    import subprocess
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = os.path.join(root, "oracle", "_ref", "ref_fixtures")
+    ref = os.environ.get("APGAR_REFERENCE", "/root/reference")
+    pcb = os.path.join(ref, "tests", "fixtures", "m1_exactness.kicad_pcb")
+    if not (os.path.exists(exe) and os.path.exists(pcb)):
+        pytest.skip("reference sources or the compiled reference checker are absent")
+    subprocess.run([exe, pcb, str(tmp_path)], check=True, stdout=subprocess.DEVNULL)
+    committed = os.path.join(root, "tests", "golden", "ref_corpus")
+    names = sorted(os.listdir(committed))
+    assert sorted(os.listdir(tmp_path)) == names
+    for name in names:
+        assert filecmp.cmp(os.path.join(committed, name), os.path.join(tmp_path, name),
+                           shallow=False), name
