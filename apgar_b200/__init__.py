@@ -59,6 +59,24 @@ class LatticeDesc(ctypes.Structure):
     ]
 
 
+GENERATORS = {"sweep": 0, "frontier": 1}
+
+
+class LatticeOptions(ctypes.Structure):
+    _fields_ = [
+        ("generator", ctypes.c_uint32),
+        ("max_iterations", ctypes.c_uint32),
+        ("bucket_width", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+    ]
+
+
+def _options(generator: str, max_iterations: int, bucket_width: int) -> LatticeOptions:
+    if generator not in GENERATORS:
+        raise BackendError(1, f"unknown lattice generator {generator!r}")
+    return LatticeOptions(GENERATORS[generator], max_iterations, bucket_width, 0)
+
+
 class PlanInfo(ctypes.Structure):
     _fields_ = [
         ("net_count", ctypes.c_uint32),
@@ -163,11 +181,14 @@ class DeviceLattice:
             pass
 
     def route(self, nets: np.ndarray, max_sweeps: int = 4096, cancel: np.ndarray | None = None,
-              want_paths: bool = True, path_capacity: int | None = None, out=None):
+              want_paths: bool = True, path_capacity: int | None = None, out=None,
+              generator: str = "sweep", max_rounds: int = 1 << 30, bucket_width: int = 0):
         """Searches every net; returns (results record array, packed paths).
 
-        ``out`` may supply preallocated (results, paths) host arrays (pinned
-        memory makes the transfers faster)."""
+        ``generator`` is "sweep" (budget ``max_sweeps``) or "frontier"
+        (budget ``max_rounds``, key level width ``bucket_width``, 0 = twice
+        the largest move).  ``out`` may supply preallocated (results, paths)
+        host arrays (pinned memory makes the transfers faster)."""
         nets = np.ascontiguousarray(nets)
         count = len(nets)
         if out is not None:
@@ -178,10 +199,17 @@ class DeviceLattice:
                                             + nets["win_h"].astype(np.int64)).sum() + 64 * self.layers * count + 64)
             paths = np.empty(cap if want_paths else 0, dtype=np.uint32)
         total = ctypes.c_uint64(0)
-        _check(lib().apgar_b200_lattice_route(
-            self.handle, _vp(nets), ctypes.c_uint32(count), ctypes.c_uint32(max_sweeps),
-            _vp(cancel), _vp(results), _vp(paths) if want_paths else None,
-            ctypes.c_uint64(paths.size if want_paths else 0), ctypes.byref(total)))
+        if generator == "sweep":
+            _check(lib().apgar_b200_lattice_route(
+                self.handle, _vp(nets), ctypes.c_uint32(count), ctypes.c_uint32(max_sweeps),
+                _vp(cancel), _vp(results), _vp(paths) if want_paths else None,
+                ctypes.c_uint64(paths.size if want_paths else 0), ctypes.byref(total)))
+        else:
+            opts = _options(generator, max_rounds, bucket_width)
+            _check(lib().apgar_b200_lattice_route_ex(
+                self.handle, _vp(nets), ctypes.c_uint32(count), ctypes.byref(opts),
+                _vp(cancel), _vp(results), _vp(paths) if want_paths else None,
+                ctypes.c_uint64(paths.size if want_paths else 0), ctypes.byref(total)))
         return results, (paths[: total.value] if want_paths else None)
 
     def route_noalloc(self, nets: np.ndarray, max_sweeps: int = 4096, stream: int = 0,
@@ -208,20 +236,29 @@ class DeviceLattice:
             ctypes.byref(total)))
         return results, paths[: total.value]
 
-    def plan(self, nets: np.ndarray, max_sweeps: int = 4096) -> "Plan":
-        return Plan(self, nets, max_sweeps)
+    def plan(self, nets: np.ndarray, max_sweeps: int = 4096, generator: str = "sweep",
+             max_rounds: int = 1 << 30, bucket_width: int = 0) -> "Plan":
+        return Plan(self, nets, max_sweeps, generator, max_rounds, bucket_width)
 
 
 class Plan:
     """A planned batch resident on the device (execute may be graph-captured)."""
 
-    def __init__(self, lattice: DeviceLattice, nets: np.ndarray, max_sweeps: int):
+    def __init__(self, lattice: DeviceLattice, nets: np.ndarray, max_sweeps: int,
+                 generator: str = "sweep", max_rounds: int = 1 << 30, bucket_width: int = 0):
         self.lattice = lattice
         self.nets = np.ascontiguousarray(nets)
+        self.generator = generator
         handle = ctypes.c_void_p()
-        _check(lib().apgar_b200_lattice_plan(lattice.handle, _vp(self.nets),
-                                             ctypes.c_uint32(len(self.nets)),
-                                             ctypes.c_uint32(max_sweeps), ctypes.byref(handle)))
+        if generator == "sweep":
+            _check(lib().apgar_b200_lattice_plan(lattice.handle, _vp(self.nets),
+                                                 ctypes.c_uint32(len(self.nets)),
+                                                 ctypes.c_uint32(max_sweeps), ctypes.byref(handle)))
+        else:
+            opts = _options(generator, max_rounds, bucket_width)
+            _check(lib().apgar_b200_lattice_plan_ex(lattice.handle, _vp(self.nets),
+                                                    ctypes.c_uint32(len(self.nets)),
+                                                    ctypes.byref(opts), ctypes.byref(handle)))
         self.handle = handle
 
     def execute(self, stream: int = 0) -> None:

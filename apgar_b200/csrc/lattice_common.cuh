@@ -64,6 +64,29 @@ struct SweepLaunch {
   const volatile uint32_t* cancel;  // host-mapped flag or nullptr
 };
 
+// One width class of the frontier form (lattice_frontier.cu).  A net's
+// label words (label << 32 | ~round stamp, window layout [layer][y][x]) start
+// at word plan.dist_offset of `words`, its far-list bits at word
+// dist_offset / 32 of `far_bits`, and its three queue lists at entry
+// 3 * dist_offset of `lists`; dist_offset is a multiple of 128 cells.
+struct FrontierLaunch {
+  LatticeDeviceView lat;
+  const apgar_b200_lattice_net* nets;
+  const NetPlan* plans;
+  uint32_t plan_count;
+  uint32_t max_rounds;
+  uint32_t bucket_width;
+  unsigned long long* words;
+  uint32_t* far_bits;
+  uint32_t* lists;
+  apgar_b200_lattice_result* results;
+  uint32_t* path_arena;
+  uint64_t path_arena_capacity;
+  unsigned long long* arena_cursor;
+  unsigned int* next_plan;            // work-stealing cursor of this class
+  const volatile uint32_t* cancel;  // host-mapped flag or nullptr
+};
+
 __device__ __forceinline__ uint32_t sat(uint32_t v) { return v < kLabelInf ? v : kLabelInf; }
 
 // 32 bits of a bit-packed row starting at signed bit position `pos`; bits

@@ -1,0 +1,520 @@
+// Lattice-mode frontier search: bucketed, label-correcting A* per net window,
+// one warp group per net, persistent work stealing over the nets of a class.
+//
+// A cell is keyed by f = g + h, with h the admissible, consistent
+// octile-plus-via bound to the goal.  The search works through key levels
+// of width delta (the bucket width), with thr the current level's upper bound:
+//   * a round expands every cell of the current list.  It relaxes the 8
+//     planar moves and the 2 vias, and a lowered cell joins the next round's
+//     list if its key is below thr, else the deferred ("far") list;
+//   * when a round leaves the current list empty, the level is done: thr
+//     grows by delta and the far list becomes the current list.  Every
+//     child key lies within twice the largest move cost of its parent's key,
+//     and the host keeps delta >= 2 * max move, so the far list holds exactly
+//     the next level: a cell that left it keeps a key below thr from then on
+//     and never rejoins it, which is why far bits are never cleared.
+// The search stops when nothing is queued (disconnected, or every reachable
+// cell is final), or when a level is done with thr above the goal label.
+//
+// Why the labels the canonical walk reads are exact: f is non-decreasing
+// along any optimal path under a consistent h, so every cell on an optimal
+// start-goal path has true f at most the optimum C*.
+//  - Suppose such a cell's label were still above its distance.  Take the
+//    first inexact cell on its optimal path; its predecessor p is exact.
+//  - When p's label became exact, p was queued.  Had p been expanded since,
+//    the next cell would be exact, so p must still be waiting.
+//  - A cell waiting in the current list blocks the stop (the list is empty at
+//    a stop).  p in the far list means its key was at least the current thr,
+//    yet its key f*(p) <= C* <= goal label < thr at the stop, a contradiction.
+// The canonical walk accepts a predecessor only when label + move cost equals
+// the current label, and an upper-bound label passes that test only when it
+// is exact.  So the reverse path equals the one under full-window exact
+// labels (reference tie-break, gpu/cuda/planar_router.cu:977-1009 and
+// :1084-1165).
+//
+// The heuristic follows the reference's octile bound (src/routing/
+// cpu_astar.cc:176-190), plus |dl| * via for the layer difference.
+//
+// Each cell's 64-bit word holds its label in the high half.  The low half
+// holds ~s, with s the round whose list it last joined; 0 when deferred.  One
+// 64-bit atomicMin both lowers the label and reports whether the cell is
+// already in the next round's list.  A per-cell bit keeps a cell at most once
+// in the far list.  So no list holds more entries than the window has cells.
+// Queue entries are packed cells (layer << 28 | y << 14 | x, window-local).
+// Appends take one packed warp scan and one shared atomic per warp and list.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "lattice_common.cuh"
+
+namespace apgar_b200 {
+namespace {
+
+constexpr int kCancelPollRounds = 32;
+constexpr uint64_t kWordInf = (static_cast<uint64_t>(kLabelInf) << 32) | 0xFFFFFFFFull;
+
+__host__ __device__ constexpr int frontier_groups_per_block(int G) { return G >= 4 ? 1 : 4 / G; }
+
+__device__ __forceinline__ uint32_t pack_cell(int l, int x, int y) {
+  return (static_cast<uint32_t>(l) << 28) | (static_cast<uint32_t>(y) << 14) |
+         static_cast<uint32_t>(x);
+}
+
+struct Window {
+  int x0, y0, w, h;
+  int gl, gx, gy;  // goal, window-local
+};
+
+__device__ __forceinline__ uint32_t cell_index(const Window& win, int l, int x, int y) {
+  return (static_cast<uint32_t>(l) * static_cast<uint32_t>(win.h) + static_cast<uint32_t>(y)) *
+             static_cast<uint32_t>(win.w) +
+         static_cast<uint32_t>(x);
+}
+
+// Planar heading d (0 E, 1 NE, 2 N, 3 NW, 4 W, 5 SW, 6 S, 7 SE) as a step.
+__host__ __device__ constexpr int fdx(int d) {
+  return (d == 0 || d == 1 || d == 7) ? 1 : (d == 2 || d == 6) ? 0 : -1;
+}
+__host__ __device__ constexpr int fdy(int d) {
+  return (d >= 1 && d <= 3) ? 1 : (d == 0 || d == 4) ? 0 : -1;
+}
+
+// Admissible, consistent bound on the remaining cost: octile in the plane,
+// the via cost per layer of difference.
+__device__ __forceinline__ uint32_t heuristic(const LatticeDeviceView& lat, const Window& win,
+                                              int l, int x, int y) {
+  const uint32_t dx = static_cast<uint32_t>(abs(x - win.gx));
+  const uint32_t dy = static_cast<uint32_t>(abs(y - win.gy));
+  const uint32_t lo = min(dx, dy), hi = max(dx, dy);
+  const uint32_t planar = lat.diag >= lat.orth
+                              ? lo * min(lat.diag, 2u * lat.orth) + (hi - lo) * lat.orth
+                              : hi * lat.diag;
+  return planar + static_cast<uint32_t>(abs(l - win.gl)) * lat.via;
+}
+
+// Free bits of window cells x-1..x+1 (bits 0..2) in row y of layer l; cells
+// outside the window read as blocked.
+__device__ __forceinline__ uint32_t free3(const LatticeDeviceView& lat, const Window& win, int l,
+                                          int x, int y) {
+  if (y < 0 || y >= win.h) return 0u;
+  const uint32_t* row =
+      lat.blocked + (static_cast<size_t>(l) * lat.height + (win.y0 + y)) * lat.words;
+  uint32_t f = ~fetch_bits32(row, lat.words, win.x0 + x - 1) & 7u;
+  if (x == 0) f &= ~1u;
+  if (x + 1 >= win.w) f &= ~4u;
+  return f;
+}
+
+__device__ __forceinline__ bool cell_free_w(const LatticeDeviceView& lat, const Window& win, int l,
+                                            int x, int y) {
+  if (l < 0 || l >= lat.layers || x < 0 || y < 0 || x >= win.w || y >= win.h) return false;
+  const int gx = win.x0 + x, gy = win.y0 + y;
+  const uint32_t word =
+      __ldg(lat.blocked + (static_cast<size_t>(l) * lat.height + gy) * lat.words + (gx >> 5));
+  return ((word >> (gx & 31)) & 1u) == 0;
+}
+
+__device__ __forceinline__ bool via_allowed(const LatticeDeviceView& lat, const Window& win,
+                                            int lower, int x, int y) {
+  if (lat.via_ok == nullptr) return true;
+  const int gx = win.x0 + x, gy = win.y0 + y;
+  const uint32_t word =
+      __ldg(lat.via_ok + (static_cast<size_t>(lower) * lat.height + gy) * lat.words + (gx >> 5));
+  return ((word >> (gx & 31)) & 1u) != 0;
+}
+
+__device__ __forceinline__ uint32_t label_of(const unsigned long long* w) {
+  return static_cast<uint32_t>(__ldcg(w) >> 32);
+}
+
+template <int G>
+__device__ __forceinline__ void fsync(int barrier_id) {
+  if constexpr (G == 1) {
+    __syncwarp();
+  } else {
+    __threadfence_block();
+    asm volatile("bar.sync %0, %1;" ::"r"(barrier_id), "r"(G * 32) : "memory");
+  }
+}
+
+// Expands one queued cell.  The memory operations are issued move-parallel in
+// waves: the cell's label, mask bits and all in-window neighbour labels
+// together, then the 64-bit atomicMins, then far-bit atomics for the lowered
+// cells that leave the level.  So one cell costs a few L2 round trips, not a
+// few per move.  Lowered neighbours that join the next round's list are
+// flagged in cur_mask, those that join the far list in far_mask; ne[d] holds
+// the packed cell.
+__device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const Window& win,
+                                            uint32_t e, unsigned long long* words,
+                                            uint32_t* farbit, uint32_t thr, uint32_t next_stamp,
+                                            uint32_t (&ne)[10], uint32_t& cur_mask,
+                                            uint32_t& far_mask) {
+  const int l = static_cast<int>(e >> 28), y = static_cast<int>((e >> 14) & 0x3FFFu),
+            x = static_cast<int>(e & 0x3FFFu);
+  const uint32_t here = cell_index(win, l, x, y);
+  const uint32_t plane = static_cast<uint32_t>(win.w) * static_cast<uint32_t>(win.h);
+  uint32_t ni[10];
+  uint32_t inside = 0;  // neighbour lies in the window (its word may be read)
+#pragma unroll
+  for (int d = 0; d < 8; ++d) {
+    const int nx = x + fdx(d), ny = y + fdy(d);
+    inside |= (nx >= 0 && nx < win.w && ny >= 0 && ny < win.h) ? (1u << d) : 0u;
+    ni[d] = here + static_cast<uint32_t>(fdy(d) * win.w + fdx(d));
+  }
+  inside |= l > 0 ? (1u << 8) : 0u;
+  inside |= l + 1 < lat.layers ? (1u << 9) : 0u;
+  ni[8] = here - plane;
+  ni[9] = here + plane;
+  // wave 1: own label, neighbour labels, mask bits
+  const uint32_t gv = label_of(words + here);
+  uint32_t seen[10];
+#pragma unroll
+  for (int d = 0; d < 10; ++d) seen[d] = (inside & (1u << d)) ? label_of(words + ni[d]) : 0u;
+  const uint32_t r0 = free3(lat, win, l, x, y - 1);
+  const uint32_t r1 = free3(lat, win, l, x, y);
+  const uint32_t r2 = free3(lat, win, l, x, y + 1);
+  const bool down_ok = l > 0 && cell_free_w(lat, win, l - 1, x, y) && via_allowed(lat, win, l - 1, x, y);
+  const bool up_ok = l + 1 < lat.layers && cell_free_w(lat, win, l + 1, x, y) &&
+                     via_allowed(lat, win, l, x, y);
+  uint32_t legal = (down_ok ? (1u << 8) : 0u) | (up_ok ? (1u << 9) : 0u);
+#pragma unroll
+  for (int d = 0; d < 8; ++d) {
+    const int dx = fdx(d), dy = fdy(d);
+    const uint32_t row = dy < 0 ? r0 : (dy == 0 ? r1 : r2);
+    bool ok = (row >> (1 + dx)) & 1u;
+    if (d & 1) ok = ok && ((r1 >> (1 + dx)) & 1u) && ((row >> 1) & 1u);
+    legal |= ok ? (1u << d) : 0u;
+  }
+  // wave 2: lower the labels (the low half carries the list membership)
+  const uint32_t cur_low = 0xFFFFFFFFu - next_stamp;
+  uint32_t cand[10], low[10];
+  unsigned long long old[10];
+#pragma unroll
+  for (int d = 0; d < 10; ++d) {
+    const uint32_t cost = d >= 8 ? lat.via : ((d & 1) ? lat.diag : lat.orth);
+    cand[d] = gv + cost;
+    old[d] = ~0ull;
+    low[d] = 0xFFFFFFFFu;
+    if ((legal & (1u << d)) && cand[d] < seen[d]) {
+      const int nl = d == 8 ? l - 1 : (d == 9 ? l + 1 : l);
+      const int nx = d < 8 ? x + fdx(d) : x, ny = d < 8 ? y + fdy(d) : y;
+      ne[d] = pack_cell(nl, nx, ny);
+      low[d] = cand[d] + heuristic(lat, win, nl, nx, ny) < thr ? cur_low : 0xFFFFFFFFu;
+      old[d] = atomicMin(words + ni[d], (static_cast<unsigned long long>(cand[d]) << 32) | low[d]);
+    }
+  }
+  // wave 3: queue membership of the lowered cells
+  cur_mask = 0;
+  far_mask = 0;
+  uint32_t far_try = 0;
+#pragma unroll
+  for (int d = 0; d < 10; ++d) {
+    const bool lowered = old[d] != ~0ull && cand[d] < static_cast<uint32_t>(old[d] >> 32);
+    if (!lowered) continue;
+    if (low[d] == cur_low) {
+      cur_mask |= static_cast<uint32_t>(old[d]) != cur_low ? (1u << d) : 0u;
+    } else {
+      far_try |= 1u << d;
+    }
+  }
+  uint32_t prior[10];
+#pragma unroll
+  for (int d = 0; d < 10; ++d) {
+    prior[d] = ~0u;
+    if (far_try & (1u << d)) prior[d] = atomicOr(farbit + (ni[d] >> 5), 1u << (ni[d] & 31));
+  }
+#pragma unroll
+  for (int d = 0; d < 10; ++d) {
+    if ((far_try & (1u << d)) && (prior[d] & (1u << (ni[d] & 31))) == 0u) far_mask |= 1u << d;
+  }
+}
+
+struct GroupShared {
+  uint32_t count[3];  // next-round list being built, rotated per round
+  uint32_t far_count;
+  uint32_t plan;
+  uint32_t cancel[2];
+  uint32_t sums[16];
+};
+
+template <int G>
+__global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
+    lattice_frontier_kernel(FrontierLaunch p) {
+  constexpr int kGroups = frontier_groups_per_block(G);
+  constexpr int T = G * 32;
+  __shared__ GroupShared shared_groups[kGroups];
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int gi = warp / G;
+  const int g = warp - gi * G;
+  const int tid = g * 32 + lane;
+  const int barrier_id = gi + 1;
+  GroupShared& sh = shared_groups[gi];
+  const LatticeDeviceView& lat = p.lat;
+  const uint32_t orth = lat.orth, diag = lat.diag, via = lat.via;
+
+  for (;;) {
+    if (tid == 0) sh.plan = atomicAdd(p.next_plan, 1u);
+    fsync<G>(barrier_id);
+    const uint32_t plan_index = sh.plan;
+    if (plan_index >= p.plan_count) return;  // uniform within the group
+    const NetPlan plan = p.plans[plan_index];
+    const apgar_b200_lattice_net net = p.nets[plan.net];
+    Window win;
+    win.x0 = static_cast<int>(net.win_x0);
+    win.y0 = static_cast<int>(net.win_y0);
+    win.w = static_cast<int>(net.win_w);
+    win.h = static_cast<int>(net.win_h);
+    win.gl = static_cast<int>(net.goal_layer);
+    win.gx = static_cast<int>(net.goal_x) - win.x0;
+    win.gy = static_cast<int>(net.goal_y) - win.y0;
+    const int sl = static_cast<int>(net.start_layer);
+    const int sx = static_cast<int>(net.start_x) - win.x0, sy = static_cast<int>(net.start_y) - win.y0;
+    const uint32_t cells = static_cast<uint32_t>(lat.layers) * win.w * win.h;
+    const uint32_t padded = (cells + 127u) & ~127u;
+    unsigned long long* words = p.words + plan.dist_offset;
+    uint32_t* farbit = p.far_bits + plan.dist_offset / 32;
+    uint32_t* list_a = p.lists + 3 * plan.dist_offset;
+    uint32_t* list_b = list_a + cells;
+    uint32_t* list_c = list_b + cells;
+
+    // clear the net's label words and far bits (16-byte stores over the
+    // padded slab)
+    {
+      uint4* w4 = reinterpret_cast<uint4*>(words);
+      const uint4 inf2 = make_uint4(0xFFFFFFFFu, kLabelInf, 0xFFFFFFFFu, kLabelInf);
+      for (uint32_t i = tid; i < padded / 2; i += T) w4[i] = inf2;
+      uint4* f4 = reinterpret_cast<uint4*>(farbit);
+      for (uint32_t i = tid; i < padded / 128; i += T) f4[i] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    const bool endpoints_free = cell_free_w(lat, win, sl, sx, sy) &&
+                                cell_free_w(lat, win, win.gl, win.gx, win.gy);
+    // every clearing store of the group lands before the start is seeded
+    fsync<G>(barrier_id);
+    if (tid == 0) {
+      sh.count[0] = sh.count[1] = sh.count[2] = 0;
+      sh.far_count = 0;
+      sh.cancel[0] = sh.cancel[1] = 0;
+      if (endpoints_free) {
+        // label 0, in the list of round 0 (stamp 1)
+        words[cell_index(win, sl, sx, sy)] = 0xFFFFFFFFull - 1ull;
+        list_a[0] = pack_cell(sl, sx, sy);
+      }
+    }
+    fsync<G>(barrier_id);
+
+    uint32_t completion = APGAR_B200_COMPLETION_DISCONNECTED;
+    uint32_t rounds = 0, levels = 0;
+    uint32_t expanded = 0;  // this thread's expansions
+    if (endpoints_free) {
+      const uint32_t goal_index = cell_index(win, win.gl, win.gx, win.gy);
+      const uint32_t delta = p.bucket_width;
+      const uint32_t h0 = heuristic(lat, win, sl, sx, sy);
+      uint32_t thr = h0 + min(delta, 0xFFFFFFFFu - h0);
+      uint32_t n = 1;
+      uint32_t* cur = list_a;
+      uint32_t* nxt = list_b;
+      uint32_t* far = list_c;
+      completion = APGAR_B200_COMPLETION_REACHED;  // refined from the goal label below
+      for (uint32_t r = 0;; ++r) {
+        // written during round r - 1, before its closing barrier
+        if (r > 0 && sh.cancel[(r + 1) & 1] != 0u) {
+          completion = APGAR_B200_COMPLETION_CANCELLED;
+          break;
+        }
+        if (n == 0u) {
+          // ---- the level is done: open the next one from the far list ----
+          const uint32_t nf = sh.far_count;
+          const uint32_t goal_label = label_of(words + goal_index);
+          if (nf == 0u) break;           // every reachable cell is final
+          if (thr > goal_label) break;   // every cell with key <= C* is final
+          ++levels;
+          thr += min(delta, 0xFFFFFFFFu - thr);
+          uint32_t* t = cur;
+          cur = far;
+          far = t;
+          n = nf;
+          fsync<G>(barrier_id);  // everyone has read the far count
+          if (tid == 0) sh.far_count = 0;
+          fsync<G>(barrier_id);
+        }
+        if (r == p.max_rounds) {
+          completion = APGAR_B200_COMPLETION_BUDGET_EXHAUSTED;
+          break;
+        }
+        rounds = r + 1;
+        if (tid == 0) {
+          sh.count[(r + 1) % 3] = 0;  // last read after round r - 2
+          if (p.cancel != nullptr && (r % kCancelPollRounds) == 0u) {
+            sh.cancel[r & 1] = *p.cancel != 0u ? 1u : 0u;
+          } else {
+            sh.cancel[r & 1] = sh.cancel[(r + 1) & 1];
+          }
+        }
+        uint32_t* count = &sh.count[r % 3];
+        const uint32_t next_stamp = r + 2;
+        for (uint32_t base = static_cast<uint32_t>(g) * 32u; base < n; base += T) {
+          const uint32_t i = base + static_cast<uint32_t>(lane);
+          const bool valid = i < n;
+          uint32_t cur_mask = 0, far_mask = 0;
+          uint32_t ne[10];
+          if (valid) {
+            ++expanded;
+            expand_cell(lat, win, cur[i], words, farbit, thr, next_stamp, ne, cur_mask, far_mask);
+          }
+          // one packed warp scan places both lists' entries
+          const uint32_t nc = __popc(cur_mask), nfar = __popc(far_mask);
+          uint32_t packed = nc | (nfar << 16);
+#pragma unroll
+          for (int sft = 1; sft < 32; sft <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, packed, sft);
+            if (lane >= sft) packed += o;
+          }
+          const uint32_t totals = __shfl_sync(0xFFFFFFFFu, packed, 31);
+          uint32_t at_cur = 0, at_far = 0;
+          if (lane == 0) {
+            if ((totals & 0xFFFFu) != 0u) at_cur = atomicAdd(count, totals & 0xFFFFu);
+            if ((totals >> 16) != 0u) at_far = atomicAdd(&sh.far_count, totals >> 16);
+          }
+          at_cur = __shfl_sync(0xFFFFFFFFu, at_cur, 0) + (packed & 0xFFFFu) - nc;
+          at_far = __shfl_sync(0xFFFFFFFFu, at_far, 0) + (packed >> 16) - nfar;
+#pragma unroll
+          for (int d = 0; d < 10; ++d) {
+            if (cur_mask & (1u << d)) nxt[at_cur++] = ne[d];
+            if (far_mask & (1u << d)) far[at_far++] = ne[d];
+          }
+        }
+        fsync<G>(barrier_id);
+        n = *count;
+        uint32_t* t = cur;
+        cur = nxt;
+        nxt = t;
+      }
+    }
+    // expansions summed over the group (reported in the row_steps field)
+    expanded = __reduce_add_sync(0xFFFFFFFFu, expanded);
+    if constexpr (G > 1) {
+      fsync<G>(barrier_id);
+      if (lane == 0) sh.sums[g] = expanded;
+      fsync<G>(barrier_id);
+      expanded = __reduce_add_sync(0xFFFFFFFFu, lane < G ? sh.sums[lane] : 0u);
+    }
+
+    // ------------------------- result + canonical walk -------------------------
+    if (g == 0) {
+      apgar_b200_lattice_result res{};
+      res.cost = APGAR_B200_UNREACHABLE;
+      res.completion = completion;
+      res.sweeps = rounds;
+      res.row_steps = expanded;
+      res.row_stores = levels;
+      if (completion == APGAR_B200_COMPLETION_REACHED) {
+        const uint32_t goal = label_of(words + cell_index(win, win.gl, win.gx, win.gy));
+        if (goal >= kLabelInf) {
+          res.completion = APGAR_B200_COMPLETION_DISCONNECTED;
+        } else {
+          res.cost = goal;
+          const uint32_t min_move = min(orth, min(diag, via));
+          const unsigned long long bound = goal / min_move + 1ull;
+          unsigned long long base = 0;
+          if (lane == 0) base = atomicAdd(p.arena_cursor, bound);
+          base = __shfl_sync(0xFFFFFFFFu, base, 0);
+          if (base + bound > p.path_arena_capacity) {
+            res.completion = APGAR_B200_COMPLETION_REJECTED;
+            res.cost = APGAR_B200_UNREACHABLE;
+          } else {
+            int cl = win.gl, cx = win.gx, cy = win.gy;
+            uint32_t here = goal;
+            uint32_t len = 0;
+            bool ok = false;
+            while (len < bound) {
+              if (lane == 0) {
+                p.path_arena[base + len] = static_cast<uint32_t>(
+                    (static_cast<size_t>(cl) * lat.height + (win.y0 + cy)) * lat.width +
+                    (win.x0 + cx));
+              }
+              ++len;
+              if (cl == sl && cx == sx && cy == sy) {
+                ok = true;
+                break;
+              }
+              // lanes 0..7: planar predecessors by incoming heading; 8, 9: vias
+              bool cand = false;
+              int pl = cl, px = cx, py = cy;
+              uint32_t pd = kLabelInf;
+              if (lane < 8) {
+                px = cx - fdx(lane);
+                py = cy - fdy(lane);
+                bool legal = cell_free_w(lat, win, cl, px, py);
+                if (legal && (lane & 1)) {
+                  legal = cell_free_w(lat, win, cl, cx, py) && cell_free_w(lat, win, cl, px, cy);
+                }
+                if (legal) {
+                  pd = label_of(words + cell_index(win, cl, px, py));
+                  cand = pd < kLabelInf && pd + ((lane & 1) ? diag : orth) == here;
+                }
+              } else if (lane == 8 || lane == 9) {
+                pl = (lane == 8) ? cl - 1 : cl + 1;
+                const int lower = (lane == 8) ? cl - 1 : cl;
+                if (pl >= 0 && pl < lat.layers && cell_free_w(lat, win, pl, cx, cy) &&
+                    via_allowed(lat, win, lower, cx, cy)) {
+                  pd = label_of(words + cell_index(win, pl, cx, cy));
+                  cand = pd < kLabelInf && pd + via == here;
+                }
+              }
+              const unsigned ballot = __ballot_sync(0xFFFFFFFFu, cand);
+              if (ballot == 0u) break;
+              const int hsel = __ffs(ballot) - 1;
+              cl = __shfl_sync(0xFFFFFFFFu, pl, hsel);
+              cx = __shfl_sync(0xFFFFFFFFu, px, hsel);
+              cy = __shfl_sync(0xFFFFFFFFu, py, hsel);
+              here = __shfl_sync(0xFFFFFFFFu, pd, hsel);
+            }
+            if (ok) {
+              res.path_len = len;
+              res.arena_offset = base;
+            } else {
+              res.completion = APGAR_B200_COMPLETION_REJECTED;
+              res.cost = APGAR_B200_UNREACHABLE;
+            }
+          }
+        }
+      }
+      if (lane == 0) p.results[plan.net] = res;
+    }
+    // the group's shared slots are reused by its next net
+    fsync<G>(barrier_id);
+  }
+}
+
+template <int G>
+cudaError_t launch_frontier_g(const FrontierLaunch& launch, int sm_count, cudaStream_t stream) {
+  constexpr int kGroups = frontier_groups_per_block(G);
+  int per_sm = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &per_sm, lattice_frontier_kernel<G>, kGroups * G * 32, 0);
+  if (e != cudaSuccess) return e;
+  const unsigned needed = (launch.plan_count + kGroups - 1) / kGroups;
+  const unsigned resident = static_cast<unsigned>(max(1, per_sm) * max(1, sm_count));
+  const unsigned grid = needed < resident ? needed : resident;
+  lattice_frontier_kernel<G><<<grid, kGroups * G * 32, 0, stream>>>(launch);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_lattice_frontier(int warps_per_net, const FrontierLaunch& launch, int sm_count,
+                                    cudaStream_t stream) {
+  if (launch.plan_count == 0) return cudaSuccess;
+  switch (warps_per_net) {
+    case 1: return launch_frontier_g<1>(launch, sm_count, stream);
+    case 2: return launch_frontier_g<2>(launch, sm_count, stream);
+    case 4: return launch_frontier_g<4>(launch, sm_count, stream);
+    case 8: return launch_frontier_g<8>(launch, sm_count, stream);
+    case 16: return launch_frontier_g<16>(launch, sm_count, stream);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+}  // namespace apgar_b200

@@ -26,6 +26,8 @@ cudaError_t launch_lattice_sweep(int layers, int warps_per_net, const SweepLaunc
 cudaError_t launch_accumulate_cells(const apgar_b200_lattice_result* results, uint32_t count,
                                     const uint32_t* paths, uint32_t* usage, uint64_t cell_count,
                                     int sm_count, cudaStream_t stream);
+cudaError_t launch_lattice_frontier(int warps_per_net, const FrontierLaunch& launch, int sm_count,
+                                    cudaStream_t stream);
 cudaError_t launch_lattice_pack(apgar_b200_lattice_result* results, uint32_t count,
                                 unsigned long long* total, const uint32_t* arena, uint32_t* paths,
                                 int sm_count, cudaStream_t stream);
@@ -52,7 +54,9 @@ struct PlanObject {
   int device = -1;
   int sm_count = 0;
   uint32_t count = 0;
-  uint32_t max_sweeps = 0;
+  uint32_t max_sweeps = 0;  // sweeps (SWEEP) or rounds (FRONTIER)
+  uint32_t generator = APGAR_B200_LATTICE_SWEEP;
+  uint32_t bucket_width = 0;
   uint32_t* cancel_host = nullptr;  // pinned, mapped; polled by the kernels
   uint32_t* cancel_dev = nullptr;
   std::vector<ClassRange> classes;
@@ -63,7 +67,11 @@ struct PlanObject {
   DeviceBuffer<apgar_b200_lattice_result> results;
   DeviceBuffer<uint32_t> arena;
   DeviceBuffer<uint32_t> paths;
-  DeviceBuffer<unsigned long long> counters;  // [0] arena cursor, [1] packed total
+  DeviceBuffer<unsigned long long> words;  // FRONTIER: label | ~round stamp per cell
+  DeviceBuffer<uint32_t> far_bits;         // FRONTIER: one bit per cell (in the far list)
+  DeviceBuffer<uint32_t> lists;            // FRONTIER: three queue lists per net
+  // [0] arena cursor, [1] packed total, [2 + class] work-stealing cursors
+  DeviceBuffer<unsigned long long> counters;
   uint64_t label_cells = 0;
   uint64_t arena_capacity = 0;
   cudaStream_t class_streams[kClassCount] = {};
@@ -83,7 +91,7 @@ struct PlanObject {
 
   uint64_t workspace_bytes() const {
     return nets.bytes() + plans.bytes() + dist_pool.bytes() + results.bytes() + arena.bytes() +
-           paths.bytes() + counters.bytes();
+           paths.bytes() + counters.bytes() + words.bytes() + far_bits.bytes() + lists.bytes();
   }
 };
 
@@ -114,6 +122,15 @@ int class_for_width(uint32_t width, int layers) {
     if (per_warp * static_cast<uint32_t>(kGroupSizes[i]) >= width) return i;
   }
   return -1;
+}
+
+// Frontier width class (index into kGroupSizes) from the window's cell count.
+int frontier_class(uint64_t cells) {
+  if (cells <= (1ull << 17)) return 0;
+  if (cells <= (1ull << 19)) return 1;
+  if (cells <= (1ull << 21)) return 2;
+  if (cells <= (1ull << 23)) return 3;
+  return 4;
 }
 
 // Guard-padded sweep planes from row-major bit planes `in`
@@ -167,12 +184,19 @@ std::vector<uint32_t> sweep_planes(const uint32_t* in, int planes, int height, i
 
 // Builds (or rebuilds into existing buffers) a plan for `nets`.
 int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint32_t count,
-               uint32_t max_sweeps, PlanObject* plan) {
+               uint32_t max_sweeps, PlanObject* plan,
+               uint32_t generator = APGAR_B200_LATTICE_SWEEP, uint32_t bucket_width = 0) {
   const LatticeDeviceView& v = lat->view;
+  const bool frontier = generator == APGAR_B200_LATTICE_FRONTIER;
   plan->lattice = lat;
   plan->device = lat->device;
   plan->count = count;
   plan->max_sweeps = max_sweeps;
+  plan->generator = generator;
+  // Level width: at least twice the largest move, so that every deferred cell
+  // falls in the next level (the frontier kernel relies on it: a cell that
+  // left the far list never returns to it, so its far bit needs no clearing).
+  plan->bucket_width = std::max(bucket_width, 2u * std::max(v.orth, std::max(v.diag, v.via)));
   APGAR_B200_CUDA("cudaDeviceGetAttribute",
                   cudaDeviceGetAttribute(&plan->sm_count, cudaDevAttrMultiProcessorCount,
                                          lat->device));
@@ -197,6 +221,12 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
     if (!in_lattice) continue;
     const uint64_t cells = static_cast<uint64_t>(v.layers) * n.win_w * n.win_h;
     if (cells * max_move >= kLabelInf) continue;  // uint32 cost domain not provable
+    if (frontier) {
+      // packed queue entries hold x and y in 14 bits each
+      if (n.win_w > 16384u || n.win_h > 16384u) continue;
+      members[frontier_class(cells)].push_back(i);
+      continue;
+    }
     const uint32_t frame_width = std::max(n.win_w, n.win_h);
     const uint32_t frame_rows = std::min(n.win_w, n.win_h);
     const int ci = class_for_width(frame_width, v.layers);
@@ -227,18 +257,29 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
       const apgar_b200_lattice_net& n = host_nets[i];
       NetPlan np{};
       np.net = i;
-      np.transposed = n.win_h > n.win_w ? 1u : 0u;
-      np.rows = np.transposed ? n.win_w : n.win_h;
-      np.width = np.transposed ? n.win_h : n.win_w;
-      np.pitch = (np.width + 3u) & ~3u;
-      np.dist_offset = dist_cells;
-      dist_cells += static_cast<uint64_t>(v.layers) * np.rows * np.pitch;
+      if (frontier) {
+        // window layout [layer][y][x]; slabs padded to 128 cells so that a
+        // net's far-bit words start 16-byte aligned
+        np.transposed = 0;
+        np.rows = n.win_h;
+        np.width = n.win_w;
+        np.pitch = n.win_w;
+        np.dist_offset = dist_cells;
+        dist_cells += (static_cast<uint64_t>(v.layers) * n.win_w * n.win_h + 127ull) & ~127ull;
+      } else {
+        np.transposed = n.win_h > n.win_w ? 1u : 0u;
+        np.rows = np.transposed ? n.win_w : n.win_h;
+        np.width = np.transposed ? n.win_h : n.win_w;
+        np.pitch = (np.width + 3u) & ~3u;
+        np.dist_offset = dist_cells;
+        dist_cells += static_cast<uint64_t>(v.layers) * np.rows * np.pitch;
+      }
       arena_cells += 8ull * (n.win_w + n.win_h) + 64ull * v.layers;
       range.max_rows = std::max(range.max_rows, static_cast<int>(np.rows));
       plans.push_back(np);
     }
-    if (lattice_sweep_smem_bytes(v.layers, range.warps_per_net, range.max_rows) >
-        kMaxSmemPerBlock) {
+    if (!frontier && lattice_sweep_smem_bytes(v.layers, range.warps_per_net, range.max_rows) >
+                         kMaxSmemPerBlock) {
       return set_error(APGAR_B200_UNSUPPORTED, "window too tall for the shared-memory row map");
     }
     plan->classes.push_back(range);
@@ -248,11 +289,17 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
 
   APGAR_B200_CUDA("cudaMalloc(nets)", plan->nets.ensure(std::max<uint32_t>(count, 1)));
   APGAR_B200_CUDA("cudaMalloc(plans)", plan->plans.ensure(std::max<size_t>(plans.size(), 1)));
-  APGAR_B200_CUDA("cudaMalloc(label slabs)", plan->dist_pool.ensure(std::max<uint64_t>(dist_cells, 4)));
+  if (frontier) {
+    APGAR_B200_CUDA("cudaMalloc(label words)", plan->words.ensure(std::max<uint64_t>(dist_cells, 128)));
+    APGAR_B200_CUDA("cudaMalloc(far bits)", plan->far_bits.ensure(std::max<uint64_t>(dist_cells / 32, 4)));
+    APGAR_B200_CUDA("cudaMalloc(queue lists)", plan->lists.ensure(std::max<uint64_t>(3 * dist_cells, 3)));
+  } else {
+    APGAR_B200_CUDA("cudaMalloc(label slabs)", plan->dist_pool.ensure(std::max<uint64_t>(dist_cells, 4)));
+  }
   APGAR_B200_CUDA("cudaMalloc(results)", plan->results.ensure(std::max<uint32_t>(count, 1)));
   APGAR_B200_CUDA("cudaMalloc(path arena)", plan->arena.ensure(plan->arena_capacity));
   APGAR_B200_CUDA("cudaMalloc(paths)", plan->paths.ensure(plan->arena_capacity));
-  APGAR_B200_CUDA("cudaMalloc(counters)", plan->counters.ensure(2));
+  APGAR_B200_CUDA("cudaMalloc(counters)", plan->counters.ensure(2 + kClassCount));
   if (count > 0) {
     APGAR_B200_CUDA("cudaMemcpy(nets)",
                     cudaMemcpy(plan->nets.get(), host_nets, count * sizeof(apgar_b200_lattice_net),
@@ -294,8 +341,22 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
 int execute_plan(PlanObject* plan, cudaStream_t stream) {
   if (int rc = check_device(plan->device); rc != APGAR_B200_OK) return rc;
   APGAR_B200_CUDA("cudaMemsetAsync(counters)",
-                  cudaMemsetAsync(plan->counters.get(), 0, 2 * sizeof(unsigned long long), stream));
+                  cudaMemsetAsync(plan->counters.get(), 0,
+                                  (2 + kClassCount) * sizeof(unsigned long long), stream));
   const LatticeDeviceView& v = plan->lattice->view;
+  FrontierLaunch fbase{};
+  fbase.lat = v;
+  fbase.nets = plan->nets.get();
+  fbase.max_rounds = plan->max_sweeps;
+  fbase.bucket_width = plan->bucket_width;
+  fbase.words = plan->words.get();
+  fbase.far_bits = plan->far_bits.get();
+  fbase.lists = plan->lists.get();
+  fbase.results = plan->results.get();
+  fbase.path_arena = plan->arena.get();
+  fbase.path_arena_capacity = plan->arena_capacity;
+  fbase.arena_cursor = plan->counters.get();
+  fbase.cancel = plan->cancel_dev;
   SweepLaunch base{};
   base.lat = v;
   base.nets = plan->nets.get();
@@ -318,8 +379,17 @@ int execute_plan(PlanObject* plan, cudaStream_t stream) {
       s = plan->class_streams[k];
       APGAR_B200_CUDA("cudaStreamWaitEvent", cudaStreamWaitEvent(s, plan->fork, 0));
     }
-    APGAR_B200_CUDA("lattice sweep launch",
-                    launch_lattice_sweep(v.layers, c.warps_per_net, launch, c.max_rows, s));
+    if (plan->generator == APGAR_B200_LATTICE_FRONTIER) {
+      FrontierLaunch fl = fbase;
+      fl.plans = plan->plans.get() + c.begin;
+      fl.plan_count = c.count;
+      fl.next_plan = reinterpret_cast<unsigned int*>(plan->counters.get() + 2 + k);
+      APGAR_B200_CUDA("lattice frontier launch",
+                      launch_lattice_frontier(c.warps_per_net, fl, plan->sm_count, s));
+    } else {
+      APGAR_B200_CUDA("lattice sweep launch",
+                      launch_lattice_sweep(v.layers, c.warps_per_net, launch, c.max_rows, s));
+    }
     if (fan_out) {
       APGAR_B200_CUDA("cudaEventRecord(join)", cudaEventRecord(plan->joins[k], s));
       APGAR_B200_CUDA("cudaStreamWaitEvent", cudaStreamWaitEvent(stream, plan->joins[k], 0));
@@ -518,27 +588,48 @@ extern "C" int apgar_b200_lattice_plan_release(void* plan) {
   return APGAR_B200_OK;
 }
 
-extern "C" int apgar_b200_lattice_route(void* lattice, const apgar_b200_lattice_net* nets,
-                                        uint32_t count, uint32_t max_sweeps,
-                                        const volatile uint32_t* cancel,
-                                        apgar_b200_lattice_result* results, uint32_t* paths,
-                                        uint64_t path_capacity, uint64_t* path_total) {
-  if (lattice == nullptr || (count > 0 && nets == nullptr) || results == nullptr ||
-      max_sweeps == 0 || max_sweeps > 30000) {
+namespace apgar_b200 {
+namespace {
+
+int check_options(const apgar_b200_lattice_options& o) {
+  if (o.generator == APGAR_B200_LATTICE_SWEEP) {
+    if (o.max_iterations == 0 || o.max_iterations > 30000) {
+      return set_error(APGAR_B200_INTERNAL_INVARIANT, "sweep budget must be 1..30000 sweeps");
+    }
+    return APGAR_B200_OK;
+  }
+  if (o.generator == APGAR_B200_LATTICE_FRONTIER) {
+    if (o.max_iterations == 0 || o.max_iterations > 0x7FFFFFFFu) {
+      return set_error(APGAR_B200_INTERNAL_INVARIANT, "frontier budget must be 1..2^31-1 rounds");
+    }
+    return APGAR_B200_OK;
+  }
+  return set_error(APGAR_B200_UNSUPPORTED, "unknown lattice generator");
+}
+
+int route_impl(void* lattice, const apgar_b200_lattice_net* nets, uint32_t count,
+               const apgar_b200_lattice_options& o, const volatile uint32_t* cancel,
+               apgar_b200_lattice_result* results, uint32_t* paths, uint64_t path_capacity,
+               uint64_t* path_total) {
+  if (lattice == nullptr || (count > 0 && nets == nullptr) || results == nullptr) {
     return set_error(APGAR_B200_INTERNAL_INVARIANT, "lattice route received invalid arguments");
   }
+  if (int rc = check_options(o); rc != APGAR_B200_OK) return rc;
   auto* lat = static_cast<LatticeObject*>(lattice);
   if (int rc = check_device(lat->device); rc != APGAR_B200_OK) return rc;
   try {
     std::scoped_lock lock(lat->route_mutex);
     if (lat->route_plan == nullptr) lat->route_plan = std::make_unique<PlanObject>();
     PlanObject* plan = lat->route_plan.get();
-    if (int rc = build_plan(lat, nets, count, max_sweeps, plan); rc != APGAR_B200_OK) return rc;
+    if (int rc = build_plan(lat, nets, count, o.max_iterations, plan, o.generator, o.bucket_width);
+        rc != APGAR_B200_OK) {
+      return rc;
+    }
     *reinterpret_cast<volatile uint32_t*>(plan->cancel_host) = 0u;
     if (int rc = execute_plan(plan, nullptr); rc != APGAR_B200_OK) return rc;
     // The caller's flag is sampled on the host while the batch runs and is
     // forwarded through the plan's own mapped flag, which the kernels poll
-    // between sweeps (the kernels never dereference caller memory).
+    // (the kernels never dereference caller memory).
     for (;;) {
       const cudaError_t q = cudaStreamQuery(nullptr);
       if (q == cudaSuccess) break;
@@ -553,6 +644,53 @@ extern "C" int apgar_b200_lattice_route(void* lattice, const apgar_b200_lattice_
     return rc;
   } catch (const std::bad_alloc&) {
     return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "host allocation failed during routing");
+  }
+}
+
+}  // namespace
+}  // namespace apgar_b200
+
+extern "C" int apgar_b200_lattice_route(void* lattice, const apgar_b200_lattice_net* nets,
+                                        uint32_t count, uint32_t max_sweeps,
+                                        const volatile uint32_t* cancel,
+                                        apgar_b200_lattice_result* results, uint32_t* paths,
+                                        uint64_t path_capacity, uint64_t* path_total) {
+  const apgar_b200_lattice_options o{APGAR_B200_LATTICE_SWEEP, max_sweeps, 0, 0};
+  return route_impl(lattice, nets, count, o, cancel, results, paths, path_capacity, path_total);
+}
+
+extern "C" int apgar_b200_lattice_route_ex(void* lattice, const apgar_b200_lattice_net* nets,
+                                           uint32_t count, const apgar_b200_lattice_options* options,
+                                           const volatile uint32_t* cancel,
+                                           apgar_b200_lattice_result* results, uint32_t* paths,
+                                           uint64_t path_capacity, uint64_t* path_total) {
+  if (options == nullptr) return set_error(APGAR_B200_INTERNAL_INVARIANT, "null lattice options");
+  return route_impl(lattice, nets, count, *options, cancel, results, paths, path_capacity,
+                    path_total);
+}
+
+extern "C" int apgar_b200_lattice_plan_ex(void* lattice, const apgar_b200_lattice_net* nets,
+                                          uint32_t count, const apgar_b200_lattice_options* options,
+                                          void** out_plan) {
+  if (lattice == nullptr || out_plan == nullptr || options == nullptr ||
+      (count > 0 && nets == nullptr)) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "lattice plan received invalid arguments");
+  }
+  if (int rc = check_options(*options); rc != APGAR_B200_OK) return rc;
+  auto* lat = static_cast<LatticeObject*>(lattice);
+  if (int rc = check_device(lat->device); rc != APGAR_B200_OK) return rc;
+  try {
+    auto plan = std::make_unique<PlanObject>();
+    if (int rc = build_plan(lat, nets, count, options->max_iterations, plan.get(),
+                            options->generator, options->bucket_width);
+        rc != APGAR_B200_OK) {
+      return rc;
+    }
+    *out_plan = plan.release();
+    clear_error();
+    return APGAR_B200_OK;
+  } catch (const std::bad_alloc&) {
+    return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "host allocation failed during planning");
   }
 }
 

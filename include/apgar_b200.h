@@ -366,6 +366,39 @@ typedef struct apgar_b200_plan_info {
   uint64_t path_arena_capacity; /* cells */
 } apgar_b200_plan_info;
 APGAR_B200_API int apgar_b200_lattice_plan_info(void* plan, apgar_b200_plan_info* out);
+
+/* Search generators of lattice mode, the counterpart of the reference's
+ * PlanarGenerator choice (include/apgar/gpu/planar_router.h:56-100).  Both
+ * give the same costs and the same canonical reverse paths.
+ *  SWEEP:    alternating row sweeps to the full-window fixed point.  Result
+ *            counters: sweeps, row_steps, row_stores, row_loads.
+ *  FRONTIER: bucketed, label-correcting A* (key = label + octile-plus-via
+ *            bound) in key levels of `bucket_width`.  One warp group per net,
+ *            persistent and work-stealing, largest windows first.  It stops
+ *            once every cell with key <= the goal label is final.  Result
+ *            counters: sweeps = rounds, row_steps = cell expansions,
+ *            row_stores = key levels opened, row_loads = 0.  Rounds and
+ *            expansions depend on the order of concurrent relaxations;
+ *            costs and paths do not. */
+#define APGAR_B200_LATTICE_SWEEP 0u
+#define APGAR_B200_LATTICE_FRONTIER 1u
+typedef struct apgar_b200_lattice_options {
+  uint32_t generator;      /* APGAR_B200_LATTICE_* */
+  uint32_t max_iterations; /* sweeps (SWEEP, 1..30000) or rounds (FRONTIER, 1..2^31-1) */
+  uint32_t bucket_width;   /* FRONTIER: key width of a level; raised to at least twice
+                              the largest move cost (0 = that minimum) */
+  uint32_t reserved;
+} apgar_b200_lattice_options;
+
+/* apgar_b200_lattice_plan / apgar_b200_lattice_route with a generator choice. */
+APGAR_B200_API int apgar_b200_lattice_plan_ex(void* lattice, const apgar_b200_lattice_net* nets,
+                               uint32_t count, const apgar_b200_lattice_options* options,
+                               void** out_plan);
+APGAR_B200_API int apgar_b200_lattice_route_ex(void* lattice, const apgar_b200_lattice_net* nets,
+                                uint32_t count, const apgar_b200_lattice_options* options,
+                                const volatile uint32_t* cancel,
+                                apgar_b200_lattice_result* results, uint32_t* paths,
+                                uint64_t path_capacity, uint64_t* path_total);
 APGAR_B200_API int apgar_b200_lattice_plan_release(void* plan);
 
 /* ======================= C. congestion prices ======================= */
