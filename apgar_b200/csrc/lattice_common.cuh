@@ -65,9 +65,8 @@ struct SweepLaunch {
 };
 
 // One width class of the frontier form (lattice_frontier.cu).  A net's
-// label words (label << 32 | ~round stamp, window layout [layer][y][x]) start
-// at word plan.dist_offset of `words`, its far-list bits at word
-// dist_offset / 32 of `far_bits`, and its three queue lists at entry
+// label words (label << 32 | ~list stamp, window layout [layer][y][x]) start
+// at word plan.dist_offset of `words`, and its three queue lists at entry
 // 3 * dist_offset of `lists`; dist_offset is a multiple of 128 cells.
 struct FrontierLaunch {
   LatticeDeviceView lat;
@@ -77,7 +76,6 @@ struct FrontierLaunch {
   uint32_t max_rounds;
   uint32_t bucket_width;
   unsigned long long* words;
-  uint32_t* far_bits;
   uint32_t* lists;
   apgar_b200_lattice_result* results;
   uint32_t* path_arena;

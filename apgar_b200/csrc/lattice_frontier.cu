@@ -35,11 +35,13 @@
 // The heuristic follows the reference's octile bound (src/routing/
 // cpu_astar.cc:176-190), plus |dl| * via for the layer difference.
 //
-// Each cell's 64-bit word holds its label in the high half.  The low half
-// holds ~s, with s the round whose list it last joined; 0 when deferred.  One
-// 64-bit atomicMin both lowers the label and reports whether the cell is
-// already in the next round's list.  A per-cell bit keeps a cell at most once
-// in the far list.  So no list holds more entries than the window has cells.
+// Each cell's 64-bit word holds its label in the high half and, in the low
+// half, ~s for the list it last joined: s = r + 1 for the list of round r,
+// s = 2^31 | k for the far list of level k.  One 64-bit atomicMin both lowers
+// the label and reports whether the cell already sits in the list it would
+// join (a lowered cell joins the current level's next list or the far list,
+// never both in one level, because its key only falls).  So no list ever
+// holds more entries than the window has cells.
 // Queue entries are packed cells (layer << 28 | y << 14 | x, window-local).
 // Appends take one packed warp scan and one shared atomic per warp and list.
 #include <cuda_runtime.h>
@@ -51,8 +53,9 @@
 namespace apgar_b200 {
 namespace {
 
-constexpr int kCancelPollRounds = 32;
-constexpr uint64_t kWordInf = (static_cast<uint64_t>(kLabelInf) << 32) | 0xFFFFFFFFull;
+// The cancel flag lives in host-mapped memory: every read crosses the bus, so
+// each group reads it at the start of a net and then every 256 rounds.
+constexpr int kCancelPollRounds = 256;
 
 __host__ __device__ constexpr int frontier_groups_per_block(int G) { return G >= 4 ? 1 : 4 / G; }
 
@@ -138,46 +141,63 @@ __device__ __forceinline__ void fsync(int barrier_id) {
   }
 }
 
+// Blocked bits of lattice columns X-1..X+1 (bits 0..2) in a guard-padded
+// sweep-plane row (guard words read as blocked, so X = 0 needs no test).
+__device__ __forceinline__ uint32_t blocked3(const uint32_t* row, int X) {
+  const uint32_t q = static_cast<uint32_t>(X + 31);  // bit X-1, counted from the guard word
+  return __funnelshift_r(__ldg(row + (q >> 5)), __ldg(row + (q >> 5) + 1), q & 31u) & 7u;
+}
+
 // Expands one queued cell.  The memory operations are issued move-parallel in
-// waves: the cell's label, mask bits and all in-window neighbour labels
-// together, then the 64-bit atomicMins, then far-bit atomics for the lowered
-// cells that leave the level.  So one cell costs a few L2 round trips, not a
-// few per move.  Lowered neighbours that join the next round's list are
-// flagged in cur_mask, those that join the far list in far_mask; ne[d] holds
-// the packed cell.
+// two waves: the cell's label, mask bits and all in-window neighbour labels
+// together, then the 64-bit atomicMins.  Lowered neighbours whose list stamp
+// this call set are flagged in cur_mask (next round's list) or far_mask (far
+// list); ne[d] holds the packed cell.
 __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const Window& win,
-                                            uint32_t e, unsigned long long* words,
-                                            uint32_t* farbit, uint32_t thr, uint32_t next_stamp,
-                                            uint32_t (&ne)[10], uint32_t& cur_mask,
-                                            uint32_t& far_mask) {
+                                            uint32_t e, unsigned long long* words, uint32_t thr,
+                                            uint32_t cur_low, uint32_t far_low, uint32_t (&ne)[10],
+                                            uint32_t& cur_mask, uint32_t& far_mask) {
   const int l = static_cast<int>(e >> 28), y = static_cast<int>((e >> 14) & 0x3FFFu),
             x = static_cast<int>(e & 0x3FFFu);
-  const uint32_t here = cell_index(win, l, x, y);
-  const uint32_t plane = static_cast<uint32_t>(win.w) * static_cast<uint32_t>(win.h);
-  uint32_t ni[10];
-  uint32_t inside = 0;  // neighbour lies in the window (its word may be read)
-#pragma unroll
-  for (int d = 0; d < 8; ++d) {
-    const int nx = x + fdx(d), ny = y + fdy(d);
-    inside |= (nx >= 0 && nx < win.w && ny >= 0 && ny < win.h) ? (1u << d) : 0u;
-    ni[d] = here + static_cast<uint32_t>(fdy(d) * win.w + fdx(d));
-  }
-  inside |= l > 0 ? (1u << 8) : 0u;
-  inside |= l + 1 < lat.layers ? (1u << 9) : 0u;
-  ni[8] = here - plane;
-  ni[9] = here + plane;
+  const uint32_t w = static_cast<uint32_t>(win.w);
+  const uint32_t plane = w * static_cast<uint32_t>(win.h);
+  const uint32_t here = (static_cast<uint32_t>(l) * static_cast<uint32_t>(win.h) +
+                         static_cast<uint32_t>(y)) * w + static_cast<uint32_t>(x);
+  const bool xl = x > 0, xr = x + 1 < win.w, yd = y > 0, yu = y + 1 < win.h;
+  const bool ld = l > 0, lu = l + 1 < lat.layers;
+  const uint32_t inside = (xr ? 1u : 0u) | ((xr && yu) ? 2u : 0u) | (yu ? 4u : 0u) |
+                          ((xl && yu) ? 8u : 0u) | (xl ? 16u : 0u) | ((xl && yd) ? 32u : 0u) |
+                          (yd ? 64u : 0u) | ((xr && yd) ? 128u : 0u) | (ld ? 256u : 0u) |
+                          (lu ? 512u : 0u);
   // wave 1: own label, neighbour labels, mask bits
-  const uint32_t gv = label_of(words + here);
+  const uint32_t gv = static_cast<uint32_t>(__ldcg(words + here) >> 32);
   uint32_t seen[10];
 #pragma unroll
-  for (int d = 0; d < 10; ++d) seen[d] = (inside & (1u << d)) ? label_of(words + ni[d]) : 0u;
-  const uint32_t r0 = free3(lat, win, l, x, y - 1);
-  const uint32_t r1 = free3(lat, win, l, x, y);
-  const uint32_t r2 = free3(lat, win, l, x, y + 1);
-  const bool down_ok = l > 0 && cell_free_w(lat, win, l - 1, x, y) && via_allowed(lat, win, l - 1, x, y);
-  const bool up_ok = l + 1 < lat.layers && cell_free_w(lat, win, l + 1, x, y) &&
-                     via_allowed(lat, win, l, x, y);
-  uint32_t legal = (down_ok ? (1u << 8) : 0u) | (up_ok ? (1u << 9) : 0u);
+  for (int d = 0; d < 10; ++d) {
+    const uint32_t ni = d < 8 ? here + static_cast<uint32_t>(fdy(d)) * w + static_cast<uint32_t>(fdx(d))
+                              : (d == 8 ? here - plane : here + plane);
+    seen[d] = (inside & (1u << d)) ? static_cast<uint32_t>(__ldcg(words + ni) >> 32) : 0u;
+  }
+  const int X = win.x0 + x, Y = win.y0 + y;
+  const size_t stride = static_cast<size_t>(lat.words) + 2;
+  const uint32_t* rowc = lat.sweep_rows + (static_cast<size_t>(l) * lat.height + Y) * stride;
+  const uint32_t edge = (xl ? 1u : 0u) | 2u | (xr ? 4u : 0u);
+  const uint32_t r1 = ~blocked3(rowc, X) & edge;
+  const uint32_t r0 = yd ? ~blocked3(rowc - stride, X) & edge : 0u;
+  const uint32_t r2 = yu ? ~blocked3(rowc + stride, X) & edge : 0u;
+  const size_t layer_stride = static_cast<size_t>(lat.height) * stride;
+  const uint32_t bit = 1u << (X & 31);
+  const uint32_t wi = static_cast<uint32_t>(X >> 5) + 1u;
+  bool down_ok = ld && (__ldg(rowc - layer_stride + wi) & bit) == 0u;
+  bool up_ok = lu && (__ldg(rowc + layer_stride + wi) & bit) == 0u;
+  if (lat.via_ok != nullptr) {
+    // via plane of layer pair (k, k + 1) is plane k
+    const size_t col = static_cast<size_t>(Y) * lat.words + (X >> 5);
+    const size_t via_layer = static_cast<size_t>(lat.height) * lat.words;
+    if (down_ok) down_ok = (__ldg(lat.via_ok + (l - 1) * via_layer + col) & bit) != 0u;
+    if (up_ok) up_ok = (__ldg(lat.via_ok + l * via_layer + col) & bit) != 0u;
+  }
+  uint32_t legal = (down_ok ? 256u : 0u) | (up_ok ? 512u : 0u);
 #pragma unroll
   for (int d = 0; d < 8; ++d) {
     const int dx = fdx(d), dy = fdy(d);
@@ -186,47 +206,57 @@ __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const 
     if (d & 1) ok = ok && ((r1 >> (1 + dx)) & 1u) && ((row >> 1) & 1u);
     legal |= ok ? (1u << d) : 0u;
   }
-  // wave 2: lower the labels (the low half carries the list membership)
-  const uint32_t cur_low = 0xFFFFFFFFu - next_stamp;
+  // heuristic parts: |column - goal| and |row - goal| for the 3x3 neighbourhood
+  const int ax[3] = {abs(x - 1 - win.gx), abs(x - win.gx), abs(x + 1 - win.gx)};
+  const int ay[3] = {abs(y - 1 - win.gy), abs(y - win.gy), abs(y + 1 - win.gy)};
+  const uint32_t dstep = lat.diag >= lat.orth ? min(lat.diag, 2u * lat.orth) : lat.diag;
+  // wave 2: lower the labels (all atomics issued before any result is used);
+  // the low half records the list the cell joins
   uint32_t cand[10], low[10];
   unsigned long long old[10];
 #pragma unroll
   for (int d = 0; d < 10; ++d) {
     const uint32_t cost = d >= 8 ? lat.via : ((d & 1) ? lat.diag : lat.orth);
     cand[d] = gv + cost;
-    old[d] = ~0ull;
-    low[d] = 0xFFFFFFFFu;
+    low[d] = 0u;
+    old[d] = 0ull;
     if ((legal & (1u << d)) && cand[d] < seen[d]) {
+      const int dx = d < 8 ? fdx(d) : 0, dy = d < 8 ? fdy(d) : 0;
       const int nl = d == 8 ? l - 1 : (d == 9 ? l + 1 : l);
-      const int nx = d < 8 ? x + fdx(d) : x, ny = d < 8 ? y + fdy(d) : y;
-      ne[d] = pack_cell(nl, nx, ny);
-      low[d] = cand[d] + heuristic(lat, win, nl, nx, ny) < thr ? cur_low : 0xFFFFFFFFu;
-      old[d] = atomicMin(words + ni[d], (static_cast<unsigned long long>(cand[d]) << 32) | low[d]);
+      const uint32_t a = static_cast<uint32_t>(ax[1 + dx]), b = static_cast<uint32_t>(ay[1 + dy]);
+      const uint32_t lo = min(a, b), hi = max(a, b);
+      const uint32_t planar = lat.diag >= lat.orth ? lo * dstep + (hi - lo) * lat.orth : hi * dstep;
+      const uint32_t key = cand[d] + planar + static_cast<uint32_t>(abs(nl - win.gl)) * lat.via;
+      low[d] = key < thr ? cur_low : far_low;
+      const uint32_t ni = d < 8 ? here + static_cast<uint32_t>(dy) * w + static_cast<uint32_t>(dx)
+                                : (d == 8 ? here - plane : here + plane);
+      old[d] = atomicMin(words + ni, (static_cast<unsigned long long>(cand[d]) << 32) | low[d]);
     }
   }
-  // wave 3: queue membership of the lowered cells
   cur_mask = 0;
   far_mask = 0;
-  uint32_t far_try = 0;
 #pragma unroll
   for (int d = 0; d < 10; ++d) {
-    const bool lowered = old[d] != ~0ull && cand[d] < static_cast<uint32_t>(old[d] >> 32);
-    if (!lowered) continue;
-    if (low[d] == cur_low) {
-      cur_mask |= static_cast<uint32_t>(old[d]) != cur_low ? (1u << d) : 0u;
-    } else {
-      far_try |= 1u << d;
+    // old == 0 marks a move that was not attempted (label 0 is never lowered)
+    if (cand[d] < static_cast<uint32_t>(old[d] >> 32) && static_cast<uint32_t>(old[d]) != low[d]) {
+      const int dx = d < 8 ? fdx(d) : 0, dy = d < 8 ? fdy(d) : 0;
+      const int nl = d == 8 ? l - 1 : (d == 9 ? l + 1 : l);
+      ne[d] = pack_cell(nl, x + dx, y + dy);
+      if (low[d] == cur_low) {
+        cur_mask |= 1u << d;
+        // its expansion next round reads rows y-1 and y+1 and the adjacent
+        // layers: start those lines towards L2 now
+        const uint32_t ni = d < 8 ? here + static_cast<uint32_t>(dy) * w + static_cast<uint32_t>(dx)
+                                  : (d == 8 ? here - plane : here + plane);
+        const unsigned long long* c = words + ni;
+        if (y + dy > 0) asm volatile("prefetch.global.L2 [%0];" ::"l"(c - w));
+        if (y + dy + 1 < win.h) asm volatile("prefetch.global.L2 [%0];" ::"l"(c + w));
+        if (nl > 0) asm volatile("prefetch.global.L2 [%0];" ::"l"(c - plane));
+        if (nl + 1 < lat.layers) asm volatile("prefetch.global.L2 [%0];" ::"l"(c + plane));
+      } else {
+        far_mask |= 1u << d;
+      }
     }
-  }
-  uint32_t prior[10];
-#pragma unroll
-  for (int d = 0; d < 10; ++d) {
-    prior[d] = ~0u;
-    if (far_try & (1u << d)) prior[d] = atomicOr(farbit + (ni[d] >> 5), 1u << (ni[d] & 31));
-  }
-#pragma unroll
-  for (int d = 0; d < 10; ++d) {
-    if ((far_try & (1u << d)) && (prior[d] & (1u << (ni[d] & 31))) == 0u) far_mask |= 1u << d;
   }
 }
 
@@ -274,19 +304,15 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
     const uint32_t cells = static_cast<uint32_t>(lat.layers) * win.w * win.h;
     const uint32_t padded = (cells + 127u) & ~127u;
     unsigned long long* words = p.words + plan.dist_offset;
-    uint32_t* farbit = p.far_bits + plan.dist_offset / 32;
     uint32_t* list_a = p.lists + 3 * plan.dist_offset;
     uint32_t* list_b = list_a + cells;
     uint32_t* list_c = list_b + cells;
 
-    // clear the net's label words and far bits (16-byte stores over the
-    // padded slab)
+    // clear the net's label words (16-byte stores over the padded slab)
     {
       uint4* w4 = reinterpret_cast<uint4*>(words);
       const uint4 inf2 = make_uint4(0xFFFFFFFFu, kLabelInf, 0xFFFFFFFFu, kLabelInf);
       for (uint32_t i = tid; i < padded / 2; i += T) w4[i] = inf2;
-      uint4* f4 = reinterpret_cast<uint4*>(farbit);
-      for (uint32_t i = tid; i < padded / 128; i += T) f4[i] = make_uint4(0u, 0u, 0u, 0u);
     }
     const bool endpoints_free = cell_free_w(lat, win, sl, sx, sy) &&
                                 cell_free_w(lat, win, win.gl, win.gx, win.gy);
@@ -353,7 +379,8 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
           }
         }
         uint32_t* count = &sh.count[r % 3];
-        const uint32_t next_stamp = r + 2;
+        const uint32_t cur_low = 0xFFFFFFFFu - (r + 2);              // list of round r + 1
+        const uint32_t far_low = 0xFFFFFFFFu - (0x80000000u | levels);  // far list of this level
         for (uint32_t base = static_cast<uint32_t>(g) * 32u; base < n; base += T) {
           const uint32_t i = base + static_cast<uint32_t>(lane);
           const bool valid = i < n;
@@ -361,7 +388,7 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
           uint32_t ne[10];
           if (valid) {
             ++expanded;
-            expand_cell(lat, win, cur[i], words, farbit, thr, next_stamp, ne, cur_mask, far_mask);
+            expand_cell(lat, win, cur[i], words, thr, cur_low, far_low, ne, cur_mask, far_mask);
           }
           // one packed warp scan places both lists' entries
           const uint32_t nc = __popc(cur_mask), nfar = __popc(far_mask);

@@ -68,7 +68,6 @@ struct PlanObject {
   DeviceBuffer<uint32_t> arena;
   DeviceBuffer<uint32_t> paths;
   DeviceBuffer<unsigned long long> words;  // FRONTIER: label | ~round stamp per cell
-  DeviceBuffer<uint32_t> far_bits;         // FRONTIER: one bit per cell (in the far list)
   DeviceBuffer<uint32_t> lists;            // FRONTIER: three queue lists per net
   // [0] arena cursor, [1] packed total, [2 + class] work-stealing cursors
   DeviceBuffer<unsigned long long> counters;
@@ -91,7 +90,7 @@ struct PlanObject {
 
   uint64_t workspace_bytes() const {
     return nets.bytes() + plans.bytes() + dist_pool.bytes() + results.bytes() + arena.bytes() +
-           paths.bytes() + counters.bytes() + words.bytes() + far_bits.bytes() + lists.bytes();
+           paths.bytes() + counters.bytes() + words.bytes() + lists.bytes();
   }
 };
 
@@ -258,8 +257,7 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
       NetPlan np{};
       np.net = i;
       if (frontier) {
-        // window layout [layer][y][x]; slabs padded to 128 cells so that a
-        // net's far-bit words start 16-byte aligned
+        // window layout [layer][y][x]; slabs padded to 128 cells
         np.transposed = 0;
         np.rows = n.win_h;
         np.width = n.win_w;
@@ -291,7 +289,6 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
   APGAR_B200_CUDA("cudaMalloc(plans)", plan->plans.ensure(std::max<size_t>(plans.size(), 1)));
   if (frontier) {
     APGAR_B200_CUDA("cudaMalloc(label words)", plan->words.ensure(std::max<uint64_t>(dist_cells, 128)));
-    APGAR_B200_CUDA("cudaMalloc(far bits)", plan->far_bits.ensure(std::max<uint64_t>(dist_cells / 32, 4)));
     APGAR_B200_CUDA("cudaMalloc(queue lists)", plan->lists.ensure(std::max<uint64_t>(3 * dist_cells, 3)));
   } else {
     APGAR_B200_CUDA("cudaMalloc(label slabs)", plan->dist_pool.ensure(std::max<uint64_t>(dist_cells, 4)));
@@ -350,7 +347,6 @@ int execute_plan(PlanObject* plan, cudaStream_t stream) {
   fbase.max_rounds = plan->max_sweeps;
   fbase.bucket_width = plan->bucket_width;
   fbase.words = plan->words.get();
-  fbase.far_bits = plan->far_bits.get();
   fbase.lists = plan->lists.get();
   fbase.results = plan->results.get();
   fbase.path_arena = plan->arena.get();
@@ -599,8 +595,8 @@ int check_options(const apgar_b200_lattice_options& o) {
     return APGAR_B200_OK;
   }
   if (o.generator == APGAR_B200_LATTICE_FRONTIER) {
-    if (o.max_iterations == 0 || o.max_iterations > 0x7FFFFFFFu) {
-      return set_error(APGAR_B200_INTERNAL_INVARIANT, "frontier budget must be 1..2^31-1 rounds");
+    if (o.max_iterations == 0 || o.max_iterations > (1u << 30)) {
+      return set_error(APGAR_B200_INTERNAL_INVARIANT, "frontier budget must be 1..2^30 rounds");
     }
     return APGAR_B200_OK;
   }

@@ -384,7 +384,7 @@ APGAR_B200_API int apgar_b200_lattice_plan_info(void* plan, apgar_b200_plan_info
 #define APGAR_B200_LATTICE_FRONTIER 1u
 typedef struct apgar_b200_lattice_options {
   uint32_t generator;      /* APGAR_B200_LATTICE_* */
-  uint32_t max_iterations; /* sweeps (SWEEP, 1..30000) or rounds (FRONTIER, 1..2^31-1) */
+  uint32_t max_iterations; /* sweeps (SWEEP, 1..30000) or rounds (FRONTIER, 1..2^30) */
   uint32_t bucket_width;   /* FRONTIER: key width of a level; raised to at least twice
                               the largest move cost (0 = that minimum) */
   uint32_t reserved;
