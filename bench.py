@@ -7,9 +7,12 @@ GPU): 4 layers of 2048x2048 cells, 25% blocked (rectangles + pad keep-outs),
 in its bbox + 32 window with uint32 labels and bit-packed masks.  Synthetic,
 seeded inputs (no public dataset exists for this path).
 
-One step = one batched search of all nets of the batch (plain batched sweep:
-exact labels + canonical reverse paths for every net).  A net is certified when
-its search converged (reached or proved disconnected inside its window).
+One step = one batched search of all nets of the batch: exact labels on every
+cell the canonical reverse path needs, plus that path, for every net.  A net is
+certified when its search converged (reached or proved disconnected inside its
+window).  The headline form is the persistent work-stealing frontier search
+(bucketed A*); the plain batched sweep is measured beside it on the same nets
+and reported under "plain_sweep", with the ratio of the two.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -75,7 +78,7 @@ def load_peaks():
 
 def load_traffic():
     """DRAM bytes per sweep launch from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", "lattice_sweep_traffic.json")
+    path = os.path.join(ROOT, "profiles", "lattice_traffic.json")
     if os.path.exists(path):
         with open(path) as f:
             return json.load(f)
@@ -134,6 +137,14 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm) if sm else None,
                 "sm_max_mhz": max(smax) if smax else None,
                 "reasons": reasons, "samples": len(rows)}
+
+
+def frontier_bytes(results):
+    """Bytes the frontier expansions move: per expanded cell its queue entry
+    (4 B), its label word and the words of its 10 neighbours (11 x 8 B), plus
+    4 B per emitted path cell."""
+    exp = results["row_steps"].astype(np.float64).sum()
+    return exp * (4.0 + 11 * 8.0) + 4.0 * results["path_len"].astype(np.float64).sum()
 
 
 def certified(results):
@@ -230,8 +241,6 @@ def main():
         nets = synth.make_nets(lat, args.seed + 1000 + 7919 * rank, args.nets, hpwl_median=200.0,
                                hpwl_sigma=1.0)
     dev = apgar_b200.DeviceLattice(lat)
-    plan = dev.plan(nets)
-    info = plan.info()
     stream = torch.cuda.current_stream()
 
     def barrier():
@@ -239,35 +248,58 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    # ---------------- device-resident throughput (value) ----------------
-    for _ in range(max(args.warmup, 3)):
-        plan.execute(stream.cuda_stream)
-    barrier()
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    with ClockSampler(local) as clocks:
+    def max_over_ranks(ms):
+        if dist is None:
+            return ms
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(n):
+        if dist is None:
+            return n
+        c = torch.tensor([n], device="cuda", dtype=torch.int64)
+        dist.all_reduce(c)
+        return int(c.item())
+
+    def device_resident(generator, sample_clocks):
+        """K executions of a resident plan, CUDA events on torch's stream."""
+        plan = dev.plan(nets, generator=generator)
+        info = plan.info()
+        for _ in range(max(args.warmup, 3)):
+            plan.execute(stream.cuda_stream)
+        barrier()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+        sampler = ClockSampler(local) if sample_clocks else None
+        if sampler:
+            sampler.__enter__()
         barrier()
         for i in range(args.steps):
             starts[i].record(stream)
             plan.execute(stream.cuda_stream)
             ends[i].record(stream)
         barrier()
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = starts[0].elapsed_time(ends[-1])
-    results, paths = plan.readback()
-    cert = certified(results)
-    if dist is not None:
-        t = torch.tensor([total_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
-        c = torch.tensor([cert], device="cuda", dtype=torch.int64)
-        dist.all_reduce(c)
-        cert_all = int(c.item())
-    else:
-        cert_all = cert
-    value = cert_all * args.steps / (total_ms / 1000.0)
+        if sampler:
+            sampler.__exit__(None, None, None)
+        step_ms = [a.elapsed_time(b) for a, b in zip(starts, ends)]
+        total_ms = max_over_ranks(starts[0].elapsed_time(ends[-1]))
+        results, _ = plan.readback()
+        plan.close()
+        return dict(info=info, step_ms=step_ms, total_ms=total_ms, results=results,
+                    clocks=sampler.summary() if sampler else None)
+
+    # ---------------- device-resident throughput (value) ----------------
+    front = device_resident("frontier", sample_clocks=True)
+    sweep = device_resident("sweep", sample_clocks=False)
+    cert_all = sum_over_ranks(certified(front["results"]))
+    value = cert_all * args.steps / (front["total_ms"] / 1000.0)
+    sweep_value = sum_over_ranks(certified(sweep["results"])) * args.steps / (sweep["total_ms"] / 1000.0)
+    same = bool(np.array_equal(front["results"]["cost"], sweep["results"]["cost"]) and
+                np.array_equal(front["results"]["completion"], sweep["results"]["completion"]))
 
     # ---------------- end to end through the public API (e2e) ----------------
+    info = front["info"]
     pinned_nets = torch.from_numpy(nets.view(np.uint8)).pin_memory()
     nets_host = pinned_nets.numpy().view(synth.NET_DTYPE)
     res_host = torch.empty(len(nets) * apgar_b200.RESULT_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
@@ -275,57 +307,67 @@ def main():
     path_host = torch.empty(int(info["path_arena_capacity"]), dtype=torch.int32).pin_memory()
     path_arr = path_host.numpy().view(np.uint32)
     for _ in range(2):
-        dev.route(nets_host, out=(res_arr, path_arr))
+        dev.route(nets_host, out=(res_arr, path_arr), generator="frontier")
     barrier()
     e_start = torch.cuda.Event(enable_timing=True)
     e_end = torch.cuda.Event(enable_timing=True)
     path_cells = 0
     e_start.record()
     for _ in range(args.steps):
-        r, p = dev.route(nets_host, out=(res_arr, path_arr))
+        r, p = dev.route(nets_host, out=(res_arr, path_arr), generator="frontier")
         path_cells = len(p)
     e_end.record()
     barrier()
-    e2e_ms = e_start.elapsed_time(e_end)
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e_start.elapsed_time(e_end))
     e2e_value = cert_all * args.steps / (e2e_ms / 1000.0)
     h2d = nets.nbytes
     d2h = len(nets) * apgar_b200.RESULT_DTYPE.itemsize + 4 * path_cells + 8
+    results = front["results"]
+    step_ms = front["step_ms"]
+    total_ms = front["total_ms"]
+    clocks = front["clocks"]
 
     if rank == 0:
         peak, peak_kind = load_peaks()
-        bytes_alg, one_pass = algorithmic_bytes(lat, nets, results)
         avg_ms = total_ms / args.steps
-        achieved = bytes_alg / (avg_ms / 1000.0) / 1e9
+        fbytes = frontier_bytes(results)
+        achieved = fbytes / (avg_ms / 1000.0) / 1e9
         traffic = load_traffic()
-        cl = clocks.summary()
+        sweep_ms = sweep["total_ms"] / args.steps
+        sbytes, one_pass = algorithmic_bytes(lat, nets, sweep["results"])
+        sweep_achieved = sbytes / (sweep_ms / 1000.0) / 1e9
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": avg_ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
             "config": {
-                "workload": WORKLOAD, "form": "plain batched sweep",
+                "workload": WORKLOAD, "form": "persistent work-stealing frontier (bucketed A*)",
                 "nets_per_gpu": len(nets), "lattice": [lat.layers, lat.height, lat.width],
                 "seed": args.seed, "parallelism": f"weak x{world} (independent net batches)",
-                "l2": "label slabs larger than L2 (126 MB) every step",
-                "label_slab_bytes": int(info["label_cells"]) * 4,
+                "l2": "label words (5.4 GB) larger than L2 (126 MB) and cleared every step",
                 "certified_per_step": cert_all,
             },
             "gpu_launches": int(info["kernel_launches"]) * args.steps,
             "roofline": {
                 "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "peak_kind": peak_kind,
-                "traffic": (traffic or {}).get("dram_bytes_per_step"),
-                "bytes_alg_per_step": bytes_alg, "one_pass_bytes_per_step": one_pass,
+                "traffic": (traffic or {}).get("frontier_dram_bytes_per_step"),
+                "kernel": "lattice_frontier_kernel (all width classes of one execution)",
+                "bytes_alg_per_step": fbytes,
             },
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms / args.steps},
-            "clocks": cl,
+            "clocks": clocks,
             "step_ms_min_max": [min(step_ms), max(step_ms)],
-            "sweeps_mean": float(results["sweeps"].mean()),
+            "plain_sweep": {
+                "value": sweep_value, "unit": UNIT, "ms_per_step": sweep_ms,
+                "frontier_over_sweep": value / sweep_value, "same_costs": same,
+                "roofline": {"bound": "hbm", "achieved": sweep_achieved, "peak": peak,
+                             "unit": "GB/s", "frac": sweep_achieved / peak,
+                             "traffic": (traffic or {}).get("dram_bytes_per_step"),
+                             "bytes_alg_per_step": sbytes, "one_pass_bytes_per_step": one_pass},
+                "sweeps_mean": float(sweep["results"]["sweeps"].mean()),
+            },
         }
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"], cpu_costs = cpu_baseline(lat, nets, args.cpu_sample)
@@ -333,7 +375,6 @@ def main():
             line["cpu_baseline"]["costs_match_gpu"] = bool(
                 np.array_equal(cpu_costs[ok], results["cost"][: args.cpu_sample][ok]))
         print(json.dumps(line), flush=True)
-    plan.close()
     dev.close()
     if dist is not None:
         dist.barrier()
