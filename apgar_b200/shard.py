@@ -1,0 +1,65 @@
+"""Multi-GPU plumbing of the search path: one process per GPU.
+
+Nets are independent within a routing round, so a batch shards by nets with no
+data-path collective: every rank searches its own nets over a replicated
+lattice (weak scaling).  The only collectives are the timing and count
+reductions of a measurement, and, in a negotiated-congestion round, one
+integer sum of per-cell usage.  After that sum every rank applies the same
+price update locally.  Integer sums are order independent, so every rank sees
+identical prices.
+
+Everything here works over any torch.distributed backend (nccl on GPUs, gloo
+on CPU for tests).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+from . import synth
+
+
+def rank_nets(lat, seed: int, rank: int, count: int) -> np.ndarray:
+    """The net batch of one rank: rank 0 gets the canonical medium batch of
+    ``seed``; rank r > 0 gets its own seeded batch of the same distribution."""
+    if rank == 0:
+        return synth.make_nets(lat, seed + 1000, count, hpwl_median=200.0, hpwl_sigma=1.0)
+    return synth.make_nets(lat, seed + 1000 + 7919 * rank, count, hpwl_median=200.0,
+                           hpwl_sigma=1.0)
+
+
+def split_nets(nets: np.ndarray, rank: int, world: int) -> np.ndarray:
+    """Strong-scaling split of one batch: rank r takes every world-th net
+    starting at r (keeps the size mix of the batch on every rank)."""
+    return np.ascontiguousarray(nets[rank::world])
+
+
+def max_over_ranks(value: float, dist=None, device=None) -> float:
+    """Maximum of a per-rank value (step time) over all ranks."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(value)
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(value: int, dist=None, device=None) -> int:
+    """Sum of a per-rank count (certified nets) over all ranks."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return int(value)
+    import torch
+
+    t = torch.tensor([int(value)], dtype=torch.int64, device=device)
+    dist.all_reduce(t)
+    return int(t.item())
+
+
+def allreduce_usage(usage, dist=None):
+    """In-place integer sum of a per-cell usage tensor over all ranks (the one
+    exchange of a negotiated-congestion round)."""
+    if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:
+        return usage
+    dist.all_reduce(usage)
+    return usage

@@ -234,12 +234,10 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
     import apgar_b200
-    from apgar_b200 import synth
+    from apgar_b200 import shard, synth
 
-    lat, nets = synth.config_medium(args.seed, nets=args.nets, size=args.size)
-    if world > 1 and rank > 0:
-        nets = synth.make_nets(lat, args.seed + 1000 + 7919 * rank, args.nets, hpwl_median=200.0,
-                               hpwl_sigma=1.0)
+    lat, _ = synth.config_medium(args.seed, nets=0, size=args.size)
+    nets = shard.rank_nets(lat, args.seed, rank, args.nets)  # weak scaling: a batch per rank
     dev = apgar_b200.DeviceLattice(lat)
     stream = torch.cuda.current_stream()
 
@@ -249,18 +247,10 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(ms):
-        if dist is None:
-            return ms
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return shard.max_over_ranks(ms, dist, device="cuda")
 
     def sum_over_ranks(n):
-        if dist is None:
-            return n
-        c = torch.tensor([n], device="cuda", dtype=torch.int64)
-        dist.all_reduce(c)
-        return int(c.item())
+        return shard.sum_over_ranks(n, dist, device="cuda")
 
     def device_resident(generator, sample_clocks):
         """K executions of a resident plan, CUDA events on torch's stream."""
