@@ -124,11 +124,15 @@ int class_for_width(uint32_t width, int layers) {
 }
 
 // Frontier width class (index into kGroupSizes) from the window's cell count.
+// A frontier round is a chain of dependent memory waves, so its latency falls
+// when more warps share a round's cells; the thresholds (measured on the
+// medium batch: 4-layer windows of 10^4 to 10^7 cells) give every window
+// above 256k cells 16 warps.
 int frontier_class(uint64_t cells) {
-  if (cells <= (1ull << 17)) return 0;
-  if (cells <= (1ull << 19)) return 1;
-  if (cells <= (1ull << 21)) return 2;
-  if (cells <= (1ull << 23)) return 3;
+  if (cells <= (1ull << 12)) return 0;
+  if (cells <= (1ull << 14)) return 1;
+  if (cells <= (1ull << 16)) return 2;
+  if (cells <= (1ull << 18)) return 3;
   return 4;
 }
 

@@ -128,3 +128,11 @@ def test_plan_matches_route_and_sweep():
         assert np.array_equal(p1, p_sweep)
     finally:
         dev.close()
+
+
+def test_tiny_windows_one_warp_per_net():
+    # windows of a few hundred cells (the one-warp class), many nets per CTA
+    lat = synth.make_lattice(51, 2, 256, 0.2, via_mask=True)
+    nets = synth.make_nets(lat, 52, 200, hpwl_median=10.0, hpwl_sigma=0.4, margin=6)
+    assert (2 * nets["win_w"].astype(int) * nets["win_h"] <= 4096).mean() > 0.9
+    _assert_parity(lat, nets)
