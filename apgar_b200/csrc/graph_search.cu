@@ -170,7 +170,11 @@ __global__ void __launch_bounds__(kThreads) graph_search_kernel(GraphLaunch p) {
       break;
     }
     if (rounds >= p.maximum_rounds) break;
-    if (tid == 0) sh_stop = (p.cancel != nullptr && *p.cancel != 0u) ? 1 : 0;
+    // the cancel flag is host-mapped memory (every read crosses the bus):
+    // read it on the first round and every 64 rounds after
+    if (tid == 0 && (rounds % 64u) == 0u) {
+      sh_stop = (p.cancel != nullptr && *p.cancel != 0u) ? 1 : 0;
+    }
     // ---- phase A: smallest queued label ----
     uint64_t local_min = kGraphInf;
     for (uint32_t i = tid; i < count; i += kThreads) {
