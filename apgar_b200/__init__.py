@@ -261,6 +261,13 @@ class Plan:
                                                     ctypes.byref(opts), ctypes.byref(handle)))
         self.handle = handle
 
+    def set_cell_costs(self, costs) -> None:
+        """Per-cell entry prices for later executes: a CUDA uint32 tensor of
+        layers*height*width cells (kept referenced here), or None."""
+        self._cell_costs = costs
+        ptr = None if costs is None else ctypes.c_void_p(costs.data_ptr())
+        _check(lib().apgar_b200_lattice_plan_set_cell_costs(self.handle, ptr))
+
     def execute(self, stream: int = 0) -> None:
         _check(lib().apgar_b200_lattice_execute(self.handle, ctypes.c_void_p(stream)))
 

@@ -83,6 +83,9 @@ struct FrontierLaunch {
   unsigned long long* arena_cursor;
   unsigned int* next_plan;            // work-stealing cursor of this class
   const volatile uint32_t* cancel;  // host-mapped flag or nullptr
+  // optional per-cell entry price [layers][height][width] (negotiated
+  // congestion snapshot); a move into cell c costs its move cost + cell_cost[c]
+  const uint32_t* cell_cost;
 };
 
 __device__ __forceinline__ uint32_t sat(uint32_t v) { return v < kLabelInf ? v : kLabelInf; }

@@ -155,8 +155,9 @@ __device__ __forceinline__ uint32_t blocked3(const uint32_t* row, int X) {
 // list); ne[d] holds the packed cell.
 __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const Window& win,
                                             uint32_t e, unsigned long long* words, uint32_t thr,
-                                            uint32_t cur_low, uint32_t far_low, uint32_t (&ne)[10],
-                                            uint32_t& cur_mask, uint32_t& far_mask) {
+                                            uint32_t cur_low, uint32_t far_low,
+                                            const uint32_t* cell_cost, uint32_t (&ne)[10],
+                                            uint32_t& cur_mask, uint32_t& far_mask, bool& overflow) {
   const int l = static_cast<int>(e >> 28), y = static_cast<int>((e >> 14) & 0x3FFFu),
             x = static_cast<int>(e & 0x3FFFu);
   const uint32_t w = static_cast<uint32_t>(win.w);
@@ -179,6 +180,17 @@ __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const 
     seen[d] = (inside & (1u << d)) ? static_cast<uint32_t>(__ldcg(words + ni) >> 32) : 0u;
   }
   const int X = win.x0 + x, Y = win.y0 + y;
+  // entry prices of the neighbours (0 without a price snapshot)
+  uint32_t price[10];
+#pragma unroll
+  for (int d = 0; d < 10; ++d) {
+    price[d] = 0u;
+    if (cell_cost != nullptr && (inside & (1u << d))) {
+      const int nl = d == 8 ? l - 1 : (d == 9 ? l + 1 : l);
+      const int px = d < 8 ? X + fdx(d) : X, py = d < 8 ? Y + fdy(d) : Y;
+      price[d] = __ldg(cell_cost + (static_cast<size_t>(nl) * lat.height + py) * lat.width + px);
+    }
+  }
   const size_t stride = static_cast<size_t>(lat.words) + 2;
   const uint32_t* rowc = lat.sweep_rows + (static_cast<size_t>(l) * lat.height + Y) * stride;
   const uint32_t edge = (xl ? 1u : 0u) | 2u | (xr ? 4u : 0u);
@@ -217,9 +229,15 @@ __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const 
 #pragma unroll
   for (int d = 0; d < 10; ++d) {
     const uint32_t cost = d >= 8 ? lat.via : ((d & 1) ? lat.diag : lat.orth);
-    cand[d] = gv + cost;
+    // gv < 2^31 and price < 2^31: the sum cannot wrap; at or above the
+    // sentinel it leaves the 32-bit cost domain and the net is rejected
+    cand[d] = gv + cost + price[d];
     low[d] = 0u;
     old[d] = 0ull;
+    if ((legal & (1u << d)) && cand[d] >= kLabelInf) {
+      overflow = true;
+      continue;
+    }
     if ((legal & (1u << d)) && cand[d] < seen[d]) {
       const int dx = d < 8 ? fdx(d) : 0, dy = d < 8 ? fdy(d) : 0;
       const int nl = d == 8 ? l - 1 : (d == 9 ? l + 1 : l);
@@ -265,6 +283,7 @@ struct GroupShared {
   uint32_t far_count;
   uint32_t plan;
   uint32_t cancel[2];
+  uint32_t overflow;
   uint32_t sums[16];
 };
 
@@ -322,6 +341,7 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
       sh.count[0] = sh.count[1] = sh.count[2] = 0;
       sh.far_count = 0;
       sh.cancel[0] = sh.cancel[1] = 0;
+      sh.overflow = 0;
       if (endpoints_free) {
         // label 0, in the list of round 0 (stamp 1)
         words[cell_index(win, sl, sx, sy)] = 0xFFFFFFFFull - 1ull;
@@ -388,7 +408,10 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
           uint32_t ne[10];
           if (valid) {
             ++expanded;
-            expand_cell(lat, win, cur[i], words, thr, cur_low, far_low, ne, cur_mask, far_mask);
+            bool overflow = false;
+            expand_cell(lat, win, cur[i], words, thr, cur_low, far_low, p.cell_cost, ne, cur_mask,
+                        far_mask, overflow);
+            if (overflow) sh.overflow = 1u;
           }
           // one packed warp scan places both lists' entries
           const uint32_t nc = __popc(cur_mask), nfar = __popc(far_mask);
@@ -436,7 +459,10 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
       res.sweeps = rounds;
       res.row_steps = expanded;
       res.row_stores = levels;
-      if (completion == APGAR_B200_COMPLETION_REACHED) {
+      if (sh.overflow != 0u) {
+        // a path cost reached the 32-bit sentinel: no exact result exists here
+        res.completion = APGAR_B200_COMPLETION_REJECTED;
+      } else if (completion == APGAR_B200_COMPLETION_REACHED) {
         const uint32_t goal = label_of(words + cell_index(win, win.gl, win.gx, win.gy));
         if (goal >= kLabelInf) {
           res.completion = APGAR_B200_COMPLETION_DISCONNECTED;
@@ -466,6 +492,12 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
                 ok = true;
                 break;
               }
+              // the move into the current cell paid its entry price
+              const uint32_t here_price =
+                  p.cell_cost == nullptr
+                      ? 0u
+                      : __ldg(p.cell_cost + (static_cast<size_t>(cl) * lat.height + (win.y0 + cy)) *
+                                                lat.width + (win.x0 + cx));
               // lanes 0..7: planar predecessors by incoming heading; 8, 9: vias
               bool cand = false;
               int pl = cl, px = cx, py = cy;
@@ -479,7 +511,7 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
                 }
                 if (legal) {
                   pd = label_of(words + cell_index(win, cl, px, py));
-                  cand = pd < kLabelInf && pd + ((lane & 1) ? diag : orth) == here;
+                  cand = pd < kLabelInf && pd + ((lane & 1) ? diag : orth) + here_price == here;
                 }
               } else if (lane == 8 || lane == 9) {
                 pl = (lane == 8) ? cl - 1 : cl + 1;
@@ -487,7 +519,7 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
                 if (pl >= 0 && pl < lat.layers && cell_free_w(lat, win, pl, cx, cy) &&
                     via_allowed(lat, win, lower, cx, cy)) {
                   pd = label_of(words + cell_index(win, pl, cx, cy));
-                  cand = pd < kLabelInf && pd + via == here;
+                  cand = pd < kLabelInf && pd + via + here_price == here;
                 }
               }
               const unsigned ballot = __ballot_sync(0xFFFFFFFFu, cand);

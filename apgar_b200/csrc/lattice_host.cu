@@ -28,6 +28,11 @@ cudaError_t launch_accumulate_cells(const apgar_b200_lattice_result* results, ui
                                     int sm_count, cudaStream_t stream);
 cudaError_t launch_lattice_frontier(int warps_per_net, const FrontierLaunch& launch, int sm_count,
                                     cudaStream_t stream);
+cudaError_t launch_price_update(uint32_t count, const uint32_t* usage, uint64_t factor,
+                                uint64_t next_factor, uint64_t hist_inc, uint64_t capacity,
+                                uint64_t max_value, uint64_t* present, uint64_t* history,
+                                uint64_t* total, uint64_t* next_cost, uint32_t* next_cost32,
+                                uint32_t* status, unsigned long long* stats, cudaStream_t stream);
 cudaError_t launch_lattice_pack(apgar_b200_lattice_result* results, uint32_t count,
                                 unsigned long long* total, const uint32_t* arena, uint32_t* paths,
                                 int sm_count, cudaStream_t stream);
@@ -57,6 +62,7 @@ struct PlanObject {
   uint32_t max_sweeps = 0;  // sweeps (SWEEP) or rounds (FRONTIER)
   uint32_t generator = APGAR_B200_LATTICE_SWEEP;
   uint32_t bucket_width = 0;
+  const uint32_t* cell_cost = nullptr;  // caller-owned device prices (frontier only)
   uint32_t* cancel_host = nullptr;  // pinned, mapped; polled by the kernels
   uint32_t* cancel_dev = nullptr;
   std::vector<ClassRange> classes;
@@ -357,6 +363,7 @@ int execute_plan(PlanObject* plan, cudaStream_t stream) {
   fbase.path_arena_capacity = plan->arena_capacity;
   fbase.arena_cursor = plan->counters.get();
   fbase.cancel = plan->cancel_dev;
+  fbase.cell_cost = plan->cell_cost;
   SweepLaunch base{};
   base.lat = v;
   base.nets = plan->nets.get();
@@ -565,6 +572,17 @@ extern "C" int apgar_b200_lattice_device_results(void* plan,
   auto* p = static_cast<PlanObject*>(plan);
   if (results != nullptr) *results = p->results.get();
   if (paths != nullptr) *paths = p->paths.get();
+  return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_lattice_plan_set_cell_costs(void* plan, const uint32_t* cell_costs) {
+  if (plan == nullptr) return set_error(APGAR_B200_INTERNAL_INVARIANT, "null plan");
+  auto* p = static_cast<PlanObject*>(plan);
+  if (cell_costs != nullptr && p->generator != APGAR_B200_LATTICE_FRONTIER) {
+    return set_error(APGAR_B200_UNSUPPORTED, "per-cell prices need the frontier generator");
+  }
+  p->cell_cost = cell_costs;
+  clear_error();
   return APGAR_B200_OK;
 }
 
@@ -962,4 +980,206 @@ extern "C" int apgar_b200_lattice_route_noalloc(void* lattice, const apgar_b200_
                                results, paths, path_capacity, path_total);
   if (rc == APGAR_B200_OK) clear_error();
   return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Negotiated-congestion rounds on a FRONTIER plan.
+//
+// Round p (Jacobi rip-up and reroute: every net is rerouted against the same
+// frozen snapshot):
+//   1. search every net of the plan with per-cell entry prices `cell_cost`;
+//   2. usage = number of reached paths through each cell (integer atomics, so
+//      order independent);
+//   3. one fused price pass at epoch p (src/allocator/negotiated_regeneration_plan.cc
+//      :430-442 factor schedule; cpu_sequential_negotiated_routing.cc:1300-1330
+//      history update): history += increment * overuse, and the next snapshot
+//      cell_cost = history + factor(p + 1) * max(0, usage + 1 - capacity)
+//      (cpu_sequential_negotiated_routing.cc:299-505), saturated to 2^31 - 1;
+//      the same pass counts overused cells and total overuse for the round.
+// The reference's sequential negotiated router reroutes nets one at a time
+// (Gauss-Seidel); batched rounds are Jacobi by design, so only each round's
+// per-net results under its frozen snapshot are comparable with a CPU run.
+// A run starts from zero history and zero prices, so it can be captured once
+// as a CUDA graph of all its rounds and replayed.
+namespace apgar_b200 {
+namespace {
+
+struct NegotiationObject {
+  PlanObject* plan = nullptr;
+  apgar_b200_price_policy policy{};
+  uint64_t cells = 0;
+  DeviceBuffer<uint32_t> usage, cell_cost, status;
+  DeviceBuffer<uint64_t> history;
+  DeviceBuffer<unsigned long long> stats;  // [round][overused cells, total overuse]
+  uint32_t rounds_capacity = 0;
+  cudaStream_t work = nullptr;
+  cudaEvent_t entry = nullptr, exit = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint32_t graph_rounds = 0;
+
+  ~NegotiationObject() {
+    if (exec != nullptr) cudaGraphExecDestroy(exec);
+    if (graph != nullptr) cudaGraphDestroy(graph);
+    if (entry != nullptr) cudaEventDestroy(entry);
+    if (exit != nullptr) cudaEventDestroy(exit);
+    if (work != nullptr) cudaStreamDestroy(work);
+    if (plan != nullptr) plan->cell_cost = nullptr;
+  }
+};
+
+bool checked_factor(const apgar_b200_price_policy& p, uint64_t epoch, uint64_t* out) {
+  const unsigned __int128 f =
+      static_cast<unsigned __int128>(epoch) * p.present_factor_increment + p.initial_present_factor;
+  if (f > static_cast<unsigned __int128>(~0ull)) return false;
+  *out = static_cast<uint64_t>(f);
+  return true;
+}
+
+// Enqueues a whole negotiation (reset + `rounds` rounds) on n->work.
+int enqueue_negotiation(NegotiationObject* n, uint32_t rounds) {
+  cudaStream_t s = n->work;
+  APGAR_B200_CUDA("cudaMemsetAsync(history)",
+                  cudaMemsetAsync(n->history.get(), 0, n->cells * sizeof(uint64_t), s));
+  APGAR_B200_CUDA("cudaMemsetAsync(cell costs)",
+                  cudaMemsetAsync(n->cell_cost.get(), 0, n->cells * sizeof(uint32_t), s));
+  n->plan->cell_cost = n->cell_cost.get();
+  for (uint32_t r = 0; r < rounds; ++r) {
+    uint64_t factor = 0, next_factor = 0;
+    if (!checked_factor(n->policy, r, &factor) || !checked_factor(n->policy, r + 1ull, &next_factor)) {
+      return set_error(APGAR_B200_INTERNAL_INVARIANT, "present-price schedule overflowed uint64");
+    }
+    if (int rc = execute_plan(n->plan, s); rc != APGAR_B200_OK) return rc;
+    APGAR_B200_CUDA("cudaMemsetAsync(usage)",
+                    cudaMemsetAsync(n->usage.get(), 0, n->cells * sizeof(uint32_t), s));
+    APGAR_B200_CUDA("usage accumulation launch",
+                    launch_accumulate_cells(n->plan->results.get(), n->plan->count,
+                                            n->plan->paths.get(), n->usage.get(), n->cells,
+                                            n->plan->sm_count, s));
+    APGAR_B200_CUDA("price update launch",
+                    launch_price_update(static_cast<uint32_t>(n->cells), n->usage.get(), factor,
+                                        next_factor, n->policy.historical_price_increment,
+                                        n->policy.capacity, n->policy.maximum_value, nullptr,
+                                        n->history.get(), nullptr, nullptr, n->cell_cost.get(),
+                                        n->status.get() + r, n->stats.get() + 2ull * r, s));
+  }
+  return APGAR_B200_OK;
+}
+
+}  // namespace
+}  // namespace apgar_b200
+
+extern "C" int apgar_b200_negotiation_create(void* plan, const apgar_b200_price_policy* policy,
+                                             void** out) {
+  if (plan == nullptr || policy == nullptr || out == nullptr) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "negotiation received a null argument");
+  }
+  auto* p = static_cast<PlanObject*>(plan);
+  if (p->generator != APGAR_B200_LATTICE_FRONTIER) {
+    return set_error(APGAR_B200_UNSUPPORTED, "negotiated rounds need a FRONTIER plan");
+  }
+  if (int rc = check_device(p->device); rc != APGAR_B200_OK) return rc;
+  const LatticeDeviceView& v = p->lattice->view;
+  const uint64_t cells = static_cast<uint64_t>(v.layers) * v.height * v.width;
+  if (cells > 0xFFFFFFFFull) {
+    return set_error(APGAR_B200_UNSUPPORTED, "lattice has more cells than a price pass indexes");
+  }
+  try {
+    auto n = std::make_unique<NegotiationObject>();
+    n->plan = p;
+    n->policy = *policy;
+    n->cells = cells;
+    APGAR_B200_CUDA("cudaMalloc(usage)", n->usage.ensure(cells));
+    APGAR_B200_CUDA("cudaMalloc(cell costs)", n->cell_cost.ensure(cells));
+    APGAR_B200_CUDA("cudaMalloc(history)", n->history.ensure(cells));
+    APGAR_B200_CUDA("cudaStreamCreate", cudaStreamCreateWithFlags(&n->work, cudaStreamNonBlocking));
+    APGAR_B200_CUDA("cudaEventCreate", cudaEventCreateWithFlags(&n->entry, cudaEventDisableTiming));
+    APGAR_B200_CUDA("cudaEventCreate", cudaEventCreateWithFlags(&n->exit, cudaEventDisableTiming));
+    *out = n.release();
+    clear_error();
+    return APGAR_B200_OK;
+  } catch (const std::bad_alloc&) {
+    return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "host allocation failed creating a negotiation");
+  }
+}
+
+extern "C" int apgar_b200_negotiation_run(void* negotiation, uint32_t rounds, uint32_t use_graph,
+                                          void* stream) {
+  if (negotiation == nullptr || rounds == 0 || rounds > 1000) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "negotiation needs 1..1000 rounds");
+  }
+  auto* n = static_cast<NegotiationObject*>(negotiation);
+  if (int rc = check_device(n->plan->device); rc != APGAR_B200_OK) return rc;
+  const auto caller = static_cast<cudaStream_t>(stream);
+  if (rounds > n->rounds_capacity) {
+    APGAR_B200_CUDA("cudaMalloc(round status)", n->status.ensure(rounds));
+    APGAR_B200_CUDA("cudaMalloc(round stats)", n->stats.ensure(2ull * rounds));
+    n->rounds_capacity = rounds;
+  }
+  // work runs on the negotiation's own stream, ordered after the caller's
+  APGAR_B200_CUDA("cudaEventRecord(entry)", cudaEventRecord(n->entry, caller));
+  APGAR_B200_CUDA("cudaStreamWaitEvent", cudaStreamWaitEvent(n->work, n->entry, 0));
+  if (use_graph == 0) {
+    if (int rc = enqueue_negotiation(n, rounds); rc != APGAR_B200_OK) return rc;
+  } else {
+    if (n->exec == nullptr || n->graph_rounds != rounds) {
+      if (n->exec != nullptr) cudaGraphExecDestroy(n->exec);
+      if (n->graph != nullptr) cudaGraphDestroy(n->graph);
+      n->exec = nullptr;
+      n->graph = nullptr;
+      APGAR_B200_CUDA("cudaStreamBeginCapture",
+                      cudaStreamBeginCapture(n->work, cudaStreamCaptureModeRelaxed));
+      const int rc = enqueue_negotiation(n, rounds);
+      cudaGraph_t graph = nullptr;
+      const cudaError_t end = cudaStreamEndCapture(n->work, &graph);
+      if (rc != APGAR_B200_OK) {
+        if (graph != nullptr) cudaGraphDestroy(graph);
+        return rc;
+      }
+      APGAR_B200_CUDA("cudaStreamEndCapture", end);
+      n->graph = graph;
+      APGAR_B200_CUDA("cudaGraphInstantiate", cudaGraphInstantiate(&n->exec, graph, 0));
+      n->graph_rounds = rounds;
+    }
+    APGAR_B200_CUDA("cudaGraphLaunch", cudaGraphLaunch(n->exec, n->work));
+  }
+  APGAR_B200_CUDA("cudaEventRecord(exit)", cudaEventRecord(n->exit, n->work));
+  APGAR_B200_CUDA("cudaStreamWaitEvent", cudaStreamWaitEvent(caller, n->exit, 0));
+  clear_error();
+  return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_negotiation_readback(void* negotiation, uint32_t* usage, uint64_t* history,
+                                               uint32_t* cell_costs,
+                                               apgar_b200_negotiation_round* rounds,
+                                               uint32_t round_count) {
+  if (negotiation == nullptr) return set_error(APGAR_B200_INTERNAL_INVARIANT, "null negotiation");
+  auto* n = static_cast<NegotiationObject*>(negotiation);
+  if (int rc = check_device(n->plan->device); rc != APGAR_B200_OK) return rc;
+  if (round_count > n->rounds_capacity) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "more rounds requested than were run");
+  }
+  APGAR_B200_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(n->work));
+  if (usage) APGAR_B200_CUDA("cudaMemcpy(usage)", cudaMemcpy(usage, n->usage.get(), n->cells * 4, cudaMemcpyDeviceToHost));
+  if (history) APGAR_B200_CUDA("cudaMemcpy(history)", cudaMemcpy(history, n->history.get(), n->cells * 8, cudaMemcpyDeviceToHost));
+  if (cell_costs) APGAR_B200_CUDA("cudaMemcpy(cell costs)", cudaMemcpy(cell_costs, n->cell_cost.get(), n->cells * 4, cudaMemcpyDeviceToHost));
+  if (rounds != nullptr && round_count > 0) {
+    std::vector<unsigned long long> st(2ull * round_count);
+    std::vector<uint32_t> fl(round_count);
+    APGAR_B200_CUDA("cudaMemcpy(round stats)", cudaMemcpy(st.data(), n->stats.get(), st.size() * 8, cudaMemcpyDeviceToHost));
+    APGAR_B200_CUDA("cudaMemcpy(round status)", cudaMemcpy(fl.data(), n->status.get(), fl.size() * 4, cudaMemcpyDeviceToHost));
+    for (uint32_t r = 0; r < round_count; ++r) {
+      rounds[r].overused_cells = st[2ull * r];
+      rounds[r].total_overuse = st[2ull * r + 1];
+      rounds[r].price_status = fl[r];
+      rounds[r].reserved = 0;
+    }
+  }
+  clear_error();
+  return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_negotiation_release(void* negotiation) {
+  delete static_cast<NegotiationObject*>(negotiation);
+  return APGAR_B200_OK;
 }

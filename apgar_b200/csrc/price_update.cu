@@ -39,11 +39,16 @@ __device__ __forceinline__ bool add_checked(uint64_t a, uint64_t b, uint64_t* ou
 __global__ void price_update_kernel(uint32_t count, const uint32_t* __restrict__ usage,
                                     PriceParams pp, uint64_t* __restrict__ present,
                                     uint64_t* __restrict__ history, uint64_t* __restrict__ total,
-                                    uint64_t* __restrict__ next_cost, uint32_t* status) {
+                                    uint64_t* __restrict__ next_cost,
+                                    uint32_t* __restrict__ next_cost32, uint32_t* status,
+                                    unsigned long long* stats) {
   uint32_t flags = 0;
+  unsigned long long overused = 0, overuse_sum = 0;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
     const uint64_t u = usage[i];
     const uint64_t over = u > pp.capacity ? u - pp.capacity : 0;
+    overused += over != 0 ? 1ull : 0ull;
+    overuse_sum += over;
     uint64_t h = history[i];
     uint64_t p = 0;
     if (over != 0) {
@@ -62,10 +67,10 @@ __global__ void price_update_kernel(uint32_t count, const uint32_t* __restrict__
       flags |= APGAR_B200_PRICE_OVERFLOW;
       t = ~0ull;
     }
-    present[i] = p;
+    if (present != nullptr) present[i] = p;
     history[i] = h;
-    total[i] = t;
-    if (next_cost != nullptr) {
+    if (total != nullptr) total[i] = t;
+    if (next_cost != nullptr || next_cost32 != nullptr) {
       const uint64_t predicted = u + 1;
       const uint64_t pover = predicted > pp.capacity ? predicted - pp.capacity : 0;
       uint64_t c, pc;
@@ -75,11 +80,24 @@ __global__ void price_update_kernel(uint32_t count, const uint32_t* __restrict__
       } else if (c > pp.max_value) {
         flags |= APGAR_B200_PRICE_BOUND;
       }
-      next_cost[i] = c;
+      if (next_cost != nullptr) next_cost[i] = c;
+      // the search reads a 32-bit entry price; a larger cost saturates to the
+      // label sentinel, so any path through the cell is rejected, never wrong
+      if (next_cost32 != nullptr) next_cost32[i] = c < 0x7FFFFFFFull ? static_cast<uint32_t>(c) : 0x7FFFFFFFu;
     }
   }
   flags = __reduce_or_sync(0xFFFFFFFFu, flags);
   if (flags != 0u && (threadIdx.x & 31) == 0) atomicOr(status, flags);
+  if (stats != nullptr) {
+    for (int o = 16; o > 0; o >>= 1) {
+      overused += __shfl_xor_sync(0xFFFFFFFFu, overused, o);
+      overuse_sum += __shfl_xor_sync(0xFFFFFFFFu, overuse_sum, o);
+    }
+    if ((threadIdx.x & 31) == 0 && (overused | overuse_sum) != 0ull) {
+      atomicAdd(stats, overused);
+      atomicAdd(stats + 1, overuse_sum);
+    }
+  }
 }
 
 __global__ void accumulate_cells_kernel(const apgar_b200_lattice_result* __restrict__ results,
@@ -100,14 +118,17 @@ __global__ void accumulate_cells_kernel(const apgar_b200_lattice_result* __restr
 cudaError_t launch_price_update(uint32_t count, const uint32_t* usage, uint64_t factor,
                                 uint64_t next_factor, uint64_t hist_inc, uint64_t capacity,
                                 uint64_t max_value, uint64_t* present, uint64_t* history,
-                                uint64_t* total, uint64_t* next_cost, uint32_t* status,
-                                cudaStream_t stream) {
+                                uint64_t* total, uint64_t* next_cost, uint32_t* next_cost32,
+                                uint32_t* status, unsigned long long* stats, cudaStream_t stream) {
   cudaError_t e = cudaMemsetAsync(status, 0, sizeof(uint32_t), stream);
+  if (e == cudaSuccess && stats != nullptr) {
+    e = cudaMemsetAsync(stats, 0, 2 * sizeof(unsigned long long), stream);
+  }
   if (e != cudaSuccess || count == 0) return e;
   PriceParams pp{factor, next_factor, hist_inc, capacity, max_value};
   const uint32_t blocks = (count + 255u) / 256u;
   price_update_kernel<<<blocks < 148u * 16u ? blocks : 148u * 16u, 256, 0, stream>>>(
-      count, usage, pp, present, history, total, next_cost, status);
+      count, usage, pp, present, history, total, next_cost, next_cost32, status, stats);
   return cudaGetLastError();
 }
 

@@ -1,0 +1,69 @@
+"""Negotiated-congestion rounds (rip-up and reroute) on a frontier plan.
+
+Host mirror of the apgar_b200_negotiation_* C ABI: every round reroutes all
+nets of the plan against frozen per-cell snapshot prices, counts per-cell
+usage, and runs the fused price pass (history and the next snapshot).  The
+whole run can be captured once as a CUDA graph and replayed.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _check, lib
+from .prices import PricePolicy
+
+
+class RoundStats(ctypes.Structure):
+    _fields_ = [
+        ("overused_cells", ctypes.c_uint64),
+        ("total_overuse", ctypes.c_uint64),
+        ("price_status", ctypes.c_uint32),
+        ("reserved", ctypes.c_uint32),
+    ]
+
+
+class Negotiation:
+    def __init__(self, plan, policy: PricePolicy):
+        if plan.generator != "frontier":
+            raise ValueError("negotiated rounds need a frontier plan")
+        self.plan = plan
+        self.policy = policy
+        self.cells = plan.lattice.layers * plan.lattice.height * plan.lattice.width
+        self.rounds = 0
+        handle = ctypes.c_void_p()
+        _check(lib().apgar_b200_negotiation_create(plan.handle, ctypes.byref(policy),
+                                                   ctypes.byref(handle)))
+        self.handle = handle
+
+    def run(self, rounds: int, use_graph: bool = False, stream: int = 0) -> None:
+        _check(lib().apgar_b200_negotiation_run(self.handle, ctypes.c_uint32(rounds),
+                                                ctypes.c_uint32(1 if use_graph else 0),
+                                                ctypes.c_void_p(stream)))
+        self.rounds = rounds
+
+    def readback(self):
+        """(usage, history, next snapshot prices, per-round stats list)."""
+        usage = np.empty(self.cells, np.uint32)
+        history = np.empty(self.cells, np.uint64)
+        costs = np.empty(self.cells, np.uint32)
+        stats = (RoundStats * max(self.rounds, 1))()
+        _check(lib().apgar_b200_negotiation_readback(
+            self.handle, usage.ctypes.data_as(ctypes.c_void_p), history.ctypes.data_as(ctypes.c_void_p),
+            costs.ctypes.data_as(ctypes.c_void_p), stats, ctypes.c_uint32(self.rounds)))
+        rows = [dict(overused_cells=s.overused_cells, total_overuse=s.total_overuse,
+                     price_status=s.price_status) for s in stats[: self.rounds]]
+        return usage, history, costs, rows
+
+    def close(self):
+        if self.handle:
+            lib().apgar_b200_negotiation_release(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

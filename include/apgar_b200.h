@@ -390,6 +390,15 @@ typedef struct apgar_b200_lattice_options {
   uint32_t reserved;
 } apgar_b200_lattice_options;
 
+/* Per-cell entry prices for a FRONTIER plan (no reference counterpart at this
+ * level: it carries the negotiated-congestion snapshot cost of
+ * src/allocator/cpu_sequential_negotiated_routing.cc:299-505 per lattice cell).
+ * `cell_costs` is a device array [layers][height][width] of uint32, read by
+ * every later execute until replaced; NULL removes it.  A move into cell c
+ * then costs its move cost plus cell_costs[c].  A net whose path costs reach
+ * 2^31 - 1 comes back REJECTED instead of with a wrong cost. */
+APGAR_B200_API int apgar_b200_lattice_plan_set_cell_costs(void* plan, const uint32_t* cell_costs);
+
 /* apgar_b200_lattice_plan / apgar_b200_lattice_route with a generator choice. */
 APGAR_B200_API int apgar_b200_lattice_plan_ex(void* lattice, const apgar_b200_lattice_net* nets,
                                uint32_t count, const apgar_b200_lattice_options* options,
@@ -446,6 +455,45 @@ APGAR_B200_API int apgar_b200_price_update(uint32_t count, const uint32_t* usage
  * array).  Device pointer, stream-ordered. */
 APGAR_B200_API int apgar_b200_lattice_accumulate_usage(void* plan, uint32_t* usage,
                                                        uint64_t cell_count, void* stream);
+
+/* ================= D. negotiated-congestion rounds ================= */
+
+/* Batched rip-up and reroute on a FRONTIER plan: the reference's negotiated
+ * loop (RouteCpuSequentialNegotiated, src/allocator/
+ * cpu_sequential_negotiated_routing.cc:993-1330) with the GPU batched search
+ * as its engine and one resource per lattice cell.  Round r reroutes every
+ * net of the plan against the frozen snapshot prices, counts per-cell usage
+ * of the reached paths, and runs the fused price pass at epoch r: history
+ * += increment * overuse; next snapshot = history + factor(r + 1) *
+ * max(0, usage + 1 - capacity).  Rounds are Jacobi (all nets against one
+ * snapshot), while the reference's loop is Gauss-Seidel (net by net), so the
+ * two give different routings by design; every round is exact for its
+ * snapshot. */
+typedef struct apgar_b200_negotiation_round {
+  uint64_t overused_cells; /* cells with usage > capacity after the round */
+  uint64_t total_overuse;  /* sum of max(0, usage - capacity) */
+  uint32_t price_status;   /* APGAR_B200_PRICE_* bits of the round's price pass */
+  uint32_t reserved;
+} apgar_b200_negotiation_round;
+
+/* Binds a negotiation to a FRONTIER plan (the plan must outlive it; the
+ * negotiation sets the plan's cell prices while it runs). */
+APGAR_B200_API int apgar_b200_negotiation_create(void* plan, const apgar_b200_price_policy* policy,
+                                  void** out_negotiation);
+/* Runs a whole negotiation from zero history and zero prices: `rounds`
+ * rounds, stream-ordered after `stream`.  With use_graph != 0 the rounds
+ * are captured once as one CUDA graph (re-captured when `rounds` changes)
+ * and replayed; the first call with a given round count does the capture.
+ * The plan's results and paths hold the last round's routing. */
+APGAR_B200_API int apgar_b200_negotiation_run(void* negotiation, uint32_t rounds, uint32_t use_graph,
+                               void* stream);
+/* Waits for the negotiation; copies the last round's usage, the history,
+ * the next snapshot prices (each optional, layers*height*width cells) and
+ * per-round statistics. */
+APGAR_B200_API int apgar_b200_negotiation_readback(void* negotiation, uint32_t* usage, uint64_t* history,
+                                    uint32_t* cell_costs, apgar_b200_negotiation_round* rounds,
+                                    uint32_t round_count);
+APGAR_B200_API int apgar_b200_negotiation_release(void* negotiation);
 
 #ifdef __cplusplus
 }

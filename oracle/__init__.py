@@ -31,6 +31,7 @@ class LoLattice(ctypes.Structure):
         ("orth", ctypes.c_uint32),
         ("diag", ctypes.c_uint32),
         ("via", ctypes.c_uint32),
+        ("cell_cost", U32P),
     ]
 
 
@@ -98,23 +99,27 @@ def _ptr(a, t=U32P):
 class LatticeRef:
     """Keeps the numpy buffers alive while the C struct points at them."""
 
-    def __init__(self, lat):
+    def __init__(self, lat, cell_cost=None):
         self.blocked = np.ascontiguousarray(lat.blocked, dtype=np.uint32)
         self.via_ok = None if lat.via_ok is None else np.ascontiguousarray(lat.via_ok, np.uint32)
+        self.cell_cost = None if cell_cost is None else np.ascontiguousarray(cell_cost, np.uint32)
+        if self.cell_cost is not None:
+            assert self.cell_cost.size == lat.layers * lat.height * lat.width
         self.c = LoLattice(
             lat.layers, lat.height, lat.width, _ptr(self.blocked),
             _ptr(self.via_ok) if self.via_ok is not None else U32P(),
-            lat.orth, lat.diag, lat.via)
+            lat.orth, lat.diag, lat.via,
+            _ptr(self.cell_cost) if self.cell_cost is not None else U32P())
 
 
 def _net_ptr(nets):
     return nets.ctypes.data_as(ctypes.c_void_p)
 
 
-def dijkstra(lat, net_row, full=False, want_dist=False, path_cap=1 << 22):
+def dijkstra(lat, net_row, full=False, want_dist=False, path_cap=1 << 22, cell_cost=None):
     """Returns (cost, reverse canonical path as uint32 array, dist or None)."""
     L = lib()
-    ref = LatticeRef(lat)
+    ref = LatticeRef(lat, cell_cost)
     net = np.array([net_row], dtype=net_row.dtype) if not isinstance(net_row, np.ndarray) else net_row
     net = np.ascontiguousarray(net.reshape(1))
     cells = lat.layers * int(net["win_w"][0]) * int(net["win_h"][0])
@@ -128,9 +133,11 @@ def dijkstra(lat, net_row, full=False, want_dist=False, path_cap=1 << 22):
     return cost, (path[:n].copy() if n != 0xFFFFFFFF else None), dist
 
 
-def dijkstra_batch(lat, nets, threads=None, path_cap_per_net=None):
+def dijkstra_batch(lat, nets, threads=None, path_cap_per_net=None, cell_cost=None):
+    """Exact costs and canonical reverse paths of every net; ``cell_cost``
+    (optional, uint32 [layers][height][width]) adds a per-cell entry price."""
     L = lib()
-    ref = LatticeRef(lat)
+    ref = LatticeRef(lat, cell_cost)
     nets = np.ascontiguousarray(nets)
     count = len(nets)
     threads = threads or os.cpu_count() or 1

@@ -129,6 +129,13 @@ static inline uint32_t move_cost(const lo_lattice* lat, int h) {
   return (h & 1) ? lat->diag : lat->orth;
 }
 
+/* Entry cost of window cell (l, x, y): its negotiated price, 0 without one. */
+static inline uint64_t entry_cost(const win_ctx* c, int l, int x, int y) {
+  const lo_lattice* lat = c->lat;
+  if (lat->cell_cost == NULL) return 0;
+  return lat->cell_cost[((size_t)l * lat->height + (c->y0 + y)) * lat->width + (c->x0 + x)];
+}
+
 /* Reverse canonical path from exact labels.  Returns path length, or
  * UINT32_MAX when the capacity is exceeded or the labels are inconsistent. */
 static uint32_t canonical_walk(const win_ctx* c, const uint32_t* dist, int gl, int gx, int gy,
@@ -159,7 +166,7 @@ static uint32_t canonical_walk(const win_ctx* c, const uint32_t* dist, int gl, i
       if (!legal) continue;
       const uint32_t pd = dist[cell_index(c, pl, px, py)];
       if (pd == LO_INF) continue;
-      if ((uint64_t)pd + move_cost(lat, h) == here) {
+      if ((uint64_t)pd + move_cost(lat, h) + entry_cost(c, l, x, y) == here) {
         chosen = h;
         l = pl;
         x = px;
@@ -214,8 +221,9 @@ uint32_t lo_dijkstra(const lo_lattice* lat, const lo_net* net, int full, uint32_
         legal = nl >= 0 && via_legal(&c, nl, x, y);
       }
       if (!legal) continue;
-      const uint64_t cand = (uint64_t)d + move_cost(lat, h);
+      const uint64_t cand = (uint64_t)d + move_cost(lat, h) + entry_cost(&c, nl, nx, ny);
       const size_t ni = cell_index(&c, nl, nx, ny);
+      if (cand >= LO_INF) continue; /* beyond the 32-bit cost domain */
       if (cand < dist[ni]) {
         dist[ni] = (uint32_t)cand;
         heap_push(&hp, (cand << 32) | (uint32_t)ni, (uint32_t)ni);

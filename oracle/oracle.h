@@ -47,6 +47,11 @@ typedef struct lo_lattice {
   const uint32_t* blocked;       /* [layers][height][width/32], bit x%32 of word x/32 */
   const uint32_t* via_ok;        /* [layers-1][height][width/32]; NULL = no via restriction */
   uint32_t orth, diag, via;      /* move costs */
+  /* Optional per-cell entry cost [layers][height][width] (NULL = none): a
+   * move into cell c costs its move cost plus cell_cost[c].  Only lo_dijkstra
+   * (and its batch form) reads it; it models a negotiated-congestion price
+   * snapshot. */
+  const uint32_t* cell_cost;
 } lo_lattice;
 
 typedef struct lo_net {

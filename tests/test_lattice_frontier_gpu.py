@@ -136,3 +136,47 @@ def test_tiny_windows_one_warp_per_net():
     nets = synth.make_nets(lat, 52, 200, hpwl_median=10.0, hpwl_sigma=0.4, margin=6)
     assert (2 * nets["win_w"].astype(int) * nets["win_h"] <= 4096).mean() > 0.9
     _assert_parity(lat, nets)
+
+
+def test_per_cell_prices_match_the_priced_oracle():
+    import torch
+
+    rng = np.random.default_rng(77)
+    lat, nets = synth.config_medium(5, nets=96, size=512)
+    price = rng.integers(0, 60, size=(lat.layers, lat.height, lat.width)).astype(np.uint32)
+    price[:, 100:140, :] += 400  # an expensive band that paths route around
+    dev = apgar_b200.DeviceLattice(lat)
+    try:
+        plan = dev.plan(nets, generator="frontier")
+        plan.set_cell_costs(torch.from_numpy(price.ravel().view(np.int32)).cuda())
+        plan.execute()
+        res, paths = plan.readback()
+        plan.close()
+    finally:
+        dev.close()
+    cost_o, paths_o = oracle.dijkstra_batch(lat, nets, cell_cost=price)
+    assert (res["completion"] != apgar_b200.COMPLETION_REJECTED).all()
+    assert np.array_equal(res["cost"], cost_o)
+    per = apgar_b200.split_paths(res, paths)
+    for i in range(len(nets)):
+        if cost_o[i] != oracle.lo_inf():
+            assert np.array_equal(per[i], paths_o[i]), i
+
+
+def test_price_overflow_is_rejected_not_wrong():
+    import torch
+
+    lat, nets = synth.config_small(2)
+    price = np.full((lat.layers, lat.height, lat.width), 0x3FFFFFFF, np.uint32)
+    dev = apgar_b200.DeviceLattice(lat)
+    try:
+        plan = dev.plan(nets[:8].copy(), generator="frontier")
+        plan.set_cell_costs(torch.from_numpy(price.ravel().view(np.int32)).cuda())
+        plan.execute()
+        res, _ = plan.readback()
+        plan.close()
+    finally:
+        dev.close()
+    # two entries already pass 2^31: every net with a path of 2+ moves is rejected
+    moved = (nets["start_x"][:8] != nets["goal_x"][:8]) | (nets["start_y"][:8] != nets["goal_y"][:8])
+    assert (res["completion"][moved] == apgar_b200.COMPLETION_REJECTED).all()

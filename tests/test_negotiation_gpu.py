@@ -1,0 +1,85 @@
+"""GPU negotiated-congestion rounds against a CPU restatement of the same
+Jacobi rip-up-and-reroute loop: per round, the priced oracle search of every
+net under the frozen snapshot, per-cell usage of the reached paths, the
+allocator epoch history update and the CS-RR next-pass snapshot (price
+oracle).  Bit-exact usage, history, snapshot prices, per-round overuse and the
+last round's costs and canonical paths; the CUDA-graph form replays to the
+same result."""
+
+import numpy as np
+import pytest
+
+import apgar_b200
+import oracle
+from apgar_b200 import negotiate, prices, synth
+
+pytestmark = pytest.mark.gpu
+
+
+def _cpu_rounds(lat, nets, pol, rounds):
+    cells = lat.layers * lat.height * lat.width
+    history = np.zeros(cells, np.uint64)
+    cost = np.zeros(cells, np.uint32)
+    per_round = []
+    for r in range(rounds):
+        costs, paths = oracle.dijkstra_batch(lat, nets, cell_cost=cost)
+        usage = np.zeros(cells, np.uint64)
+        for c, p in zip(costs, paths):
+            if c != oracle.lo_inf():
+                np.add.at(usage, p.astype(np.int64), 1)
+        rc, _, history, _ = oracle.price_epoch_update(
+            usage, history, pol.capacity, r, pol.initial_present_factor,
+            pol.present_factor_increment, pol.historical_price_increment)
+        assert rc == 0
+        rc, snap = oracle.price_snapshot(usage, history, pol.capacity, r + 1,
+                                         pol.initial_present_factor, pol.present_factor_increment,
+                                         pol.maximum_value)
+        assert rc == 0
+        cost = np.minimum(snap, 0x7FFFFFFF).astype(np.uint32)
+        over = np.where(usage > pol.capacity, usage - pol.capacity, 0)
+        per_round.append((int((over > 0).sum()), int(over.sum())))
+    return usage.astype(np.uint32), history, cost, costs, paths, per_round
+
+
+@pytest.mark.parametrize("use_graph", [False, True])
+def test_rounds_match_cpu_restatement(use_graph):
+    lat = synth.make_lattice(61, 2, 128, 0.15, via_mask=True)
+    nets = synth.make_nets(lat, 62, 48, hpwl_median=50.0, hpwl_sigma=0.5, margin=12)
+    pol = prices.policy(initial=20, increment=20, history_increment=5, capacity=1)
+    rounds = 4
+    usage_c, history_c, cost_c, costs_c, paths_c, per_round_c = _cpu_rounds(lat, nets, pol, rounds)
+    assert per_round_c[0][0] > 0  # the batch is congested in the first round
+    dev = apgar_b200.DeviceLattice(lat)
+    try:
+        plan = dev.plan(nets, generator="frontier")
+        neg = negotiate.Negotiation(plan, pol)
+        for _ in range(2 if use_graph else 1):  # the second graph run is a replay
+            neg.run(rounds, use_graph=use_graph)
+            usage, history, cost, rows = neg.readback()
+            res, paths = plan.readback()
+            assert np.array_equal(usage, usage_c)
+            assert np.array_equal(history, history_c)
+            assert np.array_equal(cost, cost_c)
+            assert [(r["overused_cells"], r["total_overuse"]) for r in rows] == per_round_c
+            assert all(r["price_status"] == 0 for r in rows)
+            assert np.array_equal(res["cost"], costs_c)
+            per = apgar_b200.split_paths(res, paths)
+            for i in range(len(nets)):
+                if costs_c[i] != oracle.lo_inf():
+                    assert np.array_equal(per[i], paths_c[i]), i
+        neg.close()
+        plan.close()
+    finally:
+        dev.close()
+
+
+def test_negotiation_needs_a_frontier_plan():
+    lat, nets = synth.config_small(1)
+    dev = apgar_b200.DeviceLattice(lat)
+    try:
+        plan = dev.plan(nets[:4].copy())
+        with pytest.raises(ValueError):
+            negotiate.Negotiation(plan, prices.policy())
+        plan.close()
+    finally:
+        dev.close()

@@ -178,3 +178,58 @@ def test_pinned_to_reference_graph_oracle_on_single_layer(seed):
         graph_cells = (gpath // 9).astype(np.uint32)  # node ids are y*W + x = cell ids
         assert np.array_equal(graph_cells, path), (sx, sy, gx, gy)
     assert compared == 40 and reached >= 20
+
+
+def test_priced_dijkstra_against_brute_force_relaxation():
+    """Per-cell entry prices: the oracle's labels equal a Bellman-Ford fixed
+    point computed here, and its canonical path pays move + entry costs."""
+    rng = np.random.default_rng(9)
+    lat = synth.make_lattice(9, 2, 32, 0.15, via_mask=False)
+    price = rng.integers(0, 40, size=(2, 32, 32)).astype(np.uint32)
+    dense = synth.unpack_bits(np.asarray(lat.blocked).reshape(2, 32, 1), 32)
+    free = np.argwhere(~dense)
+    for _ in range(4):
+        (sl, sy, sx), (gl, gy, gx) = free[rng.integers(len(free), size=2)]
+        net = np.array([(sl, sx, sy, gl, gx, gy, 0, 0, 32, 32)], dtype=synth.NET_DTYPE)
+        cost, path, dist = oracle.dijkstra(lat, net[0], full=True, want_dist=True, cell_cost=price)
+        # Bellman-Ford over the same move model
+        INF = 1 << 40
+        d = np.full((2, 32, 32), INF, dtype=np.int64)
+        d[sl, sy, sx] = 0
+        for _ in range(400):
+            changed = False
+            for l in range(2):
+                for y in range(32):
+                    for x in range(32):
+                        if d[l, y, x] >= INF:
+                            continue
+                        for h in range(10):
+                            if h < 8:
+                                nl, nx, ny = l, x + DX[h], y + DY[h]
+                                if not (_free(dense, net[0], l, x, y) and _free(dense, net[0], l, nx, ny)):
+                                    continue
+                                if h & 1 and not (_free(dense, net[0], l, nx, y) and _free(dense, net[0], l, x, ny)):
+                                    continue
+                                c = 14 if h & 1 else 10
+                            else:
+                                nl, nx, ny = l + (1 if h == 8 else -1), x, y
+                                if not (_free(dense, net[0], l, x, y) and _free(dense, net[0], nl, x, y)):
+                                    continue
+                                c = 50
+                            v = d[l, y, x] + c + int(price[nl, ny, nx])
+                            if v < d[nl, ny, nx]:
+                                d[nl, ny, nx] = v
+                                changed = True
+            if not changed:
+                break
+        want = d[gl, gy, gx]
+        assert (cost == oracle.lo_inf()) == (want >= INF)
+        if want < INF:
+            assert cost == want
+            # the path pays exactly its cost
+            total = 0
+            cells = [(int(c) // (32 * 32), (int(c) // 32) % 32, int(c) % 32) for c in path[::-1]]
+            for (l0, y0, x0), (l1, y1, x1) in zip(cells, cells[1:]):
+                step = 50 if l0 != l1 else (14 if (x0 != x1 and y0 != y1) else 10)
+                total += step + int(price[l1, y1, x1])
+            assert total == cost
