@@ -64,10 +64,12 @@ struct SweepLaunch {
   const volatile uint32_t* cancel;  // host-mapped flag or nullptr
 };
 
-// One width class of the frontier form (lattice_frontier.cu).  A net's
-// label words (label << 32 | ~list stamp, window layout [layer][y][x]) start
-// at word plan.dist_offset of `words`, and its three queue lists at entry
-// 3 * dist_offset of `lists`; dist_offset is a multiple of 128 cells.
+// One width class of the frontier form (lattice_frontier.cu).  The kernel
+// is persistent: each resident warp group owns one workspace slot and reuses
+// it for every net it takes.  Slot s holds `slab_cells` label words
+// (label << 32 | ~list stamp, window layout [layer][y][x]) at
+// words + s * slab_cells, and three queue lists of `list_cap` entries at
+// lists + s * 3 * list_cap.
 struct FrontierLaunch {
   LatticeDeviceView lat;
   const apgar_b200_lattice_net* nets;
@@ -77,6 +79,13 @@ struct FrontierLaunch {
   uint32_t bucket_width;
   unsigned long long* words;
   uint32_t* lists;
+  uint64_t slab_cells;  // label words per slot (>= the class's largest padded window)
+  uint32_t list_cap;    // entries per queue list per slot
+  uint32_t slots;       // workspace slots of this class (resident groups)
+  // per_net != 0: every net has its own slab at plan.dist_offset (words) and
+  // lists at 3 * plan.dist_offset (entries), used when all of them fit; the
+  // slots then only bound the number of groups
+  uint32_t per_net;
   apgar_b200_lattice_result* results;
   uint32_t* path_arena;
   uint64_t path_arena_capacity;

@@ -42,6 +42,8 @@
 // join (a lowered cell joins the current level's next list or the far list,
 // never both in one level, because its key only falls).  So no list ever
 // holds more entries than the window has cells.
+// Queue lists hold at most `list_cap` entries per slot; a net whose list
+// would outgrow it is reported REJECTED (never a truncated search).
 // Queue entries are packed cells (layer << 28 | y << 14 | x, window-local).
 // Appends take one packed warp scan and one shared atomic per warp and list.
 #include <cuda_runtime.h>
@@ -153,6 +155,7 @@ __device__ __forceinline__ uint32_t blocked3(const uint32_t* row, int X) {
 // together, then the 64-bit atomicMins.  Lowered neighbours whose list stamp
 // this call set are flagged in cur_mask (next round's list) or far_mask (far
 // list); ne[d] holds the packed cell.
+template <bool kPriced>
 __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const Window& win,
                                             uint32_t e, unsigned long long* words, uint32_t thr,
                                             uint32_t cur_low, uint32_t far_low,
@@ -185,7 +188,7 @@ __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const 
 #pragma unroll
   for (int d = 0; d < 10; ++d) {
     price[d] = 0u;
-    if (cell_cost != nullptr && (inside & (1u << d))) {
+    if (kPriced && (inside & (1u << d))) {
       const int nl = d == 8 ? l - 1 : (d == 9 ? l + 1 : l);
       const int px = d < 8 ? X + fdx(d) : X, py = d < 8 ? Y + fdy(d) : Y;
       price[d] = __ldg(cell_cost + (static_cast<size_t>(nl) * lat.height + py) * lat.width + px);
@@ -234,7 +237,7 @@ __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const 
     cand[d] = gv + cost + price[d];
     low[d] = 0u;
     old[d] = 0ull;
-    if ((legal & (1u << d)) && cand[d] >= kLabelInf) {
+    if (kPriced && (legal & (1u << d)) && cand[d] >= kLabelInf) {
       overflow = true;
       continue;
     }
@@ -287,7 +290,9 @@ struct GroupShared {
   uint32_t sums[16];
 };
 
-template <int G>
+// kPriced: the plan carries per-cell entry prices (p.cell_cost != nullptr);
+// the unpriced instantiation has no price loads or overflow tests at all.
+template <int G, bool kPriced>
 __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
     lattice_frontier_kernel(FrontierLaunch p) {
   constexpr int kGroups = frontier_groups_per_block(G);
@@ -302,6 +307,11 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
   GroupShared& sh = shared_groups[gi];
   const LatticeDeviceView& lat = p.lat;
   const uint32_t orth = lat.orth, diag = lat.diag, via = lat.via;
+  const uint32_t slot = blockIdx.x * kGroups + gi;
+  if (slot >= p.slots) return;  // whole group: no workspace slot of its own
+  unsigned long long* const slot_words = p.words + static_cast<uint64_t>(slot) * p.slab_cells;
+  uint32_t* const slot_lists = p.lists + static_cast<uint64_t>(slot) * 3u * p.list_cap;
+  const uint32_t cap = p.list_cap;
 
   for (;;) {
     if (tid == 0) sh.plan = atomicAdd(p.next_plan, 1u);
@@ -322,10 +332,13 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
     const int sx = static_cast<int>(net.start_x) - win.x0, sy = static_cast<int>(net.start_y) - win.y0;
     const uint32_t cells = static_cast<uint32_t>(lat.layers) * win.w * win.h;
     const uint32_t padded = (cells + 127u) & ~127u;
-    unsigned long long* words = p.words + plan.dist_offset;
-    uint32_t* list_a = p.lists + 3 * plan.dist_offset;
-    uint32_t* list_b = list_a + cells;
-    uint32_t* list_c = list_b + cells;
+    // a list never holds more entries than the net has cells, so the three
+    // lists sit that far apart (inside a slot the cap binds above it)
+    const uint32_t span = p.per_net ? cells : (cells < cap ? cells : cap);
+    unsigned long long* words = p.per_net ? p.words + plan.dist_offset : slot_words;
+    uint32_t* list_a = p.per_net ? p.lists + 3ull * plan.dist_offset : slot_lists;
+    uint32_t* list_b = list_a + span;
+    uint32_t* list_c = list_b + span;
 
     // clear the net's label words (16-byte stores over the padded slab)
     {
@@ -409,8 +422,8 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
           if (valid) {
             ++expanded;
             bool overflow = false;
-            expand_cell(lat, win, cur[i], words, thr, cur_low, far_low, p.cell_cost, ne, cur_mask,
-                        far_mask, overflow);
+            expand_cell<kPriced>(lat, win, cur[i], words, thr, cur_low, far_low, p.cell_cost, ne,
+                                 cur_mask, far_mask, overflow);
             if (overflow) sh.overflow = 1u;
           }
           // one packed warp scan places both lists' entries
@@ -429,14 +442,32 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
           }
           at_cur = __shfl_sync(0xFFFFFFFFu, at_cur, 0) + (packed & 0xFFFFu) - nc;
           at_far = __shfl_sync(0xFFFFFFFFu, at_far, 0) + (packed >> 16) - nfar;
+          if (p.per_net) {
+            // a per-net list spans the net's cells: it cannot overflow
 #pragma unroll
-          for (int d = 0; d < 10; ++d) {
-            if (cur_mask & (1u << d)) nxt[at_cur++] = ne[d];
-            if (far_mask & (1u << d)) far[at_far++] = ne[d];
+            for (int d = 0; d < 10; ++d) {
+              if (cur_mask & (1u << d)) nxt[at_cur++] = ne[d];
+              if (far_mask & (1u << d)) far[at_far++] = ne[d];
+            }
+          } else {
+            bool lost = false;
+#pragma unroll
+            for (int d = 0; d < 10; ++d) {
+              if (cur_mask & (1u << d)) {
+                if (at_cur < span) nxt[at_cur] = ne[d]; else lost = true;
+                ++at_cur;
+              }
+              if (far_mask & (1u << d)) {
+                if (at_far < span) far[at_far] = ne[d]; else lost = true;
+                ++at_far;
+              }
+            }
+            if (lost) sh.overflow = 1u;  // a queue list is full: the net is rejected
           }
         }
         fsync<G>(barrier_id);
         n = *count;
+        if (sh.overflow != 0u) break;  // uniform: read after the barrier
         uint32_t* t = cur;
         cur = nxt;
         nxt = t;
@@ -494,7 +525,7 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
               }
               // the move into the current cell paid its entry price
               const uint32_t here_price =
-                  p.cell_cost == nullptr
+                  !kPriced
                       ? 0u
                       : __ldg(p.cell_cost + (static_cast<size_t>(cl) * lat.height + (win.y0 + cy)) *
                                                 lat.width + (win.x0 + cx));
@@ -548,30 +579,58 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
 }
 
 template <int G>
-cudaError_t launch_frontier_g(const FrontierLaunch& launch, int sm_count, cudaStream_t stream) {
+cudaError_t resident_groups_g(int sm_count, uint32_t* out) {
+  // slots for the leaner instantiation: with the other, groups beyond the
+  // resident ones start as others finish (no group waits on another) and find
+  // the work-stealing queue drained
   constexpr int kGroups = frontier_groups_per_block(G);
-  int per_sm = 0;
+  int plain = 0, priced = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &per_sm, lattice_frontier_kernel<G>, kGroups * G * 32, 0);
+      &plain, lattice_frontier_kernel<G, false>, kGroups * G * 32, 0);
+  if (e == cudaSuccess) {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &priced, lattice_frontier_kernel<G, true>, kGroups * G * 32, 0);
+  }
   if (e != cudaSuccess) return e;
-  const unsigned needed = (launch.plan_count + kGroups - 1) / kGroups;
-  const unsigned resident = static_cast<unsigned>(max(1, per_sm) * max(1, sm_count));
-  const unsigned grid = needed < resident ? needed : resident;
-  lattice_frontier_kernel<G><<<grid, kGroups * G * 32, 0, stream>>>(launch);
+  *out = static_cast<uint32_t>(max(1, max(plain, priced)) * max(1, sm_count) * kGroups);
+  return cudaSuccess;
+}
+
+template <int G>
+cudaError_t launch_frontier_g(const FrontierLaunch& launch, cudaStream_t stream) {
+  constexpr int kGroups = frontier_groups_per_block(G);
+  // one group per workspace slot; the host sizes slots to the resident groups
+  const unsigned grid = (launch.slots + kGroups - 1) / kGroups;
+  if (launch.cell_cost != nullptr) {
+    lattice_frontier_kernel<G, true><<<grid, kGroups * G * 32, 0, stream>>>(launch);
+  } else {
+    lattice_frontier_kernel<G, false><<<grid, kGroups * G * 32, 0, stream>>>(launch);
+  }
   return cudaGetLastError();
 }
 
 }  // namespace
 
-cudaError_t launch_lattice_frontier(int warps_per_net, const FrontierLaunch& launch, int sm_count,
-                                    cudaStream_t stream) {
-  if (launch.plan_count == 0) return cudaSuccess;
+cudaError_t lattice_frontier_resident_groups(int warps_per_net, int sm_count, uint32_t* out) {
   switch (warps_per_net) {
-    case 1: return launch_frontier_g<1>(launch, sm_count, stream);
-    case 2: return launch_frontier_g<2>(launch, sm_count, stream);
-    case 4: return launch_frontier_g<4>(launch, sm_count, stream);
-    case 8: return launch_frontier_g<8>(launch, sm_count, stream);
-    case 16: return launch_frontier_g<16>(launch, sm_count, stream);
+    case 1: return resident_groups_g<1>(sm_count, out);
+    case 2: return resident_groups_g<2>(sm_count, out);
+    case 4: return resident_groups_g<4>(sm_count, out);
+    case 8: return resident_groups_g<8>(sm_count, out);
+    case 16: return resident_groups_g<16>(sm_count, out);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+cudaError_t launch_lattice_frontier(int warps_per_net, const FrontierLaunch& launch, int,
+                                    cudaStream_t stream) {
+  if (launch.plan_count == 0 || launch.slots == 0) return cudaSuccess;
+  switch (warps_per_net) {
+    case 1: return launch_frontier_g<1>(launch, stream);
+    case 2: return launch_frontier_g<2>(launch, stream);
+    case 4: return launch_frontier_g<4>(launch, stream);
+    case 8: return launch_frontier_g<8>(launch, stream);
+    case 16: return launch_frontier_g<16>(launch, stream);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -28,6 +28,7 @@ cudaError_t launch_accumulate_cells(const apgar_b200_lattice_result* results, ui
                                     int sm_count, cudaStream_t stream);
 cudaError_t launch_lattice_frontier(int warps_per_net, const FrontierLaunch& launch, int sm_count,
                                     cudaStream_t stream);
+cudaError_t lattice_frontier_resident_groups(int warps_per_net, int sm_count, uint32_t* out);
 cudaError_t launch_price_update(uint32_t count, const uint32_t* usage, uint64_t factor,
                                 uint64_t next_factor, uint64_t hist_inc, uint64_t capacity,
                                 uint64_t max_value, uint64_t* present, uint64_t* history,
@@ -52,7 +53,20 @@ struct ClassRange {
   uint32_t begin = 0;  // into plans
   uint32_t count = 0;
   int max_rows = 0;
+  // frontier workspace: `slots` persistent slots of `slab_cells` label words
+  // and 3 x `list_cap` queue entries, starting at these pool offsets
+  uint64_t slab_cells = 0;
+  uint32_t list_cap = 0;
+  uint32_t slots = 0;
+  uint64_t words_offset = 0;
+  uint64_t lists_offset = 0;
 };
+
+// Queue entries per list per frontier slot (a net needing more is rejected).
+constexpr uint64_t kMaxListEntries = 1ull << 22;
+// Frontier workspace above which nets share persistent slot slabs instead of
+// owning one slab each.
+constexpr uint64_t kPerNetFrontierBytes = 24ull << 30;
 
 struct PlanObject {
   LatticeObject* lattice = nullptr;
@@ -62,6 +76,7 @@ struct PlanObject {
   uint32_t max_sweeps = 0;  // sweeps (SWEEP) or rounds (FRONTIER)
   uint32_t generator = APGAR_B200_LATTICE_SWEEP;
   uint32_t bucket_width = 0;
+  bool per_net = false;  // FRONTIER: one slab per net (else persistent slots)
   const uint32_t* cell_cost = nullptr;  // caller-owned device prices (frontier only)
   uint32_t* cancel_host = nullptr;  // pinned, mapped; polled by the kernels
   uint32_t* cancel_dev = nullptr;
@@ -249,6 +264,8 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
   plan->classes.clear();
   uint64_t dist_cells = 0;
   uint64_t arena_cells = 0;
+  uint64_t arena_lists = 0;    // frontier queue entries over all slots
+  uint64_t per_net_cells = 0;  // frontier: padded window cells over all nets
   for (int ci = 0; ci < kClassCount; ++ci) {
     std::vector<uint32_t>& m = members[ci];
     if (m.empty()) continue;
@@ -267,13 +284,15 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
       NetPlan np{};
       np.net = i;
       if (frontier) {
-        // window layout [layer][y][x]; slabs padded to 128 cells
+        // window layout [layer][y][x] in the slot's slab, padded to 128 cells
         np.transposed = 0;
         np.rows = n.win_h;
         np.width = n.win_w;
         np.pitch = n.win_w;
-        np.dist_offset = dist_cells;
-        dist_cells += (static_cast<uint64_t>(v.layers) * n.win_w * n.win_h + 127ull) & ~127ull;
+        const uint64_t padded = (static_cast<uint64_t>(v.layers) * n.win_w * n.win_h + 127ull) & ~127ull;
+        np.dist_offset = per_net_cells;  // used when every net gets its own slab
+        per_net_cells += padded;
+        range.slab_cells = std::max<uint64_t>(range.slab_cells, padded);
       } else {
         np.transposed = n.win_h > n.win_w ? 1u : 0u;
         np.rows = np.transposed ? n.win_w : n.win_h;
@@ -290,6 +309,20 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
                          kMaxSmemPerBlock) {
       return set_error(APGAR_B200_UNSUPPORTED, "window too tall for the shared-memory row map");
     }
+    if (frontier) {
+      uint32_t resident = 0;
+      APGAR_B200_CUDA("cudaOccupancyMaxActiveBlocksPerMultiprocessor",
+                      lattice_frontier_resident_groups(range.warps_per_net, plan->sm_count, &resident));
+      range.slots = std::min<uint32_t>(resident, range.count);
+      range.list_cap = static_cast<uint32_t>(std::min<uint64_t>(range.slab_cells, kMaxListEntries));
+      // slot slabs are spaced by the largest window plus a 4 KB skew, so that
+      // equal offsets of different slots do not alias in the L2
+      range.slab_cells += 512;
+      range.words_offset = dist_cells;
+      dist_cells += static_cast<uint64_t>(range.slots) * range.slab_cells;
+      range.lists_offset = arena_lists;
+      arena_lists += static_cast<uint64_t>(range.slots) * 3ull * range.list_cap;
+    }
     plan->classes.push_back(range);
   }
   plan->label_cells = dist_cells;
@@ -298,8 +331,16 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
   APGAR_B200_CUDA("cudaMalloc(nets)", plan->nets.ensure(std::max<uint32_t>(count, 1)));
   APGAR_B200_CUDA("cudaMalloc(plans)", plan->plans.ensure(std::max<size_t>(plans.size(), 1)));
   if (frontier) {
+    // Every net gets its own slab (8 B words + 3 x 4 B list entries per
+    // cell) when that fits the per-net budget; otherwise the persistent
+    // groups reuse their slot slabs net after net.
+    plan->per_net = per_net_cells * 20ull <= kPerNetFrontierBytes;
+    if (plan->per_net) {
+      dist_cells = per_net_cells;
+      arena_lists = 3ull * per_net_cells;
+    }
     APGAR_B200_CUDA("cudaMalloc(label words)", plan->words.ensure(std::max<uint64_t>(dist_cells, 128)));
-    APGAR_B200_CUDA("cudaMalloc(queue lists)", plan->lists.ensure(std::max<uint64_t>(3 * dist_cells, 3)));
+    APGAR_B200_CUDA("cudaMalloc(queue lists)", plan->lists.ensure(std::max<uint64_t>(arena_lists, 3)));
   } else {
     APGAR_B200_CUDA("cudaMalloc(label slabs)", plan->dist_pool.ensure(std::max<uint64_t>(dist_cells, 4)));
   }
@@ -390,6 +431,16 @@ int execute_plan(PlanObject* plan, cudaStream_t stream) {
       FrontierLaunch fl = fbase;
       fl.plans = plan->plans.get() + c.begin;
       fl.plan_count = c.count;
+      fl.words = plan->words.get() + c.words_offset;
+      fl.lists = plan->lists.get() + c.lists_offset;
+      fl.slab_cells = c.slab_cells;
+      fl.list_cap = c.list_cap;
+      fl.slots = c.slots;
+      fl.per_net = plan->per_net ? 1u : 0u;
+      if (plan->per_net) {
+        fl.words = plan->words.get();
+        fl.lists = plan->lists.get();
+      }
       fl.next_plan = reinterpret_cast<unsigned int*>(plan->counters.get() + 2 + k);
       APGAR_B200_CUDA("lattice frontier launch",
                       launch_lattice_frontier(c.warps_per_net, fl, plan->sm_count, s));

@@ -225,3 +225,64 @@ def config_medium(seed: int = 2, nets: int = 4096, size: int = 2048):
 
 def window_cells(lat: Lattice, nets: np.ndarray) -> np.ndarray:
     return nets["win_w"].astype(np.int64) * nets["win_h"].astype(np.int64) * lat.layers
+
+
+def make_multi_terminal_nets(lat: Lattice, seed: int, count: int, hpwl_median: float,
+                             hpwl_sigma: float, min_terminals: int = 2, max_terminals: int = 6,
+                             margin: int = WINDOW_MARGIN) -> tuple[np.ndarray, np.ndarray]:
+    """Nets with ``min_terminals``..``max_terminals`` terminals (uniform) on free
+    cells inside a bounding box whose half-perimeter is lognormal(ln median,
+    sigma), split into 2-pin segments along a Manhattan minimum spanning tree
+    of the terminals (Prim).  Returns (segments as two-terminal net records
+    with bbox + margin windows, owning net index per segment)."""
+    rng = np.random.default_rng(seed)
+    free = ~lat.blocked_dense()
+    segs, owner = [], []
+    made = 0
+    while made < count:
+        hp = max(2, int(round(math.exp(math.log(hpwl_median) + hpwl_sigma * rng.standard_normal()))))
+        bw = min(lat.width, max(1, int(round(hp * rng.random()))) + 1)
+        bh = min(lat.height, max(1, hp - bw + 1) + 1)
+        bx = int(rng.integers(0, lat.width - bw + 1))
+        by = int(rng.integers(0, lat.height - bh + 1))
+        k = int(rng.integers(min_terminals, max_terminals + 1))
+        terms = []
+        for _ in range(64 * k):
+            x = bx + int(rng.integers(0, bw))
+            y = by + int(rng.integers(0, bh))
+            l = int(rng.integers(0, lat.layers))
+            if free[l, y, x] and (l, x, y) not in terms:
+                terms.append((l, x, y))
+                if len(terms) == k:
+                    break
+        if len(terms) < 2:
+            continue
+        # Prim's MST under Manhattan distance (ties by terminal order)
+        in_tree = [0]
+        rest = list(range(1, len(terms)))
+        while rest:
+            best = None
+            for a in in_tree:
+                for b in rest:
+                    d = abs(terms[a][1] - terms[b][1]) + abs(terms[a][2] - terms[b][2])
+                    if best is None or d < best[0]:
+                        best = (d, a, b)
+            _, a, b = best
+            (sl, sx, sy), (gl, gx, gy) = terms[a], terms[b]
+            x0, y0, w, h = _window(lat, sx, sy, gx, gy, margin)
+            segs.append((sl, sx, sy, gl, gx, gy, x0, y0, w, h))
+            owner.append(made)
+            in_tree.append(b)
+            rest.remove(b)
+        made += 1
+    return np.array(segs, dtype=NET_DTYPE), np.array(owner, dtype=np.int64)
+
+
+def config_negotiated(seed: int = 3, nets: int = 16384, size: int = 4096, layers: int = 6):
+    """6 layers of 4096x4096 (25% blocked, rectangles + pad keep-outs as in the
+    medium configuration), 16384 nets with 2-6 terminals split into 2-pin
+    segments, half-perimeter lognormal(300, 1.2), bbox + 32 windows; one
+    routing resource per cell with capacity 1."""
+    lat = make_lattice(seed, layers, size, 0.25, pads=True)
+    segs, owner = make_multi_terminal_nets(lat, seed + 1000, nets, 300.0, 1.2)
+    return lat, segs, owner
