@@ -45,4 +45,19 @@ struct GraphLaunch {
   const volatile uint32_t* cancel;  // host-mapped flag or nullptr
 };
 
+struct PathCheckLaunch {
+  const apgar_b200_node_v1* nodes;
+  uint32_t node_count;
+  uint32_t orth, diag, bend;
+  const apgar_b200_batch_query_v1* queries;
+  const apgar_b200_policy_edge_v1* policy;
+  const apgar_b200_batch_result_v1* results;
+  const apgar_b200_compact_path_v1* compact;
+  const uint32_t* states;
+  uint64_t state_count;
+  uint64_t* visited;  // [query][ceil(9N / 64)] scratch bits
+  apgar_b200_path_verdict* out;
+  uint32_t query_count;
+};
+
 }  // namespace apgar_b200

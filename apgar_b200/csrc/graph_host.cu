@@ -32,6 +32,7 @@ static_assert(sizeof(apgar_b200_route_result_header_v1) == 64, "DeviceRouteResul
 namespace apgar_b200 {
 
 cudaError_t launch_graph_search(const GraphLaunch& launch, cudaStream_t stream);
+cudaError_t launch_validate_paths(const PathCheckLaunch& launch, cudaStream_t stream);
 cudaError_t launch_graph_pack(apgar_b200_compact_path_v1* compact, uint32_t count,
                               uint64_t states_per_query, const uint32_t* stage, uint32_t* packed,
                               unsigned long long* total, int sm_count, cudaStream_t stream);
@@ -93,6 +94,7 @@ struct ViewObject {
   uint64_t persistent_bytes = 0;
   DeviceBuffer<uint32_t> neighbors;
   DeviceBuffer<uint8_t> legal_dev;
+  DeviceBuffer<apgar_b200_node_v1> nodes_dev;  // full records, for path validation
   Lease lease;
   Workspace ws;
   uint32_t* cancel_host = nullptr;
@@ -472,6 +474,10 @@ extern "C" int apgar_b200_view_upload(const apgar_b200_compiled_header_v1* heade
     APGAR_B200_CUDA("cudaMalloc(legal)", v->legal_dev.ensure(node_count));
     APGAR_B200_CUDA("cudaMemcpy(legal)", cudaMemcpy(v->legal_dev.get(), v->legal.data(), node_count,
                                                     cudaMemcpyHostToDevice));
+    APGAR_B200_CUDA("cudaMalloc(nodes)", v->nodes_dev.ensure(node_count));
+    APGAR_B200_CUDA("cudaMemcpy(nodes)", cudaMemcpy(v->nodes_dev.get(), nodes,
+                                                    node_count * sizeof(apgar_b200_node_v1),
+                                                    cudaMemcpyHostToDevice));
     *out_view = v.release();
     clear_error();
     return APGAR_B200_OK;
@@ -674,4 +680,79 @@ extern "C" int apgar_b200_readback_route(void* pending, apgar_b200_route_result_
 extern "C" int apgar_b200_release_route(void* pending) {
   delete static_cast<PendingRoute*>(pending);
   return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_validate_compact_paths(
+    void* view, const apgar_b200_batch_query_v1* queries, uint32_t query_count,
+    const apgar_b200_policy_edge_v1* policy_edges, uint64_t policy_edge_count,
+    const apgar_b200_batch_result_v1* results, const apgar_b200_compact_path_v1* compact_paths,
+    const uint32_t* path_states, uint64_t path_state_count, apgar_b200_path_verdict* verdicts) {
+  if (view == nullptr || verdicts == nullptr ||
+      (query_count > 0 && (queries == nullptr || results == nullptr || compact_paths == nullptr)) ||
+      (policy_edge_count > 0 && policy_edges == nullptr) ||
+      (path_state_count > 0 && path_states == nullptr)) {
+    return invariant("path validation received a null argument");
+  }
+  auto* v = static_cast<ViewObject*>(view);
+  if (int rc = check_device(v->device); rc != APGAR_B200_OK) return rc;
+  // policy slices must stay inside the supplied edges (a malformed query is
+  // an invariant failure of the caller, not a path verdict)
+  for (uint32_t i = 0; i < query_count; ++i) {
+    if (static_cast<uint64_t>(queries[i].policy_offset) + queries[i].policy_count > policy_edge_count) {
+      return invariant("path validation query names policy edges outside the batch");
+    }
+  }
+  try {
+    const uint64_t n = v->legal.size();
+    const uint64_t words = (9u * n + 63u) / 64u;
+    DeviceBuffer<apgar_b200_batch_query_v1> d_q;
+    DeviceBuffer<apgar_b200_policy_edge_v1> d_pol;
+    DeviceBuffer<apgar_b200_batch_result_v1> d_res;
+    DeviceBuffer<apgar_b200_compact_path_v1> d_cp;
+    DeviceBuffer<uint32_t> d_states;
+    DeviceBuffer<uint64_t> d_visited;
+    DeviceBuffer<apgar_b200_path_verdict> d_out;
+    const uint64_t Q = std::max<uint64_t>(query_count, 1);
+    APGAR_B200_CUDA("cudaMalloc(queries)", d_q.ensure(Q));
+    APGAR_B200_CUDA("cudaMalloc(policy)", d_pol.ensure(std::max<uint64_t>(policy_edge_count, 1)));
+    APGAR_B200_CUDA("cudaMalloc(results)", d_res.ensure(Q));
+    APGAR_B200_CUDA("cudaMalloc(compact)", d_cp.ensure(Q));
+    APGAR_B200_CUDA("cudaMalloc(states)", d_states.ensure(std::max<uint64_t>(path_state_count, 1)));
+    APGAR_B200_CUDA("cudaMalloc(visited)", d_visited.ensure(Q * words));
+    APGAR_B200_CUDA("cudaMalloc(verdicts)", d_out.ensure(Q));
+    if (query_count > 0) {
+      APGAR_B200_CUDA("cudaMemcpy(queries)", cudaMemcpy(d_q.get(), queries, query_count * sizeof(*queries), cudaMemcpyHostToDevice));
+      APGAR_B200_CUDA("cudaMemcpy(results)", cudaMemcpy(d_res.get(), results, query_count * sizeof(*results), cudaMemcpyHostToDevice));
+      APGAR_B200_CUDA("cudaMemcpy(compact)", cudaMemcpy(d_cp.get(), compact_paths, query_count * sizeof(*compact_paths), cudaMemcpyHostToDevice));
+    }
+    if (policy_edge_count > 0) {
+      APGAR_B200_CUDA("cudaMemcpy(policy)", cudaMemcpy(d_pol.get(), policy_edges, policy_edge_count * sizeof(*policy_edges), cudaMemcpyHostToDevice));
+    }
+    if (path_state_count > 0) {
+      APGAR_B200_CUDA("cudaMemcpy(states)", cudaMemcpy(d_states.get(), path_states, path_state_count * 4, cudaMemcpyHostToDevice));
+    }
+    PathCheckLaunch L{};
+    L.nodes = v->nodes_dev.get();
+    L.node_count = static_cast<uint32_t>(n);
+    L.orth = v->header.orthogonal_step;
+    L.diag = v->header.diagonal_step;
+    L.bend = v->header.bend;
+    L.queries = d_q.get();
+    L.policy = d_pol.get();
+    L.results = d_res.get();
+    L.compact = d_cp.get();
+    L.states = d_states.get();
+    L.state_count = path_state_count;
+    L.visited = d_visited.get();
+    L.out = d_out.get();
+    L.query_count = query_count;
+    APGAR_B200_CUDA("path validation launch", launch_validate_paths(L, nullptr));
+    if (query_count > 0) {
+      APGAR_B200_CUDA("cudaMemcpy(verdicts)", cudaMemcpy(verdicts, d_out.get(), query_count * sizeof(*verdicts), cudaMemcpyDeviceToHost));
+    }
+    clear_error();
+    return APGAR_B200_OK;
+  } catch (const std::bad_alloc&) {
+    return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "host allocation failed during path validation");
+  }
 }

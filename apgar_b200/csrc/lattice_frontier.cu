@@ -98,19 +98,6 @@ __device__ __forceinline__ uint32_t heuristic(const LatticeDeviceView& lat, cons
   return planar + static_cast<uint32_t>(abs(l - win.gl)) * lat.via;
 }
 
-// Free bits of window cells x-1..x+1 (bits 0..2) in row y of layer l; cells
-// outside the window read as blocked.
-__device__ __forceinline__ uint32_t free3(const LatticeDeviceView& lat, const Window& win, int l,
-                                          int x, int y) {
-  if (y < 0 || y >= win.h) return 0u;
-  const uint32_t* row =
-      lat.blocked + (static_cast<size_t>(l) * lat.height + (win.y0 + y)) * lat.words;
-  uint32_t f = ~fetch_bits32(row, lat.words, win.x0 + x - 1) & 7u;
-  if (x == 0) f &= ~1u;
-  if (x + 1 >= win.w) f &= ~4u;
-  return f;
-}
-
 __device__ __forceinline__ bool cell_free_w(const LatticeDeviceView& lat, const Window& win, int l,
                                             int x, int y) {
   if (l < 0 || l >= lat.layers || x < 0 || y < 0 || x >= win.w || y >= win.h) return false;

@@ -51,6 +51,10 @@ RESULT_DTYPE = np.dtype([
 COMPACT_DTYPE = np.dtype([("schema_version", "<u4"), ("state_count", "<u4"), ("query_id", "<u8"),
                           ("workspace_owner", "<u8"), ("state_offset", "<u8")])
 POLICY_EDGE_DTYPE = np.dtype([("physical_edge_index", "<u4"), ("reserved", "<u4"), ("adjustment", "<u8")])
+VERDICT_DTYPE = np.dtype([("code", "<u4"), ("reserved", "<u4"), ("failing_index", "<u8"),
+                          ("total_cost", "<u8")])
+PATH_CODES = {0: "ok", 1: "bounds", 2: "endpoint", 3: "cycle", 4: "heading", 5: "edge",
+              6: "banned", 7: "not_reached"}
 ROUTE_HEADER_DTYPE = np.dtype([
     ("schema_version", "<u4"), ("compiler_version", "<u4"), ("start_node", "<u4"), ("goal_node", "<u4"),
     ("source_board_content_hash", "<u8"), ("compiler_profile_fingerprint", "<u8"),
@@ -166,6 +170,22 @@ class View:
             _vp(policy_edges) if len(policy_edges) else None, ctypes.c_uint64(len(policy_edges)),
             _vp(cancel), ctypes.byref(handle)))
         return PendingBatch(handle, len(queries), 9 * self.node_count)
+
+    def validate_compact_paths(self, queries, policy_edges, results, compact, states):
+        """Device-side structural validation of read-back compact paths; one
+        (code, failing forward index, total cost) record per query."""
+        queries = np.ascontiguousarray(queries)
+        policy_edges = np.ascontiguousarray(policy_edges)
+        results = np.ascontiguousarray(results)
+        compact = np.ascontiguousarray(compact)
+        states = np.ascontiguousarray(states, dtype=np.uint32)
+        out = np.zeros(len(queries), dtype=VERDICT_DTYPE)
+        _check(lib().apgar_b200_validate_compact_paths(
+            self.handle, _vp(queries), ctypes.c_uint32(len(queries)),
+            _vp(policy_edges) if len(policy_edges) else None, ctypes.c_uint64(len(policy_edges)),
+            _vp(results), _vp(compact), _vp(states) if len(states) else None,
+            ctypes.c_uint64(len(states)), _vp(out)))
+        return out
 
     def execute_route(self, start_node, goal_node, generator=GENERATOR_SWEEP, maximum_rounds=100_000,
                       routing_profile_fingerprint=0, maximum_device_bytes=(1 << 64) - 1):

@@ -268,6 +268,38 @@ APGAR_B200_API int apgar_b200_readback_route(void* pending,
                                              apgar_b200_batch_telemetry* telemetry);
 APGAR_B200_API int apgar_b200_release_route(void* pending);
 
+/* Structural validation of untrusted compact paths on the device: the
+ * device-view checks of ValidateAndReconstructCompactGpuPath
+ * (src/gpu/planar_router.cc:969-1067), in the reference's order, for every
+ * query of a batch at once.  The exact-geometry stage that follows them in
+ * the reference (src/gpu/planar_router.cc:1069-1111) stays with the host.
+ * Codes name the reference's invariant ids. */
+enum {
+  APGAR_B200_PATH_OK = 0,
+  APGAR_B200_PATH_BOUNDS = 1,    /* gpu.batch.compact_path.bounds.v1 */
+  APGAR_B200_PATH_ENDPOINT = 2,  /* gpu.batch.compact_path.endpoint.v1 */
+  APGAR_B200_PATH_CYCLE = 3,     /* gpu.batch.compact_path.cycle.v1 */
+  APGAR_B200_PATH_HEADING = 4,   /* gpu.batch.compact_path.heading.v1 */
+  APGAR_B200_PATH_EDGE = 5,      /* gpu.batch.compact_path.edge.v1 */
+  APGAR_B200_PATH_BANNED = 6,    /* gpu.policy.banned_predecessor.v1 */
+  APGAR_B200_PATH_NOT_REACHED = 7 /* the query did not reach its goal: not validated */
+};
+typedef struct apgar_b200_path_verdict {
+  uint32_t code;          /* APGAR_B200_PATH_* */
+  uint32_t reserved;
+  uint64_t failing_index; /* forward index (from the start) of the first failing state */
+  uint64_t total_cost;    /* the path's cost under the query's policy when code == OK */
+} apgar_b200_path_verdict;
+
+/* Validates the compact paths of a batch (host arrays, as read back) against
+ * an uploaded view and the batch's own queries and policy edges; writes one
+ * verdict per query. */
+APGAR_B200_API int apgar_b200_validate_compact_paths(
+    void* view, const apgar_b200_batch_query_v1* queries, uint32_t query_count,
+    const apgar_b200_policy_edge_v1* policy_edges, uint64_t policy_edge_count,
+    const apgar_b200_batch_result_v1* results, const apgar_b200_compact_path_v1* compact_paths,
+    const uint32_t* path_states, uint64_t path_state_count, apgar_b200_path_verdict* verdicts);
+
 /* ======================= B. lattice mode ======================= */
 
 typedef struct apgar_b200_lattice_desc {

@@ -86,6 +86,7 @@ def lib():
         _lib.lo_astar.restype = ctypes.c_uint32
         _lib.lo_sweep_schedule.restype = ctypes.c_uint32
         _lib.go_search.restype = ctypes.c_int
+        _lib.go_validate_compact.restype = ctypes.c_int
         _lib.po_epoch_update.restype = ctypes.c_int
         _lib.po_snapshot_costs.restype = ctypes.c_int
         _lib.po_history_update.restype = ctypes.c_int
@@ -226,6 +227,30 @@ def graph_search(nodes, costs, start, goal, orth_s=0, diag_s=0, bend_s=0, policy
                           ctypes.byref(gc), ctypes.byref(gs), _ptr(path), ctypes.c_uint32(cap),
                           ctypes.byref(plen))
     return bool(reached), gc.value, gs.value, path[: plen.value].copy(), labels
+
+
+PATH_CODES = {0: "ok", 1: "bounds", 2: "endpoint", 3: "cycle", 4: "heading", 5: "edge",
+              6: "banned", 7: "not_reached"}
+
+
+def validate_compact(nodes, costs, start, goal, reverse_states, goal_state, completion=0,
+                     orth_s=0, diag_s=0, bend_s=0, policy=None):
+    """Structural validation of one compact reverse path.  Returns
+    (code name, total cost, failing forward index)."""
+    L = lib()
+    nodes = np.ascontiguousarray(nodes)
+    rev = np.ascontiguousarray(reverse_states, dtype=np.uint32)
+    pol = np.ascontiguousarray(policy) if policy is not None and len(policy) else None
+    q = GoQuery(start, goal, orth_s, diag_s, bend_s,
+                pol.ctypes.data_as(ctypes.c_void_p) if pol is not None else None,
+                len(pol) if pol is not None else 0)
+    total = ctypes.c_uint64(0)
+    index = ctypes.c_uint64(0)
+    code = L.go_validate_compact(nodes.ctypes.data_as(ctypes.c_void_p), ctypes.c_uint32(len(nodes)),
+                                 GoCosts(*costs), ctypes.byref(q), ctypes.c_uint8(completion),
+                                 ctypes.c_uint32(goal_state), _ptr(rev), ctypes.c_uint64(len(rev)),
+                                 ctypes.byref(total), ctypes.byref(index))
+    return PATH_CODES[code], total.value, index.value
 
 
 def graph_predecessors(nodes, costs, start, labels, orth_s=0, diag_s=0, bend_s=0, policy=None):

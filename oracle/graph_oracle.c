@@ -214,3 +214,89 @@ void go_predecessors(const go_node* nodes, uint32_t node_count, go_costs costs, 
     }
   }
 }
+
+/* Forward walk of a reverse compact path, check by check in the reference's
+ * order (planar_router.cc:969-1067): bounds of a reached path, endpoint
+ * binding, state bounds, then per state in forward order a repeated state,
+ * the start-only heading sentinel, one adjacent compiled legal edge (same
+ * layer, lattice delta of the heading, neighbour and legal bit), a banned
+ * resource, and the checked finite cost sum. */
+int go_validate_compact(const go_node* nodes, uint32_t node_count, go_costs costs,
+                        const go_query* q, uint8_t completion, uint32_t goal_state,
+                        const uint32_t* rev, uint64_t len, uint64_t* total_cost,
+                        uint64_t* failing_index) {
+  static const int dx[8] = {1, 1, 0, -1, -1, -1, 0, 1};
+  static const int dy[8] = {0, 1, 1, 1, 0, -1, -1, -1};
+  const uint64_t states = (uint64_t)node_count * 9u;
+  *total_cost = 0;
+  *failing_index = 0;
+  if (completion != 0) return GO_PATH_NOT_REACHED;
+  if (len == 0 || len > states) return GO_PATH_BOUNDS;
+  const uint32_t start_state = q->start_node * 9u + 8u;
+  if (rev[0] != goal_state || rev[len - 1] != start_state || goal_state / 9u != q->goal_node ||
+      goal_state % 9u >= 8u) {
+    return GO_PATH_ENDPOINT;
+  }
+  for (uint64_t i = 0; i < len; ++i) {
+    if (rev[i] >= states) return GO_PATH_BOUNDS;
+  }
+  uint64_t* visited = (uint64_t*)calloc((states + 63u) / 64u, sizeof(uint64_t));
+  uint64_t total = 0;
+  int code = GO_PATH_OK;
+  for (uint64_t index = 0; index < len && code == GO_PATH_OK; ++index) {
+    const uint64_t r = len - 1u - index;
+    const uint32_t state = rev[r];
+    *failing_index = index;
+    const uint64_t bit = 1ull << (state % 64u);
+    if (visited[state / 64u] & bit) {
+      code = GO_PATH_CYCLE;
+      break;
+    }
+    visited[state / 64u] |= bit;
+    const uint32_t node = state / 9u;
+    if (node >= node_count) {
+      code = GO_PATH_BOUNDS;
+      break;
+    }
+    if (index == 0) {
+      if (state != start_state) code = GO_PATH_ENDPOINT;
+      continue;
+    }
+    const uint32_t pred_state = rev[r + 1u];
+    const uint32_t pred = pred_state / 9u;
+    const uint32_t incoming = state % 9u, pred_heading = pred_state % 9u;
+    if (incoming >= 8u || (pred_heading == 8u && pred_state != start_state)) {
+      code = GO_PATH_HEADING;
+      break;
+    }
+    const go_node* a = &nodes[pred];
+    const go_node* b = &nodes[node];
+    if (a->layer != b->layer || b->lattice_x - a->lattice_x != dx[incoming] ||
+        b->lattice_y - a->lattice_y != dy[incoming] || a->neighbors[incoming] != node ||
+        (a->legal_edges & (1u << incoming)) == 0) {
+      code = GO_PATH_EDGE;
+      break;
+    }
+    const uint32_t edge = physical_edge(nodes, pred, incoming);
+    const uint64_t adj = policy_adjustment(q, edge);
+    if (adj == GO_INF) {
+      code = GO_PATH_BANNED;
+      break;
+    }
+    /* transition in 128-bit arithmetic, rejected at the sentinel */
+    unsigned __int128 t = (incoming & 1u)
+                              ? (unsigned __int128)costs.diagonal_step + q->diagonal_step_surcharge
+                              : (unsigned __int128)costs.orthogonal_step + q->orthogonal_step_surcharge;
+    if (pred_heading != 8u && pred_heading != incoming) t += (unsigned __int128)costs.bend + q->bend_surcharge;
+    t += adj;
+    uint64_t next;
+    if (t >= GO_INF || !checked_add(total, (uint64_t)t, &next)) {
+      code = GO_PATH_EDGE;
+      break;
+    }
+    total = next;
+  }
+  free(visited);
+  if (code == GO_PATH_OK) *total_cost = total;
+  return code;
+}

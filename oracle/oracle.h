@@ -140,6 +140,27 @@ int go_search(const go_node* nodes, uint32_t node_count, go_costs costs, const g
 void go_predecessors(const go_node* nodes, uint32_t node_count, go_costs costs,
                      const go_query* query, const uint64_t* labels, uint32_t* preds);
 
+/* Structural validation of one untrusted compact reverse path (goal state
+ * first), restating the device-view checks of the reference's
+ * ValidateAndReconstructCompactGpuPath (src/gpu/planar_router.cc:969-1067)
+ * in its order; the exact-geometry stage after them is not restated.
+ * Returns a GO_PATH_* code; *total_cost receives the path cost when OK and
+ * *failing_index the forward index of the first failing state otherwise. */
+enum {
+  GO_PATH_OK = 0,
+  GO_PATH_BOUNDS = 1,    /* gpu.batch.compact_path.bounds.v1 */
+  GO_PATH_ENDPOINT = 2,  /* gpu.batch.compact_path.endpoint.v1 */
+  GO_PATH_CYCLE = 3,     /* gpu.batch.compact_path.cycle.v1 */
+  GO_PATH_HEADING = 4,   /* gpu.batch.compact_path.heading.v1 */
+  GO_PATH_EDGE = 5,      /* gpu.batch.compact_path.edge.v1 */
+  GO_PATH_BANNED = 6,    /* gpu.policy.banned_predecessor.v1 */
+  GO_PATH_NOT_REACHED = 7
+};
+int go_validate_compact(const go_node* nodes, uint32_t node_count, go_costs costs,
+                        const go_query* query, uint8_t completion, uint32_t goal_state,
+                        const uint32_t* reverse_states, uint64_t length, uint64_t* total_cost,
+                        uint64_t* failing_index);
+
 /* ---------------- congestion prices (integer, checked) ---------------- */
 
 /* Allocator epoch update (negotiated_regeneration_plan.cc:676-760):

@@ -95,3 +95,59 @@ def test_fixtures_regenerate_from_the_reference(tmp_path):
     for name in names:
         assert filecmp.cmp(os.path.join(committed, name), os.path.join(tmp_path, name),
                            shallow=False), name
+
+
+def _mutations(case, q, path):
+    """(label, mutated reverse path, policy, expected code) for one reached path."""
+    n = len(case.nodes)
+    out = [("valid", path, q.policy, "ok")]
+    out.append(("truncated start", path[:-1], q.policy, "endpoint"))
+    out.append(("wrong goal", np.concatenate([[path[0] ^ 1], path[1:]]).astype(np.uint32), q.policy,
+                "endpoint"))
+    if len(path) > 3:
+        rep = path.copy()
+        rep[1] = rep[3]
+        out.append(("repeated state", rep, q.policy, None))  # cycle, edge or heading
+        hd = path.copy()
+        node, h = divmod(int(hd[1]), 9)
+        hd[1] = node * 9 + (h + 1) % 8
+        out.append(("turned heading", hd, q.policy, None))
+        oob = path.copy()
+        oob[1] = 9 * n + 3
+        out.append(("state out of range", oob, q.policy, "bounds"))
+    if len(path) > 2:
+        # ban the physical edge of the first move
+        s0, s1 = int(path[-1]), int(path[-2])
+        d = s1 % 9
+        src = s0 // 9
+        edge = src * 8 + d if d < 4 else int(case.nodes[src]["neighbors"][d]) * 8 + d - 4
+        ban = np.zeros(1, dtype=ref_corpus.POLICY_EDGE_DTYPE)
+        ban[0] = (edge, 0, U64_MAX)
+        pol = ban if not len(q.policy) else np.sort(
+            np.concatenate([q.policy[q.policy["physical_edge_index"] != edge], ban]),
+            order="physical_edge_index")
+        out.append(("banned first edge", path, pol, "banned"))
+    return out
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c.name for c in CASES])
+def test_compact_path_validation_pins_the_reference_cost(case):
+    """Valid canonical paths validate with exactly the reference CPU A* cost;
+    each kind of corruption is reported with the reference's invariant."""
+    for q in case.queries:
+        if q.cpu_status != 0:
+            continue
+        ok, cost, goal_state, path, _ = oracle.graph_search(
+            case.nodes, case.costs, q.start_node, q.goal_node, q.orthogonal_surcharge,
+            q.diagonal_surcharge, q.bend_surcharge, q.policy)
+        assert ok and cost == q.cpu_cost
+        for label, rev, pol, want in _mutations(case, q, path):
+            code, total, _ = oracle.validate_compact(
+                case.nodes, case.costs, q.start_node, q.goal_node, rev, goal_state, 0,
+                q.orthogonal_surcharge, q.diagonal_surcharge, q.bend_surcharge, pol)
+            if want is None:
+                assert code in ("cycle", "heading", "edge"), (label, code)
+            else:
+                assert code == want, (case.name, label, code)
+            if label == "valid":
+                assert total == q.cpu_cost
