@@ -95,6 +95,11 @@ struct FrontierLaunch {
   // optional per-cell entry price [layers][height][width] (negotiated
   // congestion snapshot); a move into cell c costs its move cost + cell_cost[c]
   const uint32_t* cell_cost;
+  // optional partial rip-up: a net with skip[net] != 0 is not searched; its
+  // previous result and path (prev_results, packed prev_paths) are carried over
+  const uint8_t* skip;
+  const apgar_b200_lattice_result* prev_results;
+  const uint32_t* prev_paths;
 };
 
 __device__ __forceinline__ uint32_t sat(uint32_t v) { return v < kLabelInf ? v : kLabelInf; }

@@ -306,6 +306,31 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
     const uint32_t plan_index = sh.plan;
     if (plan_index >= p.plan_count) return;  // uniform within the group
     const NetPlan plan = p.plans[plan_index];
+    if (p.skip != nullptr && p.skip[plan.net] != 0u) {  // uniform within the group
+      // kept route: carry the previous result and path into this execution
+      if (g == 0) {
+        apgar_b200_lattice_result res = p.prev_results[plan.net];
+        res.arena_offset = 0;
+        if (res.completion == APGAR_B200_COMPLETION_REACHED && res.path_len > 0) {
+          unsigned long long base = 0;
+          if (lane == 0) base = atomicAdd(p.arena_cursor, static_cast<unsigned long long>(res.path_len));
+          base = __shfl_sync(0xFFFFFFFFu, base, 0);
+          if (base + res.path_len > p.path_arena_capacity) {
+            res.completion = APGAR_B200_COMPLETION_REJECTED;
+            res.cost = APGAR_B200_UNREACHABLE;
+            res.path_len = 0;
+          } else {
+            for (uint32_t j = lane; j < res.path_len; j += 32) {
+              p.path_arena[base + j] = p.prev_paths[res.path_offset + j];
+            }
+            res.arena_offset = base;
+          }
+        }
+        if (lane == 0) p.results[plan.net] = res;
+      }
+      fsync<G>(barrier_id);
+      continue;
+    }
     const apgar_b200_lattice_net net = p.nets[plan.net];
     Window win;
     win.x0 = static_cast<int>(net.win_x0);

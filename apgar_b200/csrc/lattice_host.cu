@@ -34,6 +34,9 @@ cudaError_t launch_price_update(uint32_t count, const uint32_t* usage, uint64_t 
                                 uint64_t max_value, uint64_t* present, uint64_t* history,
                                 uint64_t* total, uint64_t* next_cost, uint32_t* next_cost32,
                                 uint32_t* status, unsigned long long* stats, cudaStream_t stream);
+cudaError_t launch_mark_dirty(const apgar_b200_lattice_result* results, uint32_t count,
+                              const uint32_t* paths, const uint32_t* usage, uint64_t cell_count,
+                              uint32_t capacity, uint8_t* skip, int sm_count, cudaStream_t stream);
 cudaError_t launch_lattice_pack(apgar_b200_lattice_result* results, uint32_t count,
                                 unsigned long long* total, const uint32_t* arena, uint32_t* paths,
                                 int sm_count, cudaStream_t stream);
@@ -78,6 +81,10 @@ struct PlanObject {
   uint32_t bucket_width = 0;
   bool per_net = false;  // FRONTIER: one slab per net (else persistent slots)
   const uint32_t* cell_cost = nullptr;  // caller-owned device prices (frontier only)
+  // partial rip-up (set by a negotiation): kept nets and their previous routes
+  const uint8_t* skip = nullptr;
+  const apgar_b200_lattice_result* prev_results = nullptr;
+  const uint32_t* prev_paths = nullptr;
   uint32_t* cancel_host = nullptr;  // pinned, mapped; polled by the kernels
   uint32_t* cancel_dev = nullptr;
   std::vector<ClassRange> classes;
@@ -405,6 +412,9 @@ int execute_plan(PlanObject* plan, cudaStream_t stream) {
   fbase.arena_cursor = plan->counters.get();
   fbase.cancel = plan->cancel_dev;
   fbase.cell_cost = plan->cell_cost;
+  fbase.skip = plan->skip;
+  fbase.prev_results = plan->prev_results;
+  fbase.prev_paths = plan->prev_paths;
   SweepLaunch base{};
   base.lat = v;
   base.nets = plan->nets.get();
@@ -1063,6 +1073,11 @@ struct NegotiationObject {
   DeviceBuffer<uint64_t> history;
   DeviceBuffer<unsigned long long> stats;  // [round][overused cells, total overuse]
   uint32_t rounds_capacity = 0;
+  // partial rip-up: previous round's routes and the per-net keep flags
+  DeviceBuffer<apgar_b200_lattice_result> prev_results;
+  DeviceBuffer<uint32_t> prev_paths;
+  DeviceBuffer<uint8_t> skip;
+  uint32_t graph_flags = 0;
   cudaStream_t work = nullptr;
   cudaEvent_t entry = nullptr, exit = nullptr;
   cudaGraph_t graph = nullptr;
@@ -1075,7 +1090,12 @@ struct NegotiationObject {
     if (entry != nullptr) cudaEventDestroy(entry);
     if (exit != nullptr) cudaEventDestroy(exit);
     if (work != nullptr) cudaStreamDestroy(work);
-    if (plan != nullptr) plan->cell_cost = nullptr;
+    if (plan != nullptr) {
+      plan->cell_cost = nullptr;
+      plan->skip = nullptr;
+      plan->prev_results = nullptr;
+      plan->prev_paths = nullptr;
+    }
   }
 };
 
@@ -1087,8 +1107,11 @@ bool checked_factor(const apgar_b200_price_policy& p, uint64_t epoch, uint64_t* 
   return true;
 }
 
-// Enqueues a whole negotiation (reset + `rounds` rounds) on n->work.
-int enqueue_negotiation(NegotiationObject* n, uint32_t rounds) {
+// Enqueues a whole negotiation (reset + `rounds` rounds) on n->work.  With
+// `partial`, round r >= 1 reroutes only the nets whose previous route did not
+// reach its goal or crosses a cell overused after round r - 1; the others
+// keep their routes.
+int enqueue_negotiation(NegotiationObject* n, uint32_t rounds, bool partial) {
   cudaStream_t s = n->work;
   APGAR_B200_CUDA("cudaMemsetAsync(history)",
                   cudaMemsetAsync(n->history.get(), 0, n->cells * sizeof(uint64_t), s));
@@ -1100,7 +1123,32 @@ int enqueue_negotiation(NegotiationObject* n, uint32_t rounds) {
     if (!checked_factor(n->policy, r, &factor) || !checked_factor(n->policy, r + 1ull, &next_factor)) {
       return set_error(APGAR_B200_INTERNAL_INVARIANT, "present-price schedule overflowed uint64");
     }
-    if (int rc = execute_plan(n->plan, s); rc != APGAR_B200_OK) return rc;
+    PlanObject* plan = n->plan;
+    if (partial && r > 0) {
+      APGAR_B200_CUDA("mark dirty launch",
+                      launch_mark_dirty(n->prev_results.get(), plan->count, n->prev_paths.get(),
+                                        n->usage.get(), n->cells,
+                                        static_cast<uint32_t>(n->policy.capacity), n->skip.get(),
+                                        plan->sm_count, s));
+      plan->skip = n->skip.get();
+      plan->prev_results = n->prev_results.get();
+      plan->prev_paths = n->prev_paths.get();
+    } else {
+      plan->skip = nullptr;
+    }
+    const int exec_rc = execute_plan(plan, s);
+    plan->skip = nullptr;
+    if (exec_rc != APGAR_B200_OK) return exec_rc;
+    if (partial && r + 1 < rounds) {
+      APGAR_B200_CUDA("cudaMemcpyAsync(previous results)",
+                      cudaMemcpyAsync(n->prev_results.get(), plan->results.get(),
+                                      plan->count * sizeof(apgar_b200_lattice_result),
+                                      cudaMemcpyDeviceToDevice, s));
+      APGAR_B200_CUDA("cudaMemcpyAsync(previous paths)",
+                      cudaMemcpyAsync(n->prev_paths.get(), plan->paths.get(),
+                                      plan->arena_capacity * sizeof(uint32_t),
+                                      cudaMemcpyDeviceToDevice, s));
+    }
     APGAR_B200_CUDA("cudaMemsetAsync(usage)",
                     cudaMemsetAsync(n->usage.get(), 0, n->cells * sizeof(uint32_t), s));
     APGAR_B200_CUDA("usage accumulation launch",
@@ -1143,6 +1191,9 @@ extern "C" int apgar_b200_negotiation_create(void* plan, const apgar_b200_price_
     APGAR_B200_CUDA("cudaMalloc(usage)", n->usage.ensure(cells));
     APGAR_B200_CUDA("cudaMalloc(cell costs)", n->cell_cost.ensure(cells));
     APGAR_B200_CUDA("cudaMalloc(history)", n->history.ensure(cells));
+    APGAR_B200_CUDA("cudaMalloc(previous results)", n->prev_results.ensure(std::max<uint32_t>(p->count, 1)));
+    APGAR_B200_CUDA("cudaMalloc(previous paths)", n->prev_paths.ensure(std::max<uint64_t>(p->arena_capacity, 1)));
+    APGAR_B200_CUDA("cudaMalloc(keep flags)", n->skip.ensure(std::max<uint32_t>(p->count, 1)));
     APGAR_B200_CUDA("cudaStreamCreate", cudaStreamCreateWithFlags(&n->work, cudaStreamNonBlocking));
     APGAR_B200_CUDA("cudaEventCreate", cudaEventCreateWithFlags(&n->entry, cudaEventDisableTiming));
     APGAR_B200_CUDA("cudaEventCreate", cudaEventCreateWithFlags(&n->exit, cudaEventDisableTiming));
@@ -1154,11 +1205,14 @@ extern "C" int apgar_b200_negotiation_create(void* plan, const apgar_b200_price_
   }
 }
 
-extern "C" int apgar_b200_negotiation_run(void* negotiation, uint32_t rounds, uint32_t use_graph,
-                                          void* stream) {
-  if (negotiation == nullptr || rounds == 0 || rounds > 1000) {
-    return set_error(APGAR_B200_INTERNAL_INVARIANT, "negotiation needs 1..1000 rounds");
+extern "C" int apgar_b200_negotiation_run_ex(void* negotiation, uint32_t rounds, uint32_t flags,
+                                             void* stream) {
+  if (negotiation == nullptr || rounds == 0 || rounds > 1000 ||
+      (flags & ~(APGAR_B200_NEGOTIATE_GRAPH | APGAR_B200_NEGOTIATE_PARTIAL)) != 0u) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "negotiation needs 1..1000 rounds and known flags");
   }
+  const bool use_graph = (flags & APGAR_B200_NEGOTIATE_GRAPH) != 0u;
+  const bool partial = (flags & APGAR_B200_NEGOTIATE_PARTIAL) != 0u;
   auto* n = static_cast<NegotiationObject*>(negotiation);
   if (int rc = check_device(n->plan->device); rc != APGAR_B200_OK) return rc;
   const auto caller = static_cast<cudaStream_t>(stream);
@@ -1170,17 +1224,17 @@ extern "C" int apgar_b200_negotiation_run(void* negotiation, uint32_t rounds, ui
   // work runs on the negotiation's own stream, ordered after the caller's
   APGAR_B200_CUDA("cudaEventRecord(entry)", cudaEventRecord(n->entry, caller));
   APGAR_B200_CUDA("cudaStreamWaitEvent", cudaStreamWaitEvent(n->work, n->entry, 0));
-  if (use_graph == 0) {
-    if (int rc = enqueue_negotiation(n, rounds); rc != APGAR_B200_OK) return rc;
+  if (!use_graph) {
+    if (int rc = enqueue_negotiation(n, rounds, partial); rc != APGAR_B200_OK) return rc;
   } else {
-    if (n->exec == nullptr || n->graph_rounds != rounds) {
+    if (n->exec == nullptr || n->graph_rounds != rounds || n->graph_flags != flags) {
       if (n->exec != nullptr) cudaGraphExecDestroy(n->exec);
       if (n->graph != nullptr) cudaGraphDestroy(n->graph);
       n->exec = nullptr;
       n->graph = nullptr;
       APGAR_B200_CUDA("cudaStreamBeginCapture",
                       cudaStreamBeginCapture(n->work, cudaStreamCaptureModeRelaxed));
-      const int rc = enqueue_negotiation(n, rounds);
+      const int rc = enqueue_negotiation(n, rounds, partial);
       cudaGraph_t graph = nullptr;
       const cudaError_t end = cudaStreamEndCapture(n->work, &graph);
       if (rc != APGAR_B200_OK) {
@@ -1191,6 +1245,7 @@ extern "C" int apgar_b200_negotiation_run(void* negotiation, uint32_t rounds, ui
       n->graph = graph;
       APGAR_B200_CUDA("cudaGraphInstantiate", cudaGraphInstantiate(&n->exec, graph, 0));
       n->graph_rounds = rounds;
+      n->graph_flags = flags;
     }
     APGAR_B200_CUDA("cudaGraphLaunch", cudaGraphLaunch(n->exec, n->work));
   }
@@ -1198,6 +1253,12 @@ extern "C" int apgar_b200_negotiation_run(void* negotiation, uint32_t rounds, ui
   APGAR_B200_CUDA("cudaStreamWaitEvent", cudaStreamWaitEvent(caller, n->exit, 0));
   clear_error();
   return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_negotiation_run(void* negotiation, uint32_t rounds, uint32_t use_graph,
+                                          void* stream) {
+  return apgar_b200_negotiation_run_ex(negotiation, rounds,
+                                       use_graph != 0u ? APGAR_B200_NEGOTIATE_GRAPH : 0u, stream);
 }
 
 extern "C" int apgar_b200_negotiation_readback(void* negotiation, uint32_t* usage, uint64_t* history,

@@ -113,7 +113,39 @@ __global__ void accumulate_cells_kernel(const apgar_b200_lattice_result* __restr
   }
 }
 
+// Partial rip-up: a net keeps its route (skip = 1) when it reached its goal
+// and no cell of its path is overused; otherwise it is rerouted.
+__global__ void mark_dirty_kernel(const apgar_b200_lattice_result* __restrict__ results,
+                                  uint32_t count, const uint32_t* __restrict__ paths,
+                                  const uint32_t* __restrict__ usage, uint64_t cell_count,
+                                  uint32_t capacity, uint8_t* __restrict__ skip) {
+  const int lane = threadIdx.x & 31;
+  for (uint32_t n = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5); n < count;
+       n += gridDim.x * (blockDim.x / 32)) {
+    const apgar_b200_lattice_result r = results[n];
+    bool dirty = r.completion != APGAR_B200_COMPLETION_REACHED;
+    for (uint32_t j = lane; !dirty && j < r.path_len; j += 32) {
+      const uint32_t c = paths[r.path_offset + j];
+      if (c >= cell_count || usage[c] > capacity) dirty = true;
+    }
+    dirty = __any_sync(0xFFFFFFFFu, dirty);
+    if (lane == 0) skip[n] = dirty ? 0u : 1u;
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_mark_dirty(const apgar_b200_lattice_result* results, uint32_t count,
+                              const uint32_t* paths, const uint32_t* usage, uint64_t cell_count,
+                              uint32_t capacity, uint8_t* skip, int sm_count, cudaStream_t stream) {
+  if (count == 0) return cudaSuccess;
+  const uint32_t warps = 8;
+  const uint32_t cap = static_cast<uint32_t>(sm_count > 0 ? sm_count * 16 : 2048);
+  const uint32_t blocks = (count + warps - 1) / warps;
+  mark_dirty_kernel<<<blocks < cap ? blocks : cap, warps * 32, 0, stream>>>(
+      results, count, paths, usage, cell_count, capacity, skip);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_price_update(uint32_t count, const uint32_t* usage, uint64_t factor,
                                 uint64_t next_factor, uint64_t hist_inc, uint64_t capacity,

@@ -38,10 +38,13 @@ class Negotiation:
                                                    ctypes.byref(handle)))
         self.handle = handle
 
-    def run(self, rounds: int, use_graph: bool = False, stream: int = 0) -> None:
-        _check(lib().apgar_b200_negotiation_run(self.handle, ctypes.c_uint32(rounds),
-                                                ctypes.c_uint32(1 if use_graph else 0),
-                                                ctypes.c_void_p(stream)))
+    def run(self, rounds: int, use_graph: bool = False, stream: int = 0,
+            partial: bool = False) -> None:
+        """A whole negotiation from zero prices.  ``partial``: from round 1 on,
+        reroute only nets whose route crosses an overused cell."""
+        flags = (1 if use_graph else 0) | (2 if partial else 0)
+        _check(lib().apgar_b200_negotiation_run_ex(self.handle, ctypes.c_uint32(rounds),
+                                                   ctypes.c_uint32(flags), ctypes.c_void_p(stream)))
         self.rounds = rounds
 
     def readback(self):

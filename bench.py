@@ -61,6 +61,9 @@ def parse_args():
                     help="medium: the headline batch; negotiated: 10 rip-up/reroute rounds "
                          "on the 6 x 4096^2 lattice with multi-terminal nets (one CUDA graph)")
     ap.add_argument("--rounds", type=int, default=10)
+    ap.add_argument("--full-ripup", action="store_true",
+                    help="negotiated: reroute every net each round (default: only nets "
+                         "crossing overused cells after round 0)")
     return ap.parse_args()
 
 
@@ -240,15 +243,16 @@ def run_negotiated(args, rank, world, local):
     plan = dev.plan(segs, generator="frontier")
     neg = negotiate.Negotiation(plan, prices.policy(capacity=1))
     stream = torch.cuda.current_stream()
+    partial = not args.full_ripup
     for _ in range(max(args.warmup, 3)):
-        neg.run(args.rounds, use_graph=True, stream=stream.cuda_stream)
+        neg.run(args.rounds, use_graph=True, stream=stream.cuda_stream, partial=partial)
     torch.cuda.synchronize()
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clocks:
         start.record(stream)
         for _ in range(args.steps):
-            neg.run(args.rounds, use_graph=True, stream=stream.cuda_stream)
+            neg.run(args.rounds, use_graph=True, stream=stream.cuda_stream, partial=partial)
         end.record(stream)
         torch.cuda.synchronize()
     ms = start.elapsed_time(end) / args.steps
@@ -265,7 +269,7 @@ def run_negotiated(args, rank, world, local):
     for _ in range(max(1, args.steps // 2)):
         p2 = dev.plan(segs, generator="frontier")
         n2 = negotiate.Negotiation(p2, prices.policy(capacity=1))
-        n2.run(args.rounds, use_graph=False, stream=0)
+        n2.run(args.rounds, use_graph=False, stream=0, partial=partial)
         r2, pa2 = p2.readback()
         n2.close()
         p2.close()
@@ -280,6 +284,7 @@ def run_negotiated(args, rank, world, local):
         "data": "synthetic",
         "config": {"workload": NEG_WORKLOAD, "segments": len(segs), "rounds": args.rounds,
                    "form": "frontier search + fused snapshot prices, Jacobi rounds, one CUDA graph",
+                   "rip_up": "full" if args.full_ripup else "partial (nets crossing overused cells)",
                    "workspace_bytes": plan.info()["workspace_bytes"]},
         "gpu_launches": args.rounds * (plan.info()["kernel_launches"] + 2) * args.steps,
         "e2e": {"value": routes / (e2e_ms / 1000.0), "unit": "routes/s",

@@ -519,6 +519,14 @@ APGAR_B200_API int apgar_b200_negotiation_create(void* plan, const apgar_b200_pr
  * The plan's results and paths hold the last round's routing. */
 APGAR_B200_API int apgar_b200_negotiation_run(void* negotiation, uint32_t rounds, uint32_t use_graph,
                                void* stream);
+/* Flags of apgar_b200_negotiation_run_ex. */
+#define APGAR_B200_NEGOTIATE_GRAPH 1u   /* capture the rounds once as one CUDA graph */
+#define APGAR_B200_NEGOTIATE_PARTIAL 2u /* partial rip-up: from round 1 on, reroute only the
+                                           nets whose route crosses an overused cell (or
+                                           did not reach its goal); the others keep theirs */
+/* apgar_b200_negotiation_run with flags (run == run_ex with GRAPH or 0). */
+APGAR_B200_API int apgar_b200_negotiation_run_ex(void* negotiation, uint32_t rounds, uint32_t flags,
+                                  void* stream);
 /* Waits for the negotiation; copies the last round's usage, the history,
  * the next snapshot prices (each optional, layers*height*width cells) and
  * per-round statistics. */

@@ -16,13 +16,27 @@ from apgar_b200 import negotiate, prices, synth
 pytestmark = pytest.mark.gpu
 
 
-def _cpu_rounds(lat, nets, pol, rounds):
+def _cpu_rounds(lat, nets, pol, rounds, partial=False):
     cells = lat.layers * lat.height * lat.width
     history = np.zeros(cells, np.uint64)
     cost = np.zeros(cells, np.uint32)
     per_round = []
+    costs = paths = usage = None
     for r in range(rounds):
-        costs, paths = oracle.dijkstra_batch(lat, nets, cell_cost=cost)
+        if partial and r > 0:
+            # reroute only nets that did not reach or cross an overused cell
+            dirty = [c == oracle.lo_inf() or bool((usage[p.astype(np.int64)] > pol.capacity).any())
+                     for c, p in zip(costs, paths)]
+            idx = np.flatnonzero(dirty)
+            new_costs, new_paths = (oracle.dijkstra_batch(lat, nets[idx], cell_cost=cost)
+                                    if len(idx) else (np.zeros(0, np.uint32), []))
+            costs = costs.copy()
+            paths = list(paths)
+            for k, i in enumerate(idx):
+                costs[i] = new_costs[k]
+                paths[i] = new_paths[k]
+        else:
+            costs, paths = oracle.dijkstra_batch(lat, nets, cell_cost=cost)
         usage = np.zeros(cells, np.uint64)
         for c, p in zip(costs, paths):
             if c != oracle.lo_inf():
@@ -41,20 +55,22 @@ def _cpu_rounds(lat, nets, pol, rounds):
     return usage.astype(np.uint32), history, cost, costs, paths, per_round
 
 
+@pytest.mark.parametrize("partial", [False, True])
 @pytest.mark.parametrize("use_graph", [False, True])
-def test_rounds_match_cpu_restatement(use_graph):
+def test_rounds_match_cpu_restatement(use_graph, partial):
     lat = synth.make_lattice(61, 2, 128, 0.15, via_mask=True)
     nets = synth.make_nets(lat, 62, 48, hpwl_median=50.0, hpwl_sigma=0.5, margin=12)
     pol = prices.policy(initial=20, increment=20, history_increment=5, capacity=1)
     rounds = 4
-    usage_c, history_c, cost_c, costs_c, paths_c, per_round_c = _cpu_rounds(lat, nets, pol, rounds)
+    usage_c, history_c, cost_c, costs_c, paths_c, per_round_c = _cpu_rounds(lat, nets, pol, rounds,
+                                                                            partial)
     assert per_round_c[0][0] > 0  # the batch is congested in the first round
     dev = apgar_b200.DeviceLattice(lat)
     try:
         plan = dev.plan(nets, generator="frontier")
         neg = negotiate.Negotiation(plan, pol)
         for _ in range(2 if use_graph else 1):  # the second graph run is a replay
-            neg.run(rounds, use_graph=use_graph)
+            neg.run(rounds, use_graph=use_graph, partial=partial)
             usage, history, cost, rows = neg.readback()
             res, paths = plan.readback()
             assert np.array_equal(usage, usage_c)
