@@ -100,6 +100,13 @@ struct FrontierLaunch {
   const uint8_t* skip;
   const apgar_b200_lattice_result* prev_results;
   const uint32_t* prev_paths;
+  // optional rip-up pricing (needs cell_cost, prev_results and prev_paths):
+  // a move into a cell of the net's own previous path costs cell_cost_own
+  // instead of cell_cost.  own_bits is one bit per label word, laid out like
+  // `words` (bit i of word k / 32 belongs to label word k); a net clears and
+  // fills its slab's bits before its search.
+  const uint32_t* cell_cost_own;
+  uint32_t* own_bits;
 };
 
 __device__ __forceinline__ uint32_t sat(uint32_t v) { return v < kLabelInf ? v : kLabelInf; }

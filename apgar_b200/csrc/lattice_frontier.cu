@@ -146,7 +146,8 @@ template <bool kPriced>
 __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const Window& win,
                                             uint32_t e, unsigned long long* words, uint32_t thr,
                                             uint32_t cur_low, uint32_t far_low,
-                                            const uint32_t* cell_cost, uint32_t (&ne)[10],
+                                            const uint32_t* cell_cost, const uint32_t* cost_own,
+                                            const uint32_t* own, uint32_t (&ne)[10],
                                             uint32_t& cur_mask, uint32_t& far_mask, bool& overflow) {
   const int l = static_cast<int>(e >> 28), y = static_cast<int>((e >> 14) & 0x3FFFu),
             x = static_cast<int>(e & 0x3FFFu);
@@ -170,7 +171,8 @@ __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const 
     seen[d] = (inside & (1u << d)) ? static_cast<uint32_t>(__ldcg(words + ni) >> 32) : 0u;
   }
   const int X = win.x0 + x, Y = win.y0 + y;
-  // entry prices of the neighbours (0 without a price snapshot)
+  // entry prices of the neighbours (0 without a price snapshot); a cell of
+  // the net's own previous path is priced without the net's own use
   uint32_t price[10];
 #pragma unroll
   for (int d = 0; d < 10; ++d) {
@@ -178,7 +180,13 @@ __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const 
     if (kPriced && (inside & (1u << d))) {
       const int nl = d == 8 ? l - 1 : (d == 9 ? l + 1 : l);
       const int px = d < 8 ? X + fdx(d) : X, py = d < 8 ? Y + fdy(d) : Y;
-      price[d] = __ldg(cell_cost + (static_cast<size_t>(nl) * lat.height + py) * lat.width + px);
+      const uint32_t* src = cell_cost;
+      if (own != nullptr) {
+        const uint32_t ni = d < 8 ? here + static_cast<uint32_t>(fdy(d)) * w + static_cast<uint32_t>(fdx(d))
+                                  : (d == 8 ? here - plane : here + plane);
+        if ((__ldcg(own + (ni >> 5)) >> (ni & 31u)) & 1u) src = cost_own;
+      }
+      price[d] = __ldg(src + (static_cast<size_t>(nl) * lat.height + py) * lat.width + px);
     }
   }
   const size_t stride = static_cast<size_t>(lat.words) + 2;
@@ -348,6 +356,11 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
     // lists sit that far apart (inside a slot the cap binds above it)
     const uint32_t span = p.per_net ? cells : (cells < cap ? cells : cap);
     unsigned long long* words = p.per_net ? p.words + plan.dist_offset : slot_words;
+    // own-path bits of this slab (rip-up pricing from the second round on)
+    uint32_t* const own =
+        (kPriced && p.cell_cost_own != nullptr)
+            ? p.own_bits + (p.per_net ? plan.dist_offset : static_cast<uint64_t>(slot) * p.slab_cells) / 32u
+            : nullptr;
     uint32_t* list_a = p.per_net ? p.lists + 3ull * plan.dist_offset : slot_lists;
     uint32_t* list_b = list_a + span;
     uint32_t* list_c = list_b + span;
@@ -357,11 +370,32 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
       uint4* w4 = reinterpret_cast<uint4*>(words);
       const uint4 inf2 = make_uint4(0xFFFFFFFFu, kLabelInf, 0xFFFFFFFFu, kLabelInf);
       for (uint32_t i = tid; i < padded / 2; i += T) w4[i] = inf2;
+      if (own != nullptr) {
+        for (uint32_t i = tid; i < padded / 32u; i += T) own[i] = 0u;
+      }
     }
     const bool endpoints_free = cell_free_w(lat, win, sl, sx, sy) &&
                                 cell_free_w(lat, win, win.gl, win.gx, win.gy);
     // every clearing store of the group lands before the start is seeded
     fsync<G>(barrier_id);
+    if (own != nullptr) {
+      // mark the cells of the net's previous route (packed reverse path of
+      // global cell ids); cells outside the window cannot be entered anyway
+      const apgar_b200_lattice_result prev = p.prev_results[plan.net];
+      if (prev.completion == APGAR_B200_COMPLETION_REACHED) {
+        const uint32_t lw = static_cast<uint32_t>(lat.width), lh = static_cast<uint32_t>(lat.height);
+        for (uint32_t j = tid; j < prev.path_len; j += T) {
+          const uint32_t c = p.prev_paths[prev.path_offset + j];
+          const int cx = static_cast<int>(c % lw) - win.x0;
+          const int cy = static_cast<int>((c / lw) % lh) - win.y0;
+          const uint32_t cl = c / lw / lh;
+          if (cl < static_cast<uint32_t>(lat.layers) && cx >= 0 && cx < win.w && cy >= 0 && cy < win.h) {
+            const uint32_t i = cell_index(win, static_cast<int>(cl), cx, cy);
+            atomicOr(own + (i >> 5), 1u << (i & 31u));
+          }
+        }
+      }
+    }
     if (tid == 0) {
       sh.count[0] = sh.count[1] = sh.count[2] = 0;
       sh.far_count = 0;
@@ -434,7 +468,8 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
           if (valid) {
             ++expanded;
             bool overflow = false;
-            expand_cell<kPriced>(lat, win, cur[i], words, thr, cur_low, far_low, p.cell_cost, ne,
+            expand_cell<kPriced>(lat, win, cur[i], words, thr, cur_low, far_low, p.cell_cost,
+                                 p.cell_cost_own, own, ne,
                                  cur_mask, far_mask, overflow);
             if (overflow) sh.overflow = 1u;
           }
@@ -536,11 +571,14 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
                 break;
               }
               // the move into the current cell paid its entry price
-              const uint32_t here_price =
-                  !kPriced
-                      ? 0u
-                      : __ldg(p.cell_cost + (static_cast<size_t>(cl) * lat.height + (win.y0 + cy)) *
-                                                lat.width + (win.x0 + cx));
+              uint32_t here_price = 0u;
+              if (kPriced) {
+                const uint32_t hi = cell_index(win, cl, cx, cy);
+                const bool mine = own != nullptr && ((__ldcg(own + (hi >> 5)) >> (hi & 31u)) & 1u);
+                here_price = __ldg((mine ? p.cell_cost_own : p.cell_cost) +
+                                   (static_cast<size_t>(cl) * lat.height + (win.y0 + cy)) *
+                                       lat.width + (win.x0 + cx));
+              }
               // lanes 0..7: planar predecessors by incoming heading; 8, 9: vias
               bool cand = false;
               int pl = cl, px = cx, py = cy;

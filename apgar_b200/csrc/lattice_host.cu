@@ -33,7 +33,8 @@ cudaError_t launch_price_update(uint32_t count, const uint32_t* usage, uint64_t 
                                 uint64_t next_factor, uint64_t hist_inc, uint64_t capacity,
                                 uint64_t max_value, uint64_t* present, uint64_t* history,
                                 uint64_t* total, uint64_t* next_cost, uint32_t* next_cost32,
-                                uint32_t* status, unsigned long long* stats, cudaStream_t stream);
+                                uint32_t* next_cost_own32, uint32_t* status,
+                                unsigned long long* stats, cudaStream_t stream);
 cudaError_t launch_mark_dirty(const apgar_b200_lattice_result* results, uint32_t count,
                               const uint32_t* paths, const uint32_t* usage, uint64_t cell_count,
                               uint32_t capacity, uint8_t* skip, int sm_count, cudaStream_t stream);
@@ -85,6 +86,10 @@ struct PlanObject {
   const uint8_t* skip = nullptr;
   const apgar_b200_lattice_result* prev_results = nullptr;
   const uint32_t* prev_paths = nullptr;
+  // rip-up pricing (set by a negotiation): prices of a net's own previous
+  // cells, and one bit per label word to mark them
+  const uint32_t* cell_cost_own = nullptr;
+  uint32_t* own_bits = nullptr;
   uint32_t* cancel_host = nullptr;  // pinned, mapped; polled by the kernels
   uint32_t* cancel_dev = nullptr;
   std::vector<ClassRange> classes;
@@ -415,6 +420,7 @@ int execute_plan(PlanObject* plan, cudaStream_t stream) {
   fbase.skip = plan->skip;
   fbase.prev_results = plan->prev_results;
   fbase.prev_paths = plan->prev_paths;
+  fbase.cell_cost_own = plan->cell_cost_own;
   SweepLaunch base{};
   base.lat = v;
   base.nets = plan->nets.get();
@@ -447,9 +453,11 @@ int execute_plan(PlanObject* plan, cudaStream_t stream) {
       fl.list_cap = c.list_cap;
       fl.slots = c.slots;
       fl.per_net = plan->per_net ? 1u : 0u;
+      fl.own_bits = plan->own_bits == nullptr ? nullptr : plan->own_bits + c.words_offset / 32u;
       if (plan->per_net) {
         fl.words = plan->words.get();
         fl.lists = plan->lists.get();
+        fl.own_bits = plan->own_bits;
       }
       fl.next_plan = reinterpret_cast<unsigned int*>(plan->counters.get() + 2 + k);
       APGAR_B200_CUDA("lattice frontier launch",
@@ -1049,14 +1057,19 @@ extern "C" int apgar_b200_lattice_route_noalloc(void* lattice, const apgar_b200_
 // Round p (Jacobi rip-up and reroute: every net is rerouted against the same
 // frozen snapshot):
 //   1. search every net of the plan with per-cell entry prices `cell_cost`;
+//      from the second round on, a cell of the net's own previous route is
+//      priced from the usage of the other nets only (`cell_cost_own`), as
+//      the reference rips a net's incumbent route up before pricing its
+//      query (cpu_sequential_negotiated_routing.cc:1023-1034);
 //   2. usage = number of reached paths through each cell (integer atomics, so
 //      order independent);
 //   3. one fused price pass at epoch p (src/allocator/negotiated_regeneration_plan.cc
 //      :430-442 factor schedule; cpu_sequential_negotiated_routing.cc:1300-1330
 //      history update): history += increment * overuse, and the next snapshot
 //      cell_cost = history + factor(p + 1) * max(0, usage + 1 - capacity)
-//      (cpu_sequential_negotiated_routing.cc:299-505), saturated to 2^31 - 1;
-//      the same pass counts overused cells and total overuse for the round.
+//      (cpu_sequential_negotiated_routing.cc:299-505), saturated to 2^31 - 1,
+//      and cell_cost_own = the same with usage - 1 in place of usage; the
+//      same pass counts overused cells and total overuse for the round.
 // The reference's sequential negotiated router reroutes nets one at a time
 // (Gauss-Seidel); batched rounds are Jacobi by design, so only each round's
 // per-net results under its frozen snapshot are comparable with a CPU run.
@@ -1070,6 +1083,8 @@ struct NegotiationObject {
   apgar_b200_price_policy policy{};
   uint64_t cells = 0;
   DeviceBuffer<uint32_t> usage, cell_cost, status;
+  DeviceBuffer<uint32_t> cell_cost_own;  // the snapshot seen from a net's own previous cells
+  DeviceBuffer<uint32_t> own_bits;       // one bit per label word of the plan
   DeviceBuffer<uint64_t> history;
   DeviceBuffer<unsigned long long> stats;  // [round][overused cells, total overuse]
   uint32_t rounds_capacity = 0;
@@ -1095,6 +1110,8 @@ struct NegotiationObject {
       plan->skip = nullptr;
       plan->prev_results = nullptr;
       plan->prev_paths = nullptr;
+      plan->cell_cost_own = nullptr;
+      plan->own_bits = nullptr;
     }
   }
 };
@@ -1124,6 +1141,11 @@ int enqueue_negotiation(NegotiationObject* n, uint32_t rounds, bool partial) {
       return set_error(APGAR_B200_INTERNAL_INVARIANT, "present-price schedule overflowed uint64");
     }
     PlanObject* plan = n->plan;
+    // from round 1 on the previous round's routes drive rip-up pricing
+    plan->prev_results = r > 0 ? n->prev_results.get() : nullptr;
+    plan->prev_paths = r > 0 ? n->prev_paths.get() : nullptr;
+    plan->cell_cost_own = r > 0 ? n->cell_cost_own.get() : nullptr;
+    plan->own_bits = r > 0 ? n->own_bits.get() : nullptr;
     if (partial && r > 0) {
       APGAR_B200_CUDA("mark dirty launch",
                       launch_mark_dirty(n->prev_results.get(), plan->count, n->prev_paths.get(),
@@ -1131,15 +1153,17 @@ int enqueue_negotiation(NegotiationObject* n, uint32_t rounds, bool partial) {
                                         static_cast<uint32_t>(n->policy.capacity), n->skip.get(),
                                         plan->sm_count, s));
       plan->skip = n->skip.get();
-      plan->prev_results = n->prev_results.get();
-      plan->prev_paths = n->prev_paths.get();
     } else {
       plan->skip = nullptr;
     }
     const int exec_rc = execute_plan(plan, s);
     plan->skip = nullptr;
+    plan->prev_results = nullptr;
+    plan->prev_paths = nullptr;
+    plan->cell_cost_own = nullptr;
+    plan->own_bits = nullptr;
     if (exec_rc != APGAR_B200_OK) return exec_rc;
-    if (partial && r + 1 < rounds) {
+    if (r + 1 < rounds) {
       APGAR_B200_CUDA("cudaMemcpyAsync(previous results)",
                       cudaMemcpyAsync(n->prev_results.get(), plan->results.get(),
                                       plan->count * sizeof(apgar_b200_lattice_result),
@@ -1160,7 +1184,8 @@ int enqueue_negotiation(NegotiationObject* n, uint32_t rounds, bool partial) {
                                         next_factor, n->policy.historical_price_increment,
                                         n->policy.capacity, n->policy.maximum_value, nullptr,
                                         n->history.get(), nullptr, nullptr, n->cell_cost.get(),
-                                        n->status.get() + r, n->stats.get() + 2ull * r, s));
+                                        n->cell_cost_own.get(), n->status.get() + r,
+                                        n->stats.get() + 2ull * r, s));
   }
   return APGAR_B200_OK;
 }
@@ -1190,6 +1215,8 @@ extern "C" int apgar_b200_negotiation_create(void* plan, const apgar_b200_price_
     n->cells = cells;
     APGAR_B200_CUDA("cudaMalloc(usage)", n->usage.ensure(cells));
     APGAR_B200_CUDA("cudaMalloc(cell costs)", n->cell_cost.ensure(cells));
+    APGAR_B200_CUDA("cudaMalloc(own-route cell costs)", n->cell_cost_own.ensure(cells));
+    APGAR_B200_CUDA("cudaMalloc(own-route bits)", n->own_bits.ensure(p->words.count() / 32 + 1));
     APGAR_B200_CUDA("cudaMalloc(history)", n->history.ensure(cells));
     APGAR_B200_CUDA("cudaMalloc(previous results)", n->prev_results.ensure(std::max<uint32_t>(p->count, 1)));
     APGAR_B200_CUDA("cudaMalloc(previous paths)", n->prev_paths.ensure(std::max<uint64_t>(p->arena_capacity, 1)));

@@ -10,7 +10,8 @@ cudaError_t launch_price_update(uint32_t count, const uint32_t* usage, uint64_t 
                                 uint64_t next_factor, uint64_t hist_inc, uint64_t capacity,
                                 uint64_t max_value, uint64_t* present, uint64_t* history,
                                 uint64_t* total, uint64_t* next_cost, uint32_t* next_cost32,
-                                uint32_t* status, unsigned long long* stats, cudaStream_t stream);
+                                uint32_t* next_cost_own32, uint32_t* status,
+                                unsigned long long* stats, cudaStream_t stream);
 namespace {
 
 // factor = initial + epoch * increment with checked arithmetic
@@ -45,7 +46,8 @@ extern "C" int apgar_b200_price_update_device(uint32_t count, const uint32_t* us
                   launch_price_update(count, usage, factor, next_factor,
                                       policy->historical_price_increment, policy->capacity,
                                       policy->maximum_value, present, history, total, next_cost,
-                                      nullptr, status, nullptr, static_cast<cudaStream_t>(stream)));
+                                      nullptr, nullptr, status, nullptr,
+                                      static_cast<cudaStream_t>(stream)));
   clear_error();
   return APGAR_B200_OK;
 }

@@ -40,7 +40,8 @@ __global__ void price_update_kernel(uint32_t count, const uint32_t* __restrict__
                                     PriceParams pp, uint64_t* __restrict__ present,
                                     uint64_t* __restrict__ history, uint64_t* __restrict__ total,
                                     uint64_t* __restrict__ next_cost,
-                                    uint32_t* __restrict__ next_cost32, uint32_t* status,
+                                    uint32_t* __restrict__ next_cost32,
+                                    uint32_t* __restrict__ next_cost_own32, uint32_t* status,
                                     unsigned long long* stats) {
   uint32_t flags = 0;
   unsigned long long overused = 0, overuse_sum = 0;
@@ -84,6 +85,16 @@ __global__ void price_update_kernel(uint32_t count, const uint32_t* __restrict__
       // the search reads a 32-bit entry price; a larger cost saturates to the
       // label sentinel, so any path through the cell is rejected, never wrong
       if (next_cost32 != nullptr) next_cost32[i] = c < 0x7FFFFFFFull ? static_cast<uint32_t>(c) : 0x7FFFFFFFu;
+      if (next_cost_own32 != nullptr) {
+        // the same snapshot for a net whose own previous path holds one of
+        // the u units: the reference rips that net up before pricing, so it
+        // sees u - 1 other uses (u - 1 + 1 - capacity).  c_own <= c, so no
+        // new overflow or bound can arise here.
+        const uint64_t oover = u > pp.capacity ? u - pp.capacity : 0;
+        uint64_t co, opc;
+        if (!mul_checked(pp.next_factor, oover, &opc) || !add_checked(h, opc, &co)) co = ~0ull;
+        next_cost_own32[i] = co < 0x7FFFFFFFull ? static_cast<uint32_t>(co) : 0x7FFFFFFFu;
+      }
     }
   }
   flags = __reduce_or_sync(0xFFFFFFFFu, flags);
@@ -151,7 +162,8 @@ cudaError_t launch_price_update(uint32_t count, const uint32_t* usage, uint64_t 
                                 uint64_t next_factor, uint64_t hist_inc, uint64_t capacity,
                                 uint64_t max_value, uint64_t* present, uint64_t* history,
                                 uint64_t* total, uint64_t* next_cost, uint32_t* next_cost32,
-                                uint32_t* status, unsigned long long* stats, cudaStream_t stream) {
+                                uint32_t* next_cost_own32, uint32_t* status,
+                                unsigned long long* stats, cudaStream_t stream) {
   cudaError_t e = cudaMemsetAsync(status, 0, sizeof(uint32_t), stream);
   if (e == cudaSuccess && stats != nullptr) {
     e = cudaMemsetAsync(stats, 0, 2 * sizeof(unsigned long long), stream);
@@ -160,7 +172,8 @@ cudaError_t launch_price_update(uint32_t count, const uint32_t* usage, uint64_t 
   PriceParams pp{factor, next_factor, hist_inc, capacity, max_value};
   const uint32_t blocks = (count + 255u) / 256u;
   price_update_kernel<<<blocks < 148u * 16u ? blocks : 148u * 16u, 256, 0, stream>>>(
-      count, usage, pp, present, history, total, next_cost, next_cost32, status, stats);
+      count, usage, pp, present, history, total, next_cost, next_cost32, next_cost_own32, status,
+      stats);
   return cudaGetLastError();
 }
 

@@ -1,9 +1,11 @@
 """Negotiated-congestion rounds (rip-up and reroute) on a frontier plan.
 
 Host mirror of the apgar_b200_negotiation_* C ABI: every round reroutes all
-nets of the plan against frozen per-cell snapshot prices, counts per-cell
-usage, and runs the fused price pass (history and the next snapshot).  The
-whole run can be captured once as a CUDA graph and replayed.
+nets of the plan (or, with partial rip-up, only those crossing overused
+cells) against frozen per-cell snapshot prices, with each net's own previous
+cells priced from the other nets' usage; then it counts per-cell usage and
+runs the fused price pass (history and the next snapshot).  The whole run can
+be captured once as a CUDA graph and replayed.
 """
 
 from __future__ import annotations

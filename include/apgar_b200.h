@@ -497,10 +497,13 @@ APGAR_B200_API int apgar_b200_lattice_accumulate_usage(void* plan, uint32_t* usa
  * net of the plan against the frozen snapshot prices, counts per-cell usage
  * of the reached paths, and runs the fused price pass at epoch r: history
  * += increment * overuse; next snapshot = history + factor(r + 1) *
- * max(0, usage + 1 - capacity).  Rounds are Jacobi (all nets against one
- * snapshot), while the reference's loop is Gauss-Seidel (net by net), so the
- * two give different routings by design; every round is exact for its
- * snapshot. */
+ * max(0, usage + 1 - capacity).  From round 1 on, a net pays for the cells
+ * of its own previous route the snapshot of the other nets' usage (usage - 1
+ * in place of usage), as the reference rips the incumbent route up before
+ * pricing a query (cpu_sequential_negotiated_routing.cc:1023-1034).  Rounds
+ * are Jacobi (all nets against one snapshot), while the reference's loop is
+ * Gauss-Seidel (net by net), so the two give different routings by design;
+ * every round is exact for its snapshot. */
 typedef struct apgar_b200_negotiation_round {
   uint64_t overused_cells; /* cells with usage > capacity after the round */
   uint64_t total_overuse;  /* sum of max(0, usage - capacity) */

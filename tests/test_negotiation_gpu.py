@@ -1,8 +1,10 @@
 """GPU negotiated-congestion rounds against a CPU restatement of the same
 Jacobi rip-up-and-reroute loop: per round, the priced oracle search of every
-net under the frozen snapshot, per-cell usage of the reached paths, the
-allocator epoch history update and the CS-RR next-pass snapshot (price
-oracle).  Bit-exact usage, history, snapshot prices, per-round overuse and the
+net under the frozen snapshot, with the cells of the net's own previous route
+priced from the other nets' usage (the reference removes a net's incumbent
+uses before pricing its query, cpu_sequential_negotiated_routing.cc:1023-1034),
+per-cell usage of the reached paths, the allocator epoch history update and
+the CS-RR next-pass snapshot (price oracle).  Bit-exact usage, history, snapshot prices, per-round overuse and the
 last round's costs and canonical paths; the CUDA-graph form replays to the
 same result."""
 
@@ -16,27 +18,42 @@ from apgar_b200 import negotiate, prices, synth
 pytestmark = pytest.mark.gpu
 
 
+def _snapshot32(usage, history, pol, epoch):
+    rc, snap = oracle.price_snapshot(usage, history, pol.capacity, epoch,
+                                     pol.initial_present_factor, pol.present_factor_increment,
+                                     pol.maximum_value)
+    assert rc == 0
+    return np.minimum(snap, 0x7FFFFFFF).astype(np.uint32)
+
+
 def _cpu_rounds(lat, nets, pol, rounds, partial=False):
     cells = lat.layers * lat.height * lat.width
     history = np.zeros(cells, np.uint64)
     cost = np.zeros(cells, np.uint32)
+    cost_own = cost
     per_round = []
     costs = paths = usage = None
     for r in range(rounds):
-        if partial and r > 0:
-            # reroute only nets that did not reach or cross an overused cell
-            dirty = [c == oracle.lo_inf() or bool((usage[p.astype(np.int64)] > pol.capacity).any())
-                     for c, p in zip(costs, paths)]
-            idx = np.flatnonzero(dirty)
-            new_costs, new_paths = (oracle.dijkstra_batch(lat, nets[idx], cell_cost=cost)
-                                    if len(idx) else (np.zeros(0, np.uint32), []))
+        if r == 0:
+            costs, paths = oracle.dijkstra_batch(lat, nets, cell_cost=cost)
+        else:
+            if partial:
+                # reroute only nets that did not reach or cross an overused cell
+                idx = [i for i, (c, p) in enumerate(zip(costs, paths))
+                       if c == oracle.lo_inf() or (usage[p.astype(np.int64)] > pol.capacity).any()]
+            else:
+                idx = range(len(nets))
             costs = costs.copy()
             paths = list(paths)
-            for k, i in enumerate(idx):
-                costs[i] = new_costs[k]
-                paths[i] = new_paths[k]
-        else:
-            costs, paths = oracle.dijkstra_batch(lat, nets, cell_cost=cost)
+            for i in idx:
+                # the net's own previous cells are priced without its own use
+                mine = cost.copy()
+                if costs[i] != oracle.lo_inf():
+                    own = paths[i].astype(np.int64)
+                    mine[own] = cost_own[own]
+                c, p = oracle.dijkstra_batch(lat, nets[i:i + 1], cell_cost=mine)
+                costs[i] = c[0]
+                paths[i] = p[0]
         usage = np.zeros(cells, np.uint64)
         for c, p in zip(costs, paths):
             if c != oracle.lo_inf():
@@ -45,11 +62,9 @@ def _cpu_rounds(lat, nets, pol, rounds, partial=False):
             usage, history, pol.capacity, r, pol.initial_present_factor,
             pol.present_factor_increment, pol.historical_price_increment)
         assert rc == 0
-        rc, snap = oracle.price_snapshot(usage, history, pol.capacity, r + 1,
-                                         pol.initial_present_factor, pol.present_factor_increment,
-                                         pol.maximum_value)
-        assert rc == 0
-        cost = np.minimum(snap, 0x7FFFFFFF).astype(np.uint32)
+        cost = _snapshot32(usage, history, pol, r + 1)
+        cost_own = _snapshot32(np.where(usage > 0, usage - 1, 0).astype(np.uint64), history, pol,
+                               r + 1)
         over = np.where(usage > pol.capacity, usage - pol.capacity, 0)
         per_round.append((int((over > 0).sum()), int(over.sum())))
     return usage.astype(np.uint32), history, cost, costs, paths, per_round
