@@ -268,6 +268,26 @@ class Plan:
         ptr = None if costs is None else ctypes.c_void_p(costs.data_ptr())
         _check(lib().apgar_b200_lattice_plan_set_cell_costs(self.handle, ptr))
 
+    def set_corridors(self, bits) -> None:
+        """Corridor mode for later executes: a CUDA uint32 tensor [nets][128]
+        of coarse corridor bitmaps (see ``apgar_b200.corridor``; kept
+        referenced here), or None."""
+        import torch
+
+        if bits is not None and (bits.dtype != torch.uint32 or bits.numel() != 128 * len(self.nets)
+                                 or not bits.is_cuda or not bits.is_contiguous()):
+            raise ValueError("corridors are a contiguous CUDA uint32 tensor of 128 words per net")
+        self._corridors = bits
+        ptr = None if bits is None else ctypes.c_void_p(bits.data_ptr())
+        _check(lib().apgar_b200_lattice_plan_set_corridors(self.handle, ptr))
+
+    def corridor_status(self) -> np.ndarray:
+        """Per-net corridor outcomes of the last corridor-mode execute
+        (``apgar_b200.corridor`` CERTIFIED / FALLBACK_*)."""
+        out = np.empty(len(self.nets), dtype=np.uint8)
+        _check(lib().apgar_b200_lattice_plan_corridor_status(self.handle, _vp(out)))
+        return out
+
     def execute(self, stream: int = 0) -> None:
         _check(lib().apgar_b200_lattice_execute(self.handle, ctypes.c_void_p(stream)))
 

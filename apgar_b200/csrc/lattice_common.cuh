@@ -107,6 +107,15 @@ struct FrontierLaunch {
   // fills its slab's bits before its search.
   const uint32_t* cell_cost_own;
   uint32_t* own_bits;
+  // optional corridor mode: net n's corridor is the 64 x 64 coarse bitmap at
+  // corridor + 128 * n (bit cx of word 2 * cy + cx / 32; a coarse cell covers
+  // 2^s x 2^s window cells on every layer, s the least value >= 2 that keeps
+  // the window within 64 coarse cells per side); corridor_status[n] receives
+  // the net's APGAR_B200_CORRIDOR_* outcome
+  const uint32_t* corridor;
+  uint8_t* corridor_status;
+  // optional: the class's plan count, read on the device (overrides plan_count)
+  const uint32_t* plan_count_dev;
 };
 
 __device__ __forceinline__ uint32_t sat(uint32_t v) { return v < kLabelInf ? v : kLabelInf; }

@@ -46,6 +46,29 @@
 // would outgrow it is reported REJECTED (never a truncated search).
 // Queue entries are packed cells (layer << 28 | y << 14 | x, window-local).
 // Appends take one packed warp scan and one shared atomic per warp and list.
+//
+// Corridor mode (kCorr): a net first searches only the cells of its corridor,
+// a bitmap of coarse cells (2^s x 2^s lattice cells, all layers) over its
+// window.  Every legal move from a corridor cell u into a window cell v
+// outside the corridor is an exit; the search keeps the least key g(u) +
+// cost(u, v) + h(v) over all exits it expands.  The corridor result is
+// accepted (certified) only when its goal label C is strictly below that
+// least exit key:
+//  - any start-goal path that leaves the corridor first leaves it by some
+//    exit (u, v) with its prefix inside the corridor, so it costs at least
+//    that exit's key with the exact corridor distance of u;
+//  - every exit whose exact key is at most C is expanded with its exact
+//    label before the search stops (the same argument as for the labels
+//    above, on the corridor subgraph), and the least key over stale labels
+//    is never below the exact one;
+//  - so with C below the least key no optimal full-window path leaves the
+//    corridor: C is the full-window optimum, every cell on an optimal path
+//    has its exact label, and no outside cell passes the walk's equality
+//    test, so the canonical path is the full-window one as well.
+// Otherwise (goal not reached in the corridor, a terminal outside it, or an
+// exit key at or below C) the same group clears the whole window and searches
+// it without the corridor.  Cells outside the corridor are never read or
+// written in the corridor pass, so only the corridor's blocks are cleared.
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -120,6 +143,13 @@ __device__ __forceinline__ uint32_t label_of(const unsigned long long* w) {
   return static_cast<uint32_t>(__ldcg(w) >> 32);
 }
 
+// Corridor membership of window cell (x, y): bit x >> s of row y >> s of the
+// net's 64 x 64 coarse bitmap (two words per coarse row).
+__device__ __forceinline__ bool corr_has(const uint32_t* corr, int cshift, int x, int y) {
+  const uint32_t cx = static_cast<uint32_t>(x) >> cshift, cy = static_cast<uint32_t>(y) >> cshift;
+  return ((corr[cy * 2u + (cx >> 5)] >> (cx & 31u)) & 1u) != 0u;
+}
+
 template <int G>
 __device__ __forceinline__ void fsync(int barrier_id) {
   if constexpr (G == 1) {
@@ -142,12 +172,13 @@ __device__ __forceinline__ uint32_t blocked3(const uint32_t* row, int X) {
 // together, then the 64-bit atomicMins.  Lowered neighbours whose list stamp
 // this call set are flagged in cur_mask (next round's list) or far_mask (far
 // list); ne[d] holds the packed cell.
-template <bool kPriced>
+template <bool kPriced, bool kCorr>
 __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const Window& win,
                                             uint32_t e, unsigned long long* words, uint32_t thr,
                                             uint32_t cur_low, uint32_t far_low,
                                             const uint32_t* cell_cost, const uint32_t* cost_own,
-                                            const uint32_t* own, uint32_t (&ne)[10],
+                                            const uint32_t* own, const uint32_t* corr, int cshift,
+                                            uint32_t& exit_min, uint32_t (&ne)[10],
                                             uint32_t& cur_mask, uint32_t& far_mask, bool& overflow) {
   const int l = static_cast<int>(e >> 28), y = static_cast<int>((e >> 14) & 0x3FFFu),
             x = static_cast<int>(e & 0x3FFFu);
@@ -161,6 +192,17 @@ __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const 
                           ((xl && yu) ? 8u : 0u) | (xl ? 16u : 0u) | ((xl && yd) ? 32u : 0u) |
                           (yd ? 64u : 0u) | ((xr && yd) ? 128u : 0u) | (ld ? 256u : 0u) |
                           (lu ? 512u : 0u);
+  // neighbours inside the corridor (a via keeps the cell's column); only
+  // these are read, lowered or priced
+  uint32_t corr_in = 0x3FFu;
+  if constexpr (kCorr) {
+    corr_in = 0x300u;
+#pragma unroll
+    for (int d = 0; d < 8; ++d) {
+      if ((inside & (1u << d)) && corr_has(corr, cshift, x + fdx(d), y + fdy(d))) corr_in |= 1u << d;
+    }
+  }
+  const uint32_t reach = inside & corr_in;
   // wave 1: own label, neighbour labels, mask bits
   const uint32_t gv = static_cast<uint32_t>(__ldcg(words + here) >> 32);
   uint32_t seen[10];
@@ -168,7 +210,7 @@ __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const 
   for (int d = 0; d < 10; ++d) {
     const uint32_t ni = d < 8 ? here + static_cast<uint32_t>(fdy(d)) * w + static_cast<uint32_t>(fdx(d))
                               : (d == 8 ? here - plane : here + plane);
-    seen[d] = (inside & (1u << d)) ? static_cast<uint32_t>(__ldcg(words + ni) >> 32) : 0u;
+    seen[d] = (reach & (1u << d)) ? static_cast<uint32_t>(__ldcg(words + ni) >> 32) : 0u;
   }
   const int X = win.x0 + x, Y = win.y0 + y;
   // entry prices of the neighbours (0 without a price snapshot); a cell of
@@ -177,7 +219,7 @@ __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const 
 #pragma unroll
   for (int d = 0; d < 10; ++d) {
     price[d] = 0u;
-    if (kPriced && (inside & (1u << d))) {
+    if (kPriced && (reach & (1u << d))) {
       const int nl = d == 8 ? l - 1 : (d == 9 ? l + 1 : l);
       const int px = d < 8 ? X + fdx(d) : X, py = d < 8 ? Y + fdy(d) : Y;
       const uint32_t* src = cell_cost;
@@ -236,13 +278,21 @@ __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const 
       overflow = true;
       continue;
     }
-    if ((legal & (1u << d)) && cand[d] < seen[d]) {
-      const int dx = d < 8 ? fdx(d) : 0, dy = d < 8 ? fdy(d) : 0;
-      const int nl = d == 8 ? l - 1 : (d == 9 ? l + 1 : l);
-      const uint32_t a = static_cast<uint32_t>(ax[1 + dx]), b = static_cast<uint32_t>(ay[1 + dy]);
+    // key of the neighbour reached by move d at label cand[d]
+    const auto key_of = [&](int m) {
+      const int mx = m < 8 ? fdx(m) : 0, my = m < 8 ? fdy(m) : 0;
+      const int nl = m == 8 ? l - 1 : (m == 9 ? l + 1 : l);
+      const uint32_t a = static_cast<uint32_t>(ax[1 + mx]), b = static_cast<uint32_t>(ay[1 + my]);
       const uint32_t lo = min(a, b), hi = max(a, b);
       const uint32_t planar = lat.diag >= lat.orth ? lo * dstep + (hi - lo) * lat.orth : hi * dstep;
-      const uint32_t key = cand[d] + planar + static_cast<uint32_t>(abs(nl - win.gl)) * lat.via;
+      return cand[m] + planar + static_cast<uint32_t>(abs(nl - win.gl)) * lat.via;
+    };
+    if constexpr (kCorr) {
+      if (legal & ~corr_in & (1u << d)) exit_min = min(exit_min, key_of(d));  // a corridor exit
+    }
+    if ((legal & (1u << d)) && cand[d] < seen[d]) {
+      const int dx = d < 8 ? fdx(d) : 0, dy = d < 8 ? fdy(d) : 0;
+      const uint32_t key = key_of(d);
       low[d] = key < thr ? cur_low : far_low;
       const uint32_t ni = d < 8 ? here + static_cast<uint32_t>(dy) * w + static_cast<uint32_t>(dx)
                                 : (d == 8 ? here - plane : here + plane);
@@ -282,17 +332,21 @@ struct GroupShared {
   uint32_t plan;
   uint32_t cancel[2];
   uint32_t overflow;
+  uint32_t bound;  // corridor pass: least expanded exit key
   uint32_t sums[16];
 };
 
 // kPriced: the plan carries per-cell entry prices (p.cell_cost != nullptr);
 // the unpriced instantiation has no price loads or overflow tests at all.
-template <int G, bool kPriced>
+// kCorr: corridor mode (p.corridor != nullptr), unpriced only.
+template <int G, bool kPriced, bool kCorr>
 __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
     lattice_frontier_kernel(FrontierLaunch p) {
+  static_assert(!(kPriced && kCorr), "corridor mode is unpriced");
   constexpr int kGroups = frontier_groups_per_block(G);
   constexpr int T = G * 32;
   __shared__ GroupShared shared_groups[kGroups];
+  __shared__ uint32_t corridor_bits[kCorr ? kGroups * 128 : 1];
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int gi = warp / G;
@@ -300,6 +354,7 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
   const int tid = g * 32 + lane;
   const int barrier_id = gi + 1;
   GroupShared& sh = shared_groups[gi];
+  uint32_t* const corr = corridor_bits + (kCorr ? gi * 128 : 0);
   const LatticeDeviceView& lat = p.lat;
   const uint32_t orth = lat.orth, diag = lat.diag, via = lat.via;
   const uint32_t slot = blockIdx.x * kGroups + gi;
@@ -312,7 +367,9 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
     if (tid == 0) sh.plan = atomicAdd(p.next_plan, 1u);
     fsync<G>(barrier_id);
     const uint32_t plan_index = sh.plan;
-    if (plan_index >= p.plan_count) return;  // uniform within the group
+    if (plan_index >= (p.plan_count_dev != nullptr ? *p.plan_count_dev : p.plan_count)) {
+      return;  // uniform within the group
+    }
     const NetPlan plan = p.plans[plan_index];
     if (p.skip != nullptr && p.skip[plan.net] != 0u) {  // uniform within the group
       // kept route: carry the previous result and path into this execution
@@ -365,8 +422,49 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
     uint32_t* list_b = list_a + span;
     uint32_t* list_c = list_b + span;
 
-    // clear the net's label words (16-byte stores over the padded slab)
-    {
+    // corridor: the coarse scale keeps the window within 64 x 64 coarse cells
+    int cshift = 2;
+    bool use_corr = false;
+    uint32_t cstatus = 0;  // corridor outcome of this net (APGAR_B200_CORRIDOR_*)
+    if constexpr (kCorr) {
+      const int span_max = win.w > win.h ? win.w : win.h;
+      while (((span_max - 1) >> cshift) >= 64) ++cshift;
+      const uint32_t* src = p.corridor + static_cast<size_t>(plan.net) * 128u;
+      for (int i = tid; i < 128; i += T) corr[i] = __ldg(src + i);
+      fsync<G>(barrier_id);
+      use_corr = corr_has(corr, cshift, sx, sy) && corr_has(corr, cshift, win.gx, win.gy);
+      cstatus = use_corr ? APGAR_B200_CORRIDOR_CERTIFIED : APGAR_B200_CORRIDOR_FALLBACK_UNREACHED;
+    }
+    const bool endpoints_free = cell_free_w(lat, win, sl, sx, sy) &&
+                                cell_free_w(lat, win, win.gl, win.gx, win.gy);
+    uint32_t completion = APGAR_B200_COMPLETION_DISCONNECTED;
+    uint32_t rounds = 0, levels = 0, total_rounds = 0, total_levels = 0;
+    uint32_t expanded = 0;  // this thread's expansions
+    // corridor pass first (corridor mode), then the whole window if the
+    // corridor result is not certified
+    for (;;) {
+    if (kCorr && use_corr) {
+      // only the corridor's blocks are ever touched: clear them, row by row
+      const uint32_t bs = 1u << cshift;
+      const uint32_t rows_all = static_cast<uint32_t>(lat.layers) * static_cast<uint32_t>(win.h);
+      for (uint32_t rr = tid; rr < rows_all; rr += T) {
+        const uint32_t yy = rr % static_cast<uint32_t>(win.h);
+        const uint32_t cy = yy >> cshift;
+        unsigned long long* row = words + static_cast<size_t>(rr) * static_cast<uint32_t>(win.w);
+#pragma unroll 1
+        for (int half = 0; half < 2; ++half) {
+          uint32_t bits = corr[cy * 2u + half];
+          while (bits != 0u) {
+            const uint32_t cx = static_cast<uint32_t>(half * 32 + __ffs(bits) - 1);
+            bits &= bits - 1u;
+            const uint32_t x0 = cx << cshift;
+            const uint32_t x1 = min(x0 + bs, static_cast<uint32_t>(win.w));
+            for (uint32_t x = x0; x < x1; ++x) row[x] = 0x7FFFFFFFFFFFFFFFull;
+          }
+        }
+      }
+    } else {
+      // clear the net's label words (16-byte stores over the padded slab)
       uint4* w4 = reinterpret_cast<uint4*>(words);
       const uint4 inf2 = make_uint4(0xFFFFFFFFu, kLabelInf, 0xFFFFFFFFu, kLabelInf);
       for (uint32_t i = tid; i < padded / 2; i += T) w4[i] = inf2;
@@ -374,8 +472,6 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
         for (uint32_t i = tid; i < padded / 32u; i += T) own[i] = 0u;
       }
     }
-    const bool endpoints_free = cell_free_w(lat, win, sl, sx, sy) &&
-                                cell_free_w(lat, win, win.gl, win.gx, win.gy);
     // every clearing store of the group lands before the start is seeded
     fsync<G>(barrier_id);
     if (own != nullptr) {
@@ -401,6 +497,7 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
       sh.far_count = 0;
       sh.cancel[0] = sh.cancel[1] = 0;
       sh.overflow = 0;
+      sh.bound = 0xFFFFFFFFu;
       if (endpoints_free) {
         // label 0, in the list of round 0 (stamp 1)
         words[cell_index(win, sl, sx, sy)] = 0xFFFFFFFFull - 1ull;
@@ -409,9 +506,10 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
     }
     fsync<G>(barrier_id);
 
-    uint32_t completion = APGAR_B200_COMPLETION_DISCONNECTED;
-    uint32_t rounds = 0, levels = 0;
-    uint32_t expanded = 0;  // this thread's expansions
+    completion = APGAR_B200_COMPLETION_DISCONNECTED;
+    rounds = 0;
+    levels = 0;
+    uint32_t exit_min = 0xFFFFFFFFu;  // this thread's least corridor exit key
     if (endpoints_free) {
       const uint32_t goal_index = cell_index(win, win.gl, win.gx, win.gy);
       const uint32_t delta = p.bucket_width;
@@ -468,9 +566,15 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
           if (valid) {
             ++expanded;
             bool overflow = false;
-            expand_cell<kPriced>(lat, win, cur[i], words, thr, cur_low, far_low, p.cell_cost,
-                                 p.cell_cost_own, own, ne,
-                                 cur_mask, far_mask, overflow);
+            if (kCorr && use_corr) {
+              expand_cell<kPriced, kCorr>(lat, win, cur[i], words, thr, cur_low, far_low,
+                                          p.cell_cost, p.cell_cost_own, own, corr, cshift,
+                                          exit_min, ne, cur_mask, far_mask, overflow);
+            } else {
+              expand_cell<kPriced, false>(lat, win, cur[i], words, thr, cur_low, far_low,
+                                          p.cell_cost, p.cell_cost_own, own, corr, cshift,
+                                          exit_min, ne, cur_mask, far_mask, overflow);
+            }
             if (overflow) sh.overflow = 1u;
           }
           // one packed warp scan places both lists' entries
@@ -520,6 +624,28 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
         nxt = t;
       }
     }
+    total_rounds += rounds;
+    total_levels += levels;
+    if constexpr (kCorr) {
+      if (use_corr) {
+        // the certificate: goal label strictly below every expanded exit key
+        exit_min = __reduce_min_sync(0xFFFFFFFFu, exit_min);
+        if (lane == 0 && exit_min != 0xFFFFFFFFu) atomicMin(&sh.bound, exit_min);
+        fsync<G>(barrier_id);
+        const uint32_t goal_label = label_of(words + cell_index(win, win.gl, win.gx, win.gy));
+        const bool reached = completion == APGAR_B200_COMPLETION_REACHED && goal_label < kLabelInf;
+        const bool certified = !endpoints_free || (reached && goal_label < sh.bound);
+        if (certified || completion == APGAR_B200_COMPLETION_CANCELLED) break;
+        cstatus = reached ? APGAR_B200_CORRIDOR_FALLBACK_EXIT : APGAR_B200_CORRIDOR_FALLBACK_UNREACHED;
+        use_corr = false;
+        fsync<G>(barrier_id);  // the bound and goal label are read before the next clear
+        continue;
+      }
+    }
+    break;
+    }  // corridor retry
+    rounds = total_rounds;
+    levels = total_levels;
     // expansions summed over the group (reported in the row_steps field)
     expanded = __reduce_add_sync(0xFFFFFFFFu, expanded);
     if constexpr (G > 1) {
@@ -590,6 +716,7 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
                 if (legal && (lane & 1)) {
                   legal = cell_free_w(lat, win, cl, cx, py) && cell_free_w(lat, win, cl, px, cy);
                 }
+                if (kCorr && use_corr && legal) legal = corr_has(corr, cshift, px, py);
                 if (legal) {
                   pd = label_of(words + cell_index(win, cl, px, py));
                   cand = pd < kLabelInf && pd + ((lane & 1) ? diag : orth) + here_price == here;
@@ -622,6 +749,7 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
         }
       }
       if (lane == 0) p.results[plan.net] = res;
+      if (kCorr && lane == 0) p.corridor_status[plan.net] = static_cast<uint8_t>(cstatus);
     }
     // the group's shared slots are reused by its next net
     fsync<G>(barrier_id);
@@ -634,15 +762,20 @@ cudaError_t resident_groups_g(int sm_count, uint32_t* out) {
   // resident ones start as others finish (no group waits on another) and find
   // the work-stealing queue drained
   constexpr int kGroups = frontier_groups_per_block(G);
-  int plain = 0, priced = 0;
+  int plain = 0, priced = 0, corridor = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &plain, lattice_frontier_kernel<G, false>, kGroups * G * 32, 0);
+      &plain, lattice_frontier_kernel<G, false, false>, kGroups * G * 32, 0);
   if (e == cudaSuccess) {
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &priced, lattice_frontier_kernel<G, true>, kGroups * G * 32, 0);
+        &priced, lattice_frontier_kernel<G, true, false>, kGroups * G * 32, 0);
+  }
+  if (e == cudaSuccess) {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &corridor, lattice_frontier_kernel<G, false, true>, kGroups * G * 32, 0);
   }
   if (e != cudaSuccess) return e;
-  *out = static_cast<uint32_t>(max(1, max(plain, priced)) * max(1, sm_count) * kGroups);
+  *out = static_cast<uint32_t>(max(1, max(plain, max(priced, corridor))) * max(1, sm_count) *
+                               kGroups);
   return cudaSuccess;
 }
 
@@ -651,10 +784,13 @@ cudaError_t launch_frontier_g(const FrontierLaunch& launch, cudaStream_t stream)
   constexpr int kGroups = frontier_groups_per_block(G);
   // one group per workspace slot; the host sizes slots to the resident groups
   const unsigned grid = (launch.slots + kGroups - 1) / kGroups;
+  if (launch.cell_cost != nullptr && launch.corridor != nullptr) return cudaErrorInvalidValue;
   if (launch.cell_cost != nullptr) {
-    lattice_frontier_kernel<G, true><<<grid, kGroups * G * 32, 0, stream>>>(launch);
+    lattice_frontier_kernel<G, true, false><<<grid, kGroups * G * 32, 0, stream>>>(launch);
+  } else if (launch.corridor != nullptr) {
+    lattice_frontier_kernel<G, false, true><<<grid, kGroups * G * 32, 0, stream>>>(launch);
   } else {
-    lattice_frontier_kernel<G, false><<<grid, kGroups * G * 32, 0, stream>>>(launch);
+    lattice_frontier_kernel<G, false, false><<<grid, kGroups * G * 32, 0, stream>>>(launch);
   }
   return cudaGetLastError();
 }

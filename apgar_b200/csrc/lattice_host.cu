@@ -90,6 +90,9 @@ struct PlanObject {
   // cells, and one bit per label word to mark them
   const uint32_t* cell_cost_own = nullptr;
   uint32_t* own_bits = nullptr;
+  // corridor mode: caller-owned device bitmaps and the per-net outcomes
+  const uint32_t* corridor = nullptr;
+  DeviceBuffer<uint8_t> corridor_status;
   uint32_t* cancel_host = nullptr;  // pinned, mapped; polled by the kernels
   uint32_t* cancel_dev = nullptr;
   std::vector<ClassRange> classes;
@@ -421,6 +424,13 @@ int execute_plan(PlanObject* plan, cudaStream_t stream) {
   fbase.prev_results = plan->prev_results;
   fbase.prev_paths = plan->prev_paths;
   fbase.cell_cost_own = plan->cell_cost_own;
+  if (plan->corridor != nullptr) {
+    if (plan->cell_cost != nullptr) {
+      return set_error(APGAR_B200_UNSUPPORTED, "corridor mode is not combined with per-cell prices");
+    }
+    fbase.corridor = plan->corridor;
+    fbase.corridor_status = plan->corridor_status.get();
+  }
   SweepLaunch base{};
   base.lat = v;
   base.nets = plan->nets.get();
@@ -651,6 +661,39 @@ extern "C" int apgar_b200_lattice_plan_set_cell_costs(void* plan, const uint32_t
     return set_error(APGAR_B200_UNSUPPORTED, "per-cell prices need the frontier generator");
   }
   p->cell_cost = cell_costs;
+  clear_error();
+  return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_lattice_plan_set_corridors(void* plan, const uint32_t* corridor_bits) {
+  if (plan == nullptr) return set_error(APGAR_B200_INTERNAL_INVARIANT, "null plan");
+  auto* p = static_cast<PlanObject*>(plan);
+  if (corridor_bits != nullptr) {
+    if (p->generator != APGAR_B200_LATTICE_FRONTIER) {
+      return set_error(APGAR_B200_UNSUPPORTED, "corridors need the frontier generator");
+    }
+    if (int rc = check_device(p->device); rc != APGAR_B200_OK) return rc;
+    APGAR_B200_CUDA("cudaMalloc(corridor status)",
+                    p->corridor_status.ensure(std::max<uint32_t>(p->count, 1)));
+  }
+  p->corridor = corridor_bits;
+  clear_error();
+  return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_lattice_plan_corridor_status(void* plan, uint8_t* out) {
+  if (plan == nullptr || out == nullptr) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "null plan or output");
+  }
+  auto* p = static_cast<PlanObject*>(plan);
+  if (p->corridor_status.get() == nullptr) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "the plan never had corridors");
+  }
+  if (int rc = check_device(p->device); rc != APGAR_B200_OK) return rc;
+  if (p->count > 0) {
+    APGAR_B200_CUDA("cudaMemcpy(corridor status)",
+                    cudaMemcpy(out, p->corridor_status.get(), p->count, cudaMemcpyDeviceToHost));
+  }
   clear_error();
   return APGAR_B200_OK;
 }

@@ -431,6 +431,29 @@ typedef struct apgar_b200_lattice_options {
  * 2^31 - 1 comes back REJECTED instead of with a wrong cost. */
 APGAR_B200_API int apgar_b200_lattice_plan_set_cell_costs(void* plan, const uint32_t* cell_costs);
 
+/* Corridor mode of a FRONTIER plan (no reference counterpart: the learned
+ * corridor with its exact certificate).  `corridor_bits` is device memory,
+ * 128 uint32 words per net of the plan: a 64 x 64 bitmap of coarse cells over
+ * the net's window, bit cx of word 2 * cy + cx / 32 for coarse cell (cx, cy).
+ * A coarse cell covers 2^s x 2^s window cells on every layer, where s is the
+ * least value >= 2 with ceil(max(win_w, win_h) / 2^s) <= 64.  Each net first
+ * searches its corridor only.  The result is kept when its cost is strictly
+ * below the least key (label + move + admissible bound) over every legal
+ * move leaving the corridor that the search expanded, which proves it equal
+ * to the full-window result, path included.  Otherwise the net is searched
+ * again over the whole window, so results never depend on the corridor.
+ * NULL detaches the corridors.  Not combined with per-cell prices. */
+enum {
+  APGAR_B200_CORRIDOR_NONE = 0,
+  APGAR_B200_CORRIDOR_CERTIFIED = 1,          /* the corridor result, certified */
+  APGAR_B200_CORRIDOR_FALLBACK_EXIT = 2,      /* reached, but an exit key was <= its cost */
+  APGAR_B200_CORRIDOR_FALLBACK_UNREACHED = 3  /* a terminal outside, or goal not reached */
+};
+APGAR_B200_API int apgar_b200_lattice_plan_set_corridors(void* plan, const uint32_t* corridor_bits);
+/* Waits for the device and copies the per-net APGAR_B200_CORRIDOR_* outcomes
+ * of the last corridor-mode execution (one byte per net) to host memory. */
+APGAR_B200_API int apgar_b200_lattice_plan_corridor_status(void* plan, uint8_t* out);
+
 /* apgar_b200_lattice_plan / apgar_b200_lattice_route with a generator choice. */
 APGAR_B200_API int apgar_b200_lattice_plan_ex(void* lattice, const apgar_b200_lattice_net* nets,
                                uint32_t count, const apgar_b200_lattice_options* options,

@@ -306,3 +306,81 @@ def accumulate_cells(offsets, lengths, cells, cell_count):
     L.po_accumulate_cells(ctypes.c_uint32(len(lengths)), offsets.ctypes.data_as(U64P), _ptr(lengths),
                           _ptr(cells), ctypes.c_uint32(cell_count), _ptr(usage))
     return usage
+
+
+# ---------------------------------------------------------------------------
+# Corridor certificate (no reference counterpart): the exact restatement of
+# the frontier corridor mode's decision.  A net is searched in its corridor
+# only (cells outside it priced out of reach); every legal planar move from a
+# reached corridor cell u to a window cell v outside the corridor is an exit
+# with key d(u) + move + h(v), h the octile-plus-via bound.  The corridor
+# result is certified when its cost is strictly below every exit key.
+CORRIDOR_CERTIFIED, CORRIDOR_FALLBACK_EXIT, CORRIDOR_FALLBACK_UNREACHED = 1, 2, 3
+_STEPS = ((1, 0), (1, 1), (0, 1), (-1, 1), (-1, 0), (-1, -1), (0, -1), (1, -1))
+
+
+def _window_free(lat, net):
+    x0, y0 = int(net["win_x0"]), int(net["win_y0"])
+    w, h = int(net["win_w"]), int(net["win_h"])
+    words = np.ascontiguousarray(lat.blocked, dtype=np.uint32).reshape(lat.layers, lat.height, -1)
+    bits = np.unpackbits(words.view(np.uint8).reshape(lat.layers, lat.height, -1), axis=2,
+                         bitorder="little")
+    return bits[:, y0:y0 + h, x0:x0 + w] == 0
+
+
+def corridor_certificate(lat, net, mask):
+    """(status, corridor cost or None, least exit key or None) of one net
+    for a bool [64][64] coarse corridor (coarse scale as in
+    apgar_b200.corridor.coarse_shift)."""
+    net = np.ascontiguousarray(np.asarray(net).reshape(1))
+    n0 = net[0]
+    w, h = int(n0["win_w"]), int(n0["win_h"])
+    x0, y0 = int(n0["win_x0"]), int(n0["win_y0"])
+    span = max(w, h)
+    s = 2
+    while ((span - 1) >> s) >= 64:
+        s += 1
+    inside = np.asarray(mask, dtype=bool)[(np.arange(h) >> s)[:, None], (np.arange(w) >> s)[None, :]]
+    sx, sy = int(n0["start_x"]) - x0, int(n0["start_y"]) - y0
+    gx, gy = int(n0["goal_x"]) - x0, int(n0["goal_y"]) - y0
+    sl, gl = int(n0["start_layer"]), int(n0["goal_layer"])
+    if not (inside[sy, sx] and inside[gy, gx]):
+        return CORRIDOR_FALLBACK_UNREACHED, None, None
+    free = _window_free(lat, n0)
+    if not (free[sl, sy, sx] and free[gl, gy, gx]):
+        return CORRIDOR_CERTIFIED, None, None  # disconnected either way
+    big = 1 << 30
+    price = np.zeros((lat.layers, lat.height, lat.width), dtype=np.uint32)
+    price[:, y0:y0 + h, x0:x0 + w][:, ~inside] = big
+    cost, _, dist = dijkstra(lat, net, full=True, want_dist=True, cell_cost=price.reshape(-1))
+    if cost >= big:
+        return CORRIDOR_FALLBACK_UNREACHED, None, None
+    d = dist.reshape(lat.layers, h, w).astype(np.uint64)
+    reached = inside[None] & (d < big)
+    layer_term = (np.abs(np.arange(lat.layers) - gl) * lat.via).astype(np.uint64)[:, None, None]
+    best = None
+    for dx, dy in _STEPS:
+        # u at (y, x) and v at (y + dy, x + dx), both inside the window
+        uy = slice(max(0, -dy), h - max(0, dy))
+        ux = slice(max(0, -dx), w - max(0, dx))
+        vy = slice(uy.start + dy, uy.stop + dy)
+        vx = slice(ux.start + dx, ux.stop + dx)
+        legal = free[:, uy, ux] & free[:, vy, vx]
+        if dx != 0 and dy != 0:
+            legal &= free[:, uy, vx] & free[:, vy, ux]
+        exits = reached[:, uy, ux] & ~inside[None, vy, vx] & legal
+        if not exits.any():
+            continue
+        move = lat.diag if (dx != 0 and dy != 0) else lat.orth
+        adx = np.abs(np.arange(w)[vx] - gx)[None, :]
+        ady = np.abs(np.arange(h)[vy] - gy)[:, None]
+        lo, hi = np.minimum(adx, ady), np.maximum(adx, ady)
+        if lat.diag >= lat.orth:
+            planar = lo * min(lat.diag, 2 * lat.orth) + (hi - lo) * lat.orth
+        else:
+            planar = hi * lat.diag
+        key = d[:, uy, ux] + np.uint64(move) + planar.astype(np.uint64)[None] + layer_term
+        m = int(key[exits].min())
+        best = m if best is None else min(best, m)
+    status = CORRIDOR_CERTIFIED if best is None or cost < best else CORRIDOR_FALLBACK_EXIT
+    return status, int(cost), best
