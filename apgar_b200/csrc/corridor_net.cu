@@ -1,0 +1,933 @@
+// The learned corridor: a 6-layer 3x3 CNN (32 channels, BF16 weights and
+// activations, FP32 accumulation) over 64 x 64 coarse rasters of each net's
+// window, trained on the GPU by its own forward and backward kernels.
+//
+// Layout.  Every net owns a 64 x 64 coarse grid (coarse cell = 2^s x 2^s
+// window cells on all layers, the corridor bitmap's scale); only the top-left
+// cw x ch cells lie inside the window.  Tensors are NHWC bf16 [net][64][64][C];
+// cells outside the window are never read (treated as zero, "same" padding at
+// the window border) and never written.
+//
+// Layers 1-5 (3x3, 16 -> 32 then 32 -> 32, bias, ReLU) run as implicit GEMMs
+// on the 5th-generation tensor cores: a CTA takes 128 output cells (two rows
+// of one net), gathers their 3x3 neighbourhoods (im2col) into shared memory
+// as the A operand (M = 128 cells, K = 9 * Cin, K-major, no swizzle), keeps
+// the weights resident as the B operand (N = 32 channels), and one elected
+// thread issues tcgen05.mma (kind::f16, bf16 x bf16 -> f32) into a 128 x 32
+// tensor-memory accumulator.  The epilogue reads it back with tcgen05.ld (one
+// warp per 32 TMEM lanes), adds the bias, applies the ReLU and stores bf16.
+// The input gradient of layers 2-5 is the same kernel run on the output
+// gradient with the spatially flipped, transposed weights; its epilogue gates
+// by the previous layer's ReLU.  The weight gradient is a second tcgen05 GEMM:
+// D[(tap, ci)][co] = sum over cells of im2col(x)[cell][(tap, ci)] *
+// dy[cell][co], with both operands MN-major (the cell index is K), so the NHWC
+// rows load as 16-byte chunks; each CTA accumulates its cells in TMEM and adds
+// its partial sums to the FP32 gradient once.
+//
+// The head (3x3, 32 -> 1, FP32 weights), the loss, the bias gradients, Adam
+// and the corridor extraction are small and run on the CUDA cores.
+//
+// Every wait on a tensor-core completion is bounded: on expiry the kernel
+// records APGAR_B200_CNN_TIMEOUT in its error word, waits once more (bounded)
+// for its own MMAs, frees its tensor memory and returns.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "apgar_b200.h"
+#include "lattice_common.cuh"
+
+namespace apgar_b200 {
+namespace {
+
+constexpr int kGrid = 64;          // coarse cells per side
+constexpr int kCells = kGrid * kGrid;
+constexpr int kCin0 = 16;          // raster channels
+constexpr int kCh = 32;            // hidden channels
+constexpr uint32_t kWaitLimit = 1u << 22;
+
+// ----------------------------- tcgen05 helpers -----------------------------
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor, no swizzle: start, leading-dimension and
+// stride-dimension byte offsets (16-byte units), descriptor version 1.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) |
+         (static_cast<uint64_t>((lbo >> 4) & 0x3FFFu) << 16) |
+         (static_cast<uint64_t>((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: bf16 A and B, f32 accumulator, M x N,
+// K-major (0) or MN-major (1) operands.
+__host__ __device__ constexpr uint32_t idesc_bf16(int m, int n, int a_mn, int b_mn) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(a_mn) << 15) |
+         (static_cast<uint32_t>(b_mn) << 16) | (static_cast<uint32_t>(n >> 3) << 17) |
+         (static_cast<uint32_t>(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc,
+                                         uint32_t accumulate) {
+  const uint32_t mask0 = 0, mask1 = 0, mask2 = 0, mask3 = 0;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(mask0), "r"(mask1), "r"(mask2), "r"(mask3));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+
+__device__ __forceinline__ void fence_after_sync() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_before_sync() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void bar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Bounded wait for the barrier phase with parity `phase`; true when it completed.
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t phase) {
+  for (uint32_t it = 0; it < kWaitLimit; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(phase)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// Warp 0 allocates `cols` TMEM columns; the base address lands in *slot.
+__device__ __forceinline__ void tmem_alloc(uint32_t* slot, uint32_t cols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(slot)),
+               "r"(cols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_free(uint32_t base, uint32_t cols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(base), "r"(cols) : "memory");
+}
+
+// 32 consecutive f32 accumulator columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_load32(uint32_t taddr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+        "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+        "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ uint32_t dims_w(uint32_t d) { return d & 0xFFu; }
+__device__ __forceinline__ uint32_t dims_h(uint32_t d) { return (d >> 8) & 0xFFu; }
+
+__device__ __forceinline__ size_t cell_of(uint32_t net, int y, int x) {
+  return (static_cast<size_t>(net) * kGrid + static_cast<size_t>(y)) * kGrid + static_cast<size_t>(x);
+}
+
+__device__ __forceinline__ uint4 pack8(const float* v) {
+  uint4 o;
+  __nv_bfloat162 a = __floats2bfloat162_rn(v[0], v[1]), b = __floats2bfloat162_rn(v[2], v[3]),
+                  c = __floats2bfloat162_rn(v[4], v[5]), d = __floats2bfloat162_rn(v[6], v[7]);
+  o.x = *reinterpret_cast<uint32_t*>(&a);
+  o.y = *reinterpret_cast<uint32_t*>(&b);
+  o.z = *reinterpret_cast<uint32_t*>(&c);
+  o.w = *reinterpret_cast<uint32_t*>(&d);
+  return o;
+}
+
+__device__ __forceinline__ void unpack8(uint4 q, float* v) {
+  const uint32_t w[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    v[2 * i] = __uint_as_float(w[i] << 16);
+    v[2 * i + 1] = __uint_as_float(w[i] & 0xFFFF0000u);
+  }
+}
+
+// ------------------------------- rasters ----------------------------------
+
+// One block per net: the 16 input channels of every coarse cell, plus the
+// net's coarse dims (cw | ch << 8 | s << 16).
+__global__ void raster_kernel(LatticeDeviceView lat, const apgar_b200_lattice_net* __restrict__ nets,
+                              uint32_t count, const uint32_t* __restrict__ cell_cost,
+                              __nv_bfloat16* __restrict__ out, uint32_t* __restrict__ dims) {
+  const uint32_t n = blockIdx.x;
+  if (n >= count) return;
+  const apgar_b200_lattice_net net = nets[n];
+  const int w = static_cast<int>(net.win_w), h = static_cast<int>(net.win_h);
+  int s = 2;
+  while ((((w > h ? w : h) - 1) >> s) >= kGrid) ++s;
+  const int cw = (w + (1 << s) - 1) >> s, ch = (h + (1 << s) - 1) >> s;
+  if (threadIdx.x == 0) dims[n] = static_cast<uint32_t>(cw) | (static_cast<uint32_t>(ch) << 8) |
+                                  (static_cast<uint32_t>(s) << 16);
+  const float scx = static_cast<float>((static_cast<int>(net.start_x) - static_cast<int>(net.win_x0)) >> s);
+  const float scy = static_cast<float>((static_cast<int>(net.start_y) - static_cast<int>(net.win_y0)) >> s);
+  const float gcx = static_cast<float>((static_cast<int>(net.goal_x) - static_cast<int>(net.win_x0)) >> s);
+  const float gcy = static_cast<float>((static_cast<int>(net.goal_y) - static_cast<int>(net.win_y0)) >> s);
+  const float sgx = gcx - scx, sgy = gcy - scy;
+  const float seg2 = sgx * sgx + sgy * sgy;
+  for (int c = threadIdx.x; c < kCells; c += blockDim.x) {
+    const int cy = c / kGrid, cx = c % kGrid;
+    float v[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = 0.f;
+    if (cx < cw && cy < ch) {
+      const int x0 = cx << s, x1 = min(w, (cx + 1) << s);
+      const int y0 = cy << s, y1 = min(h, (cy + 1) << s);
+      const int gx0 = static_cast<int>(net.win_x0) + x0, gx1 = static_cast<int>(net.win_x0) + x1;
+      uint32_t blocked = 0, all_blocked = 0;
+      for (int y = y0; y < y1; ++y) {
+        const int gy = static_cast<int>(net.win_y0) + y;
+        for (int wi = gx0 >> 5; wi <= (gx1 - 1) >> 5; ++wi) {
+          const int lo = max(gx0, wi << 5) - (wi << 5), hi = min(gx1, (wi + 1) << 5) - (wi << 5);
+          const uint32_t m = (hi >= 32 ? 0xFFFFFFFFu : ((1u << hi) - 1u)) & ~((1u << lo) - 1u);
+          uint32_t all = 0xFFFFFFFFu;
+          for (int l = 0; l < lat.layers; ++l) {
+            const uint32_t word =
+                __ldg(lat.blocked + (static_cast<size_t>(l) * lat.height + gy) * lat.words + wi);
+            blocked += __popc(word & m);
+            all &= word;
+          }
+          all_blocked += __popc(all & m);
+        }
+      }
+      const float cells = static_cast<float>((x1 - x0) * (y1 - y0));
+      v[0] = static_cast<float>(blocked) / (cells * static_cast<float>(lat.layers));
+      v[1] = static_cast<float>(all_blocked) / cells;
+      if (cell_cost != nullptr) {
+        // congestion: mean entry price over a sample of at most 4 x 4 cells per layer
+        const int step = max(1, (1 << s) / 4);
+        float sum = 0.f, k = 0.f;
+        for (int l = 0; l < lat.layers; ++l) {
+          for (int y = y0; y < y1; y += step) {
+            for (int x = x0; x < x1; x += step) {
+              const size_t gi = (static_cast<size_t>(l) * lat.height + (net.win_y0 + y)) * lat.width +
+                                (net.win_x0 + x);
+              sum += fminf(static_cast<float>(__ldg(cell_cost + gi)), 65535.f);
+              k += 1.f;
+            }
+          }
+        }
+        v[2] = fminf(sum / (k * 1024.f), 8.f);
+      }
+      const float fx = static_cast<float>(cx), fy = static_cast<float>(cy);
+      v[3] = (fx == scx && fy == scy) ? 1.f : 0.f;
+      v[4] = (fx == gcx && fy == gcy) ? 1.f : 0.f;
+      v[5] = 1.f;
+      v[6] = (fx - scx) / 32.f;
+      v[7] = (fy - scy) / 32.f;
+      v[8] = (fx - gcx) / 32.f;
+      v[9] = (fy - gcy) / 32.f;
+      // distance to the start-goal segment, in coarse cells
+      float t = seg2 > 0.f ? ((fx - scx) * sgx + (fy - scy) * sgy) / seg2 : 0.f;
+      t = fminf(fmaxf(t, 0.f), 1.f);
+      const float ex = fx - (scx + t * sgx), ey = fy - (scy + t * sgy);
+      v[10] = fminf(sqrtf(ex * ex + ey * ey) / 8.f, 4.f);
+    }
+    uint4* dst = reinterpret_cast<uint4*>(out + cell_of(n, cy, cx) * kCin0);
+    dst[0] = pack8(v);
+    dst[1] = pack8(v + 8);
+  }
+}
+
+// Coarse training labels: 1 where the net's reached path has a cell.
+__global__ void labels_kernel(const apgar_b200_lattice_net* __restrict__ nets, uint32_t count,
+                              const uint32_t* __restrict__ dims, int lat_w, int lat_h,
+                              const apgar_b200_lattice_result* __restrict__ results,
+                              const uint32_t* __restrict__ paths, uint8_t* __restrict__ labels) {
+  const uint32_t n = blockIdx.x;
+  if (n >= count) return;
+  uint8_t* lab = labels + static_cast<size_t>(n) * kCells;
+  for (int c = threadIdx.x; c < kCells; c += blockDim.x) lab[c] = 0;
+  __syncthreads();
+  const apgar_b200_lattice_result r = results[n];
+  if (r.completion != APGAR_B200_COMPLETION_REACHED) return;
+  const int s = static_cast<int>(dims[n] >> 16);
+  const apgar_b200_lattice_net net = nets[n];
+  for (uint32_t j = threadIdx.x; j < r.path_len; j += blockDim.x) {
+    const uint32_t c = paths[r.path_offset + j];
+    const int x = static_cast<int>(c % static_cast<uint32_t>(lat_w)) - static_cast<int>(net.win_x0);
+    const int y = static_cast<int>((c / static_cast<uint32_t>(lat_w)) % static_cast<uint32_t>(lat_h)) -
+                  static_cast<int>(net.win_y0);
+    if (x >= 0 && y >= 0 && x < static_cast<int>(net.win_w) && y < static_cast<int>(net.win_h)) {
+      lab[(y >> s) * kGrid + (x >> s)] = 1;
+    }
+  }
+}
+
+// ------------------------ 3x3 conv on tensor cores -------------------------
+
+struct ConvArgs {
+  const __nv_bfloat16* x;     // [n][64][64][cin]
+  const __nv_bfloat16* w;     // [32][9 * cin], k = tap * cin + ci, tap = (dy + 1) * 3 + dx + 1
+  const float* bias;          // kRelu: [32]
+  const __nv_bfloat16* gate;  // kGate: [n][64][64][32]; output *= (gate > 0)
+  __nv_bfloat16* y;           // [n][64][64][32]
+  const uint32_t* dims;
+  uint32_t count;
+  uint32_t* error;
+};
+
+enum { kEpiRelu = 0, kEpiGate = 1 };
+
+template <int CIN>
+struct ConvSmem {
+  static constexpr int K = 9 * CIN;
+  static constexpr int kChunks = K / 8;          // 16-byte chunks per operand row
+  static constexpr int kSboA = kChunks * 128;    // bytes between 8-row groups
+  static constexpr int kBytesA = 16 * kSboA;     // 128 rows
+  static constexpr int kBytesB = 4 * kSboA;      // 32 rows
+  static constexpr int kBytes = kBytesA + kBytesB + 16;
+};
+
+// out[cell][co] = epilogue(sum_{tap, ci} x[cell + tap][ci] * w[co][tap][ci]).
+template <int CIN, int EPI>
+__global__ void __launch_bounds__(128) conv3x3_tc_kernel(ConvArgs a) {
+  using S = ConvSmem<CIN>;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t* sa = smem;
+  uint8_t* sb = smem + S::kBytesA;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S::kBytesA + S::kBytesB);
+  __shared__ uint32_t tmem_slot;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+
+  // weights: the resident B operand (N = 32 rows, K-major)
+  for (int u = tid; u < 32 * S::kChunks; u += 128) {
+    const int n = u / S::kChunks, c = u % S::kChunks;
+    const uint4 v = __ldg(reinterpret_cast<const uint4*>(a.w + static_cast<size_t>(n) * S::K) + c);
+    *reinterpret_cast<uint4*>(sb + (n % 8) * 16 + (n / 8) * S::kSboA + c * 128) = v;
+  }
+  if (warp == 0) tmem_alloc(&tmem_slot, 32);
+  if (tid == 0) bar_init(smem_addr(bar), 1);
+  fence_async_smem();
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = tmem_slot;
+  const uint32_t idesc = idesc_bf16(128, 32, 0, 0);
+  uint32_t phase = 0;
+  bool failed = false;
+
+  const uint32_t items = a.count * (kGrid / 2);
+  for (uint32_t item = blockIdx.x; item < items; item += gridDim.x) {
+    const uint32_t net = item / (kGrid / 2);
+    const int y0 = static_cast<int>(item % (kGrid / 2)) * 2;
+    const uint32_t d = a.dims[net];
+    const int cw = static_cast<int>(dims_w(d)), ch = static_cast<int>(dims_h(d));
+    if (y0 >= ch) continue;  // uniform: no cell of these rows is in the window
+    // im2col: A[m][tap * CIN + ci] for the 128 cells (rows y0, y0 + 1)
+    for (int u = tid; u < 128 * 9 * (CIN / 8); u += 128) {
+      const int m = u % 128, r = u / 128;
+      const int j = r % (CIN / 8), t = r / (CIN / 8);
+      const int py = y0 + m / kGrid, px = m % kGrid;
+      const int sy = py + t / 3 - 1, sx = px + t % 3 - 1;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (px < cw && py < ch && sx >= 0 && sy >= 0 && sx < cw && sy < ch) {
+        v = __ldg(reinterpret_cast<const uint4*>(a.x + cell_of(net, sy, sx) * CIN) + j);
+      }
+      *reinterpret_cast<uint4*>(sa + (m % 8) * 16 + (m / 8) * S::kSboA + (t * (CIN / 8) + j) * 128) = v;
+    }
+    fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      fence_after_sync();
+      const uint32_t a0 = smem_addr(sa), b0 = smem_addr(sb);
+#pragma unroll 1
+      for (int kk = 0; kk < S::K / 16; ++kk) {
+        mma_bf16(tmem, umma_desc(a0 + kk * 256, 128, S::kSboA), umma_desc(b0 + kk * 256, 128, S::kSboA),
+                 idesc, kk > 0 ? 1u : 0u);
+      }
+      mma_commit(smem_addr(bar));
+    }
+    const bool ok = bar_wait(smem_addr(bar), phase);
+    phase ^= 1u;
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      break;
+    }
+    fence_after_sync();
+    // epilogue: thread = accumulator row = cell m
+    float v[32];
+    tmem_load32(tmem + (static_cast<uint32_t>(warp * 32) << 16), v);
+    const int m = warp * 32 + lane;
+    const int py = y0 + m / kGrid, px = m % kGrid;
+    if (px < cw && py < ch) {
+      const size_t cell = cell_of(net, py, px);
+      if constexpr (EPI == kEpiRelu) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) v[c] = fmaxf(v[c] + __ldg(a.bias + c), 0.f);
+      } else {
+        const uint4* g = reinterpret_cast<const uint4*>(a.gate + cell * kCh);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          float gv[8];
+          unpack8(__ldg(g + q), gv);
+#pragma unroll
+          for (int i = 0; i < 8; ++i) v[q * 8 + i] = gv[i] > 0.f ? v[q * 8 + i] : 0.f;
+        }
+      }
+      uint4* dst = reinterpret_cast<uint4*>(a.y + cell * kCh);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) dst[q] = pack8(v + q * 8);
+    }
+    fence_before_sync();
+    __syncthreads();
+  }
+  if (failed) {
+    if (tid == 0) atomicOr(a.error, APGAR_B200_CNN_TIMEOUT);
+    bar_wait(smem_addr(bar), phase);  // once more, bounded, for the MMAs in flight
+  }
+  fence_before_sync();
+  __syncthreads();
+  if (warp == 0) tmem_free(tmem, 32);
+}
+
+// ------------------- weight gradient on tensor cores ----------------------
+
+struct WgradArgs {
+  const __nv_bfloat16* x;   // layer input [n][64][64][cin]
+  const __nv_bfloat16* dy;  // gradient at the layer's pre-activation [n][64][64][32]
+  const uint32_t* dims;
+  uint32_t count;
+  float* dw;                // [32][9 * cin] (added to)
+  float* db;                // [32] (added to)
+  uint32_t* error;
+};
+
+template <int CIN>
+struct WgradSmem {
+  static constexpr int K = 9 * CIN;                    // rows of D
+  static constexpr int kTiles = (K + 127) / 128;       // M tiles of 128 rows
+  static constexpr int kSbo = 2048;                    // 16 K-groups x 128 bytes
+  static constexpr int kBytesTile = 16 * kSbo;         // 128 rows x 128 cells
+  static constexpr int kBytesA = kTiles * kBytesTile;
+  static constexpr int kBytesB = 4 * kSbo;             // 32 rows x 128 cells
+  static constexpr int kBytes = kBytesA + kBytesB + 16;
+};
+
+// dw[co][tap * CIN + ci] += sum over cells of x[cell + tap][ci] * dy[cell][co];
+// db[co] += sum over cells of dy[cell][co].  Operands MN-major: element
+// (row r, cell k) at (r % 8) * 2 + (k % 8) * 16 + (r / 8) * SBO + (k / 8) * 128.
+template <int CIN>
+__global__ void __launch_bounds__(128) conv_wgrad_tc_kernel(WgradArgs a) {
+  using S = WgradSmem<CIN>;
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t* sa = smem;
+  uint8_t* sb = smem + S::kBytesA;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S::kBytesA + S::kBytesB);
+  __shared__ uint32_t tmem_slot;
+  __shared__ float bias_part[32];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // rows K .. kTiles * 128 of the last tile stay zero
+  for (int u = tid; u < S::kBytesA / 16; u += 128) reinterpret_cast<uint4*>(sa)[u] = make_uint4(0, 0, 0, 0);
+  if (tid < 32) bias_part[tid] = 0.f;
+  if (warp == 0) tmem_alloc(&tmem_slot, 128);
+  if (tid == 0) bar_init(smem_addr(bar), 1);
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+  const uint32_t tmem = tmem_slot;
+  const uint32_t idesc = idesc_bf16(128, 32, 1, 1);
+  uint32_t phase = 0;
+  bool failed = false, any = false;
+  float bsum = 0.f;  // this thread's share of db (co = tid % 32)
+
+  const uint32_t items = a.count * (kGrid / 2);
+  for (uint32_t item = blockIdx.x; item < items; item += gridDim.x) {
+    const uint32_t net = item / (kGrid / 2);
+    const int y0 = static_cast<int>(item % (kGrid / 2)) * 2;
+    const uint32_t d = a.dims[net];
+    const int cw = static_cast<int>(dims_w(d)), ch = static_cast<int>(dims_h(d));
+    if (y0 >= ch) continue;
+    // B: dy chunks (8 channels) per cell; zero outside the window
+    for (int u = tid; u < 128 * 4; u += 128) {
+      const int k = u % 128, j = u / 128;
+      const int py = y0 + k / kGrid, px = k % kGrid;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (px < cw && py < ch) v = __ldg(reinterpret_cast<const uint4*>(a.dy + cell_of(net, py, px) * kCh) + j);
+      *reinterpret_cast<uint4*>(sb + (k % 8) * 16 + j * S::kSbo + (k / 8) * 128) = v;
+    }
+    // A: im2col rows (tap, ci) per cell
+    for (int u = tid; u < 128 * 9 * (CIN / 8); u += 128) {
+      const int k = u % 128, r = u / 128;
+      const int j = r % (CIN / 8), t = r / (CIN / 8);
+      const int py = y0 + k / kGrid, px = k % kGrid;
+      const int sy = py + t / 3 - 1, sx = px + t % 3 - 1;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (px < cw && py < ch && sx >= 0 && sy >= 0 && sx < cw && sy < ch) {
+        v = __ldg(reinterpret_cast<const uint4*>(a.x + cell_of(net, sy, sx) * CIN) + j);
+      }
+      const int row = t * CIN + j * 8;
+      *reinterpret_cast<uint4*>(sa + (row / 128) * S::kBytesTile + (k % 8) * 16 + ((row % 128) / 8) * S::kSbo +
+                                (k / 8) * 128) = v;
+    }
+    fence_async_smem();
+    __syncthreads();
+    // bias gradient from the staged dy (thread: channel tid % 32, cells tid / 32 + 4 i)
+    {
+      const int c = tid % 32;
+      for (int k = tid / 32; k < 128; k += 4) {
+        const __nv_bfloat16* e = reinterpret_cast<const __nv_bfloat16*>(
+            sb + (k % 8) * 16 + (c / 8) * S::kSbo + (k / 8) * 128) + (c % 8);
+        bsum += __bfloat162float(*e);
+      }
+    }
+    if (tid == 0) {
+      fence_after_sync();
+      const uint32_t b0 = smem_addr(sb);
+#pragma unroll 1
+      for (int mt = 0; mt < S::kTiles; ++mt) {
+        const uint32_t a0 = smem_addr(sa) + mt * S::kBytesTile;
+#pragma unroll 1
+        for (int kk = 0; kk < 8; ++kk) {
+          mma_bf16(tmem + mt * 32, umma_desc(a0 + kk * 256, 128, S::kSbo),
+                   umma_desc(b0 + kk * 256, 128, S::kSbo), idesc, (any || kk > 0) ? 1u : 0u);
+        }
+      }
+      mma_commit(smem_addr(bar));
+    }
+    any = true;
+    const bool ok = bar_wait(smem_addr(bar), phase);
+    phase ^= 1u;
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      break;
+    }
+  }
+  if (failed) {
+    if (tid == 0) atomicOr(a.error, APGAR_B200_CNN_TIMEOUT);
+    bar_wait(smem_addr(bar), phase);
+  } else if (any) {
+    fence_after_sync();
+    for (int mt = 0; mt < S::kTiles; ++mt) {
+      float v[32];
+      tmem_load32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + mt * 32, v);
+      const int row = mt * 128 + warp * 32 + lane;
+      if (row < S::K) {
+#pragma unroll
+        for (int c = 0; c < 32; ++c) atomicAdd(a.dw + c * S::K + row, v[c]);
+      }
+    }
+    atomicAdd(&bias_part[tid % 32], bsum);
+  }
+  fence_before_sync();
+  __syncthreads();
+  if (!failed && any && tid < 32) atomicAdd(a.db + tid, bias_part[tid]);
+  if (warp == 0) tmem_free(tmem, 128);
+}
+
+// ------------------------------ head + loss -------------------------------
+
+// logit[cell] = b6 + sum_{tap, ci} w6[tap][ci] * act[cell + tap][ci] (FP32).
+__global__ void head_forward_kernel(const __nv_bfloat16* __restrict__ act, const float* __restrict__ w6,
+                                    const float* __restrict__ b6, const uint32_t* __restrict__ dims,
+                                    uint32_t count, float* __restrict__ logits) {
+  __shared__ float ws[9 * kCh];
+  for (int i = threadIdx.x; i < 9 * kCh; i += blockDim.x) ws[i] = w6[i];
+  __syncthreads();
+  const size_t total = static_cast<size_t>(count) * kCells;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const uint32_t net = static_cast<uint32_t>(i / kCells);
+    const int y = static_cast<int>((i / kGrid) % kGrid), x = static_cast<int>(i % kGrid);
+    const uint32_t d = dims[net];
+    const int cw = static_cast<int>(dims_w(d)), ch = static_cast<int>(dims_h(d));
+    float z = 0.f;
+    if (x < cw && y < ch) {
+      z = b6[0];
+      for (int t = 0; t < 9; ++t) {
+        const int sy = y + t / 3 - 1, sx = x + t % 3 - 1;
+        if (sx < 0 || sy < 0 || sx >= cw || sy >= ch) continue;
+        const uint4* src = reinterpret_cast<const uint4*>(act + cell_of(net, sy, sx) * kCh);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          float v[8];
+          unpack8(__ldg(src + q), v);
+#pragma unroll
+          for (int k = 0; k < 8; ++k) z = fmaf(ws[t * kCh + q * 8 + k], v[k], z);
+        }
+      }
+    }
+    logits[i] = z;
+  }
+}
+
+// Weighted binary cross-entropy on logits, averaged over each net's window
+// cells and then over nets: dlogit = weight * (sigmoid(z) - y) / (cells * count).
+__global__ void loss_kernel(const float* __restrict__ logits, const uint8_t* __restrict__ labels,
+                            const uint32_t* __restrict__ dims, uint32_t count, float pos_weight,
+                            float* __restrict__ dlogit, float* __restrict__ loss) {
+  float acc = 0.f;
+  const size_t total = static_cast<size_t>(count) * kCells;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const uint32_t net = static_cast<uint32_t>(i / kCells);
+    const int y = static_cast<int>((i / kGrid) % kGrid), x = static_cast<int>(i % kGrid);
+    const uint32_t d = dims[net];
+    const int cw = static_cast<int>(dims_w(d)), ch = static_cast<int>(dims_h(d));
+    float g = 0.f;
+    if (x < cw && y < ch) {
+      const float z = logits[i];
+      const float t = labels[i] ? 1.f : 0.f;
+      const float wgt = labels[i] ? pos_weight : 1.f;
+      const float norm = 1.f / (static_cast<float>(cw * ch) * static_cast<float>(count));
+      const float sig = 1.f / (1.f + __expf(-z));
+      g = wgt * (sig - t) * norm;
+      acc += wgt * (fmaxf(z, 0.f) - z * t + log1pf(__expf(-fabsf(z)))) * norm;
+    }
+    dlogit[i] = g;
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+  if ((threadIdx.x & 31) == 0 && acc != 0.f) atomicAdd(loss, acc);
+}
+
+// Head backward, one warp per cell and one lane per channel ci:
+//   dact[cell][ci] = sum_tap w6[tap][ci] * dlogit[cell - tap], gated by act > 0
+//   dw6[tap][ci] += dlogit[cell] * act[cell + tap][ci];  db6 += dlogit[cell]
+__global__ void head_backward_kernel(const __nv_bfloat16* __restrict__ act, const float* __restrict__ w6,
+                                     const float* __restrict__ dlogit, const uint32_t* __restrict__ dims,
+                                     uint32_t count, __nv_bfloat16* __restrict__ dact,
+                                     float* __restrict__ dw6, float* __restrict__ db6) {
+  const int lane = threadIdx.x & 31;
+  float wcol[9], acc[9];
+#pragma unroll
+  for (int t = 0; t < 9; ++t) {
+    wcol[t] = w6[t * kCh + lane];
+    acc[t] = 0.f;
+  }
+  float bacc = 0.f;
+  const size_t total = static_cast<size_t>(count) * kCells;
+  const size_t warps = static_cast<size_t>(gridDim.x) * (blockDim.x / 32);
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x / 32) + (threadIdx.x >> 5); i < total; i += warps) {
+    const uint32_t net = static_cast<uint32_t>(i / kCells);
+    const int y = static_cast<int>((i / kGrid) % kGrid), x = static_cast<int>(i % kGrid);
+    const uint32_t d = dims[net];
+    const int cw = static_cast<int>(dims_w(d)), ch = static_cast<int>(dims_h(d));
+    if (x >= cw || y >= ch) continue;
+    const float dl = dlogit[i];
+    float da = 0.f;
+#pragma unroll
+    for (int t = 0; t < 9; ++t) {
+      const int dy = t / 3 - 1, dx = t % 3 - 1;
+      // output cell (y - dy, x - dx) reads this cell through tap t
+      const int oy = y - dy, ox = x - dx;
+      if (ox >= 0 && oy >= 0 && ox < cw && oy < ch) da = fmaf(wcol[t], dlogit[cell_of(net, oy, ox)], da);
+      const int sy = y + dy, sx = x + dx;
+      if (sx >= 0 && sy >= 0 && sx < cw && sy < ch) {
+        acc[t] = fmaf(dl, __bfloat162float(act[cell_of(net, sy, sx) * kCh + lane]), acc[t]);
+      }
+    }
+    const float a = __bfloat162float(act[cell_of(net, y, x) * kCh + lane]);
+    dact[cell_of(net, y, x) * kCh + lane] = __float2bfloat16_rn(a > 0.f ? da : 0.f);
+    bacc += dl;
+  }
+#pragma unroll
+  for (int t = 0; t < 9; ++t) atomicAdd(dw6 + t * kCh + lane, acc[t]);
+  if (lane == 0) atomicAdd(db6, bacc);
+}
+
+// ------------------------------ parameters --------------------------------
+
+// FP32 parameters: layer l (cin_l = 16 for l = 0, else 32): w [32][9][cin_l]
+// then b [32]; head: w6 [9][32] then b6.
+struct ParamOffsets {
+  uint32_t w[5], b[5], w6, b6, total;
+};
+
+__host__ __device__ constexpr ParamOffsets param_offsets() {
+  ParamOffsets o{};
+  uint32_t at = 0;
+  for (int l = 0; l < 5; ++l) {
+    const uint32_t cin = l == 0 ? kCin0 : kCh;
+    o.w[l] = at;
+    at += 32 * 9 * cin;
+    o.b[l] = at;
+    at += 32;
+  }
+  o.w6 = at;
+  at += 9 * kCh;
+  o.b6 = at;
+  at += 1;
+  o.total = at;
+  return o;
+}
+
+// bf16 operands: forward wf[l] = [co][tap * cin + ci]; backward (l >= 1)
+// wb[l] = [ci][tap' * 32 + co] with tap' = 8 - tap (flipped kernel).
+struct OperandOffsets {
+  uint32_t wf[5], wb[5], total;
+};
+
+__host__ __device__ constexpr OperandOffsets operand_offsets() {
+  OperandOffsets o{};
+  uint32_t at = 0;
+  for (int l = 0; l < 5; ++l) {
+    o.wf[l] = at;
+    at += 32 * 9 * (l == 0 ? kCin0 : kCh);
+  }
+  for (int l = 0; l < 5; ++l) {
+    o.wb[l] = at;
+    if (l > 0) at += 32 * 9 * kCh;
+  }
+  o.total = at;
+  return o;
+}
+
+__global__ void prepare_kernel(const float* __restrict__ params, __nv_bfloat16* __restrict__ ops) {
+  constexpr ParamOffsets P = param_offsets();
+  constexpr OperandOffsets O = operand_offsets();
+  for (int l = 0; l < 5; ++l) {
+    const int cin = l == 0 ? kCin0 : kCh;
+    const int n = 32 * 9 * cin;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+      const float v = params[P.w[l] + i];  // i = (co * 9 + tap) * cin + ci
+      ops[O.wf[l] + i] = __float2bfloat16_rn(v);
+      if (l > 0) {
+        const int ci = i % cin, tap = (i / cin) % 9, co = i / (9 * cin);
+        ops[O.wb[l] + ci * (9 * kCh) + (8 - tap) * kCh + co] = __float2bfloat16_rn(v);
+      }
+    }
+  }
+}
+
+__global__ void adam_kernel(float* __restrict__ params, const float* __restrict__ grads,
+                            float* __restrict__ m, float* __restrict__ v, uint32_t n, float lr,
+                            float beta1, float beta2, float eps, float c1, float c2) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float g = grads[i];
+    const float mi = beta1 * m[i] + (1.f - beta1) * g;
+    const float vi = beta2 * v[i] + (1.f - beta2) * g * g;
+    m[i] = mi;
+    v[i] = vi;
+    params[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  }
+}
+
+// -------------------------- corridors from logits -------------------------
+
+// One block per net: coarse cells with logit > threshold, dilated by
+// `dilate` coarse cells (Chebyshev), plus both terminals, as the 128-word
+// corridor bitmap (bit cx % 32 of word 2 * cy + cx / 32).
+__global__ void corridor_kernel(const float* __restrict__ logits, const uint32_t* __restrict__ dims,
+                                const apgar_b200_lattice_net* __restrict__ nets, uint32_t count,
+                                float threshold, int dilate, uint32_t* __restrict__ bits) {
+  __shared__ uint8_t hot[kCells];
+  const uint32_t n = blockIdx.x;
+  if (n >= count) return;
+  const uint32_t d = dims[n];
+  const int cw = static_cast<int>(dims_w(d)), ch = static_cast<int>(dims_h(d));
+  const int s = static_cast<int>(d >> 16);
+  const float* z = logits + static_cast<size_t>(n) * kCells;
+  for (int c = threadIdx.x; c < kCells; c += blockDim.x) {
+    const int y = c / kGrid, x = c % kGrid;
+    hot[c] = (x < cw && y < ch && z[c] > threshold) ? 1 : 0;
+  }
+  __syncthreads();
+  const apgar_b200_lattice_net net = nets[n];
+  const int sx = (static_cast<int>(net.start_x) - static_cast<int>(net.win_x0)) >> s;
+  const int sy = (static_cast<int>(net.start_y) - static_cast<int>(net.win_y0)) >> s;
+  const int gx = (static_cast<int>(net.goal_x) - static_cast<int>(net.win_x0)) >> s;
+  const int gy = (static_cast<int>(net.goal_y) - static_cast<int>(net.win_y0)) >> s;
+  // one warp per output word: 32 coarse cells of one row
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int wd = warp; wd < 128; wd += blockDim.x / 32) {
+    const int y = wd / 2, x = (wd % 2) * 32 + lane;
+    bool on = false;
+    if (x < cw && y < ch) {
+      on = (x == sx && y == sy) || (x == gx && y == gy);
+      for (int dy = -dilate; dy <= dilate && !on; ++dy) {
+        const int yy = y + dy;
+        if (yy < 0 || yy >= ch) continue;
+        for (int dx = -dilate; dx <= dilate; ++dx) {
+          const int xx = x + dx;
+          if (xx >= 0 && xx < cw && hot[yy * kGrid + xx]) {
+            on = true;
+            break;
+          }
+        }
+      }
+    }
+    const uint32_t word = __ballot_sync(0xFFFFFFFFu, on);
+    if (lane == 0) bits[static_cast<size_t>(n) * 128 + wd] = word;
+  }
+}
+
+template <int CIN, int EPI>
+cudaError_t launch_conv(const ConvArgs& a, int sm_count, cudaStream_t stream) {
+  const int bytes = ConvSmem<CIN>::kBytes;
+  cudaError_t e = cudaFuncSetAttribute(conv3x3_tc_kernel<CIN, EPI>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  const uint32_t items = a.count * (kGrid / 2);
+  const uint32_t grid = min(items, static_cast<uint32_t>(max(sm_count, 1) * 2));
+  if (grid == 0) return cudaSuccess;
+  conv3x3_tc_kernel<CIN, EPI><<<grid, 128, bytes, stream>>>(a);
+  return cudaGetLastError();
+}
+
+template <int CIN>
+cudaError_t launch_wgrad(const WgradArgs& a, int sm_count, cudaStream_t stream) {
+  const int bytes = WgradSmem<CIN>::kBytes;
+  cudaError_t e = cudaFuncSetAttribute(conv_wgrad_tc_kernel<CIN>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if (e != cudaSuccess) return e;
+  const uint32_t items = a.count * (kGrid / 2);
+  const uint32_t grid = min(items, static_cast<uint32_t>(max(sm_count, 1) * 2));
+  if (grid == 0) return cudaSuccess;
+  conv_wgrad_tc_kernel<CIN><<<grid, 128, bytes, stream>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace
+
+uint32_t cnn_param_count() { return param_offsets().total; }
+uint32_t cnn_operand_count() { return operand_offsets().total; }
+
+cudaError_t launch_rasters(const LatticeDeviceView& lat, const apgar_b200_lattice_net* nets,
+                           uint32_t count, const uint32_t* cell_cost, void* rasters, uint32_t* dims,
+                           cudaStream_t stream) {
+  if (count == 0) return cudaSuccess;
+  raster_kernel<<<count, 256, 0, stream>>>(lat, nets, count, cell_cost,
+                                           static_cast<__nv_bfloat16*>(rasters), dims);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_labels(const apgar_b200_lattice_net* nets, uint32_t count, const uint32_t* dims,
+                          int lat_w, int lat_h, const apgar_b200_lattice_result* results,
+                          const uint32_t* paths, uint8_t* labels, cudaStream_t stream) {
+  if (count == 0) return cudaSuccess;
+  labels_kernel<<<count, 256, 0, stream>>>(nets, count, dims, lat_w, lat_h, results, paths, labels);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prepare(const float* params, void* operands, cudaStream_t stream) {
+  prepare_kernel<<<64, 256, 0, stream>>>(params, static_cast<__nv_bfloat16*>(operands));
+  return cudaGetLastError();
+}
+
+// Forward: rasters -> acts[0..4] -> logits.  acts[l] may alias acts[l - 2].
+cudaError_t launch_forward(const float* params, const void* operands, const void* rasters,
+                           const uint32_t* dims, uint32_t count, void* const acts[5], float* logits,
+                           uint32_t* error, int sm_count, cudaStream_t stream) {
+  constexpr ParamOffsets P = param_offsets();
+  constexpr OperandOffsets O = operand_offsets();
+  const auto* ops = static_cast<const __nv_bfloat16*>(operands);
+  for (int l = 0; l < 5; ++l) {
+    ConvArgs a{};
+    a.x = static_cast<const __nv_bfloat16*>(l == 0 ? rasters : acts[l - 1]);
+    a.w = ops + O.wf[l];
+    a.bias = params + P.b[l];
+    a.y = static_cast<__nv_bfloat16*>(acts[l]);
+    a.dims = dims;
+    a.count = count;
+    a.error = error;
+    const cudaError_t e = l == 0 ? launch_conv<kCin0, kEpiRelu>(a, sm_count, stream)
+                                 : launch_conv<kCh, kEpiRelu>(a, sm_count, stream);
+    if (e != cudaSuccess) return e;
+  }
+  const uint32_t blocks = min(static_cast<uint32_t>(max(sm_count, 1) * 8),
+                              static_cast<uint32_t>((static_cast<size_t>(count) * kCells + 255) / 256));
+  if (blocks == 0) return cudaSuccess;
+  head_forward_kernel<<<blocks, 256, 0, stream>>>(static_cast<const __nv_bfloat16*>(acts[4]),
+                                                  params + P.w6, params + P.b6, dims, count, logits);
+  return cudaGetLastError();
+}
+
+// Backward from the logits of a forward pass with five distinct act buffers.
+// grads (FP32, same layout as params) must be zero on entry; scratch holds two
+// gradient tensors of [count][64][64][32] bf16.
+cudaError_t launch_backward(const float* params, const void* operands, const void* rasters,
+                            const uint32_t* dims, uint32_t count, void* const acts[5],
+                            const float* logits, const uint8_t* labels, float pos_weight,
+                            float* dlogit, void* scratch0, void* scratch1, float* grads, float* loss,
+                            uint32_t* error, int sm_count, cudaStream_t stream) {
+  constexpr ParamOffsets P = param_offsets();
+  constexpr OperandOffsets O = operand_offsets();
+  if (count == 0) return cudaSuccess;
+  const auto* ops = static_cast<const __nv_bfloat16*>(operands);
+  const uint32_t blocks = min(static_cast<uint32_t>(max(sm_count, 1) * 8),
+                              static_cast<uint32_t>((static_cast<size_t>(count) * kCells + 255) / 256));
+  loss_kernel<<<blocks, 256, 0, stream>>>(logits, labels, dims, count, pos_weight, dlogit, loss);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  void* g[2] = {scratch0, scratch1};
+  head_backward_kernel<<<blocks, 256, 0, stream>>>(static_cast<const __nv_bfloat16*>(acts[4]),
+                                                   params + P.w6, dlogit, dims, count,
+                                                   static_cast<__nv_bfloat16*>(g[0]), grads + P.w6,
+                                                   grads + P.b6);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  // g[cur] = gradient at layer l's pre-activation
+  int cur = 0;
+  for (int l = 4; l >= 0; --l) {
+    WgradArgs wa{};
+    wa.x = static_cast<const __nv_bfloat16*>(l == 0 ? rasters : acts[l - 1]);
+    wa.dy = static_cast<const __nv_bfloat16*>(g[cur]);
+    wa.dims = dims;
+    wa.count = count;
+    wa.dw = grads + P.w[l];
+    wa.db = grads + P.b[l];
+    wa.error = error;
+    e = l == 0 ? launch_wgrad<kCin0>(wa, sm_count, stream) : launch_wgrad<kCh>(wa, sm_count, stream);
+    if (e != cudaSuccess) return e;
+    if (l == 0) break;
+    ConvArgs a{};
+    a.x = static_cast<const __nv_bfloat16*>(g[cur]);
+    a.w = ops + O.wb[l];
+    a.gate = static_cast<const __nv_bfloat16*>(acts[l - 1]);
+    a.y = static_cast<__nv_bfloat16*>(g[cur ^ 1]);
+    a.dims = dims;
+    a.count = count;
+    a.error = error;
+    e = launch_conv<kCh, kEpiGate>(a, sm_count, stream);
+    if (e != cudaSuccess) return e;
+    cur ^= 1;
+  }
+  return cudaSuccess;
+}
+
+cudaError_t launch_adam(float* params, const float* grads, float* m, float* v, uint32_t step,
+                        float lr, float beta1, float beta2, float eps, cudaStream_t stream) {
+  const uint32_t n = param_offsets().total;
+  const float c1 = 1.f - powf(beta1, static_cast<float>(step));
+  const float c2 = 1.f - powf(beta2, static_cast<float>(step));
+  adam_kernel<<<(n + 255) / 256, 256, 0, stream>>>(params, grads, m, v, n, lr, beta1, beta2, eps, c1, c2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_corridors(const float* logits, const uint32_t* dims,
+                             const apgar_b200_lattice_net* nets, uint32_t count, float threshold,
+                             int dilate, uint32_t* bits, cudaStream_t stream) {
+  if (count == 0) return cudaSuccess;
+  corridor_kernel<<<count, 256, 0, stream>>>(logits, dims, nets, count, threshold, dilate, bits);
+  return cudaGetLastError();
+}
+
+}  // namespace apgar_b200

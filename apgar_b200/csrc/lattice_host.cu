@@ -41,6 +41,15 @@ cudaError_t launch_mark_dirty(const apgar_b200_lattice_result* results, uint32_t
 cudaError_t launch_lattice_pack(apgar_b200_lattice_result* results, uint32_t count,
                                 unsigned long long* total, const uint32_t* arena, uint32_t* paths,
                                 int sm_count, cudaStream_t stream);
+cudaError_t launch_rasters(const LatticeDeviceView& lat, const apgar_b200_lattice_net* nets,
+                           uint32_t count, const uint32_t* cell_cost, void* rasters, uint32_t* dims,
+                           cudaStream_t stream);
+cudaError_t launch_labels(const apgar_b200_lattice_net* nets, uint32_t count, const uint32_t* dims,
+                          int lat_w, int lat_h, const apgar_b200_lattice_result* results,
+                          const uint32_t* paths, uint8_t* labels, cudaStream_t stream);
+cudaError_t launch_corridors(const float* logits, const uint32_t* dims,
+                             const apgar_b200_lattice_net* nets, uint32_t count, float threshold,
+                             int dilate, uint32_t* bits, cudaStream_t stream);
 
 namespace {
 
@@ -694,6 +703,49 @@ extern "C" int apgar_b200_lattice_plan_corridor_status(void* plan, uint8_t* out)
     APGAR_B200_CUDA("cudaMemcpy(corridor status)",
                     cudaMemcpy(out, p->corridor_status.get(), p->count, cudaMemcpyDeviceToHost));
   }
+  clear_error();
+  return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_corridor_rasters(void* plan, const uint32_t* cell_costs, void* rasters,
+                                           uint32_t* dims, void* stream) {
+  if (plan == nullptr || rasters == nullptr || dims == nullptr) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "corridor rasters received a null argument");
+  }
+  auto* p = static_cast<PlanObject*>(plan);
+  if (int rc = check_device(p->device); rc != APGAR_B200_OK) return rc;
+  APGAR_B200_CUDA("raster launch", launch_rasters(p->lattice->view, p->nets.get(), p->count, cell_costs,
+                                                  rasters, dims, static_cast<cudaStream_t>(stream)));
+  clear_error();
+  return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_corridor_labels(void* plan, const uint32_t* dims, uint8_t* labels,
+                                          void* stream) {
+  if (plan == nullptr || dims == nullptr || labels == nullptr) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "corridor labels received a null argument");
+  }
+  auto* p = static_cast<PlanObject*>(plan);
+  if (int rc = check_device(p->device); rc != APGAR_B200_OK) return rc;
+  const LatticeDeviceView& v = p->lattice->view;
+  APGAR_B200_CUDA("label launch", launch_labels(p->nets.get(), p->count, dims, v.width, v.height,
+                                                p->results.get(), p->paths.get(), labels,
+                                                static_cast<cudaStream_t>(stream)));
+  clear_error();
+  return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_corridor_from_logits(void* plan, const float* logits, const uint32_t* dims,
+                                               float threshold, int32_t dilate, uint32_t* bits,
+                                               void* stream) {
+  if (plan == nullptr || logits == nullptr || dims == nullptr || bits == nullptr || dilate < 0 ||
+      dilate > 64) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "corridor extraction received a bad argument");
+  }
+  auto* p = static_cast<PlanObject*>(plan);
+  if (int rc = check_device(p->device); rc != APGAR_B200_OK) return rc;
+  APGAR_B200_CUDA("corridor launch", launch_corridors(logits, dims, p->nets.get(), p->count, threshold,
+                                                      dilate, bits, static_cast<cudaStream_t>(stream)));
   clear_error();
   return APGAR_B200_OK;
 }

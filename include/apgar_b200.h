@@ -465,6 +465,59 @@ APGAR_B200_API int apgar_b200_lattice_route_ex(void* lattice, const apgar_b200_l
                                 uint64_t path_capacity, uint64_t* path_total);
 APGAR_B200_API int apgar_b200_lattice_plan_release(void* plan);
 
+/* ===================== E. learned corridor (CNN) =====================
+ * No reference counterpart.  A 6-layer 3x3 CNN (layers 1-5: 16 -> 32 -> ... ->
+ * 32 channels, bias, ReLU, bf16 weights and activations, f32 accumulation on
+ * the tensor cores; layer 6: 32 -> 1 logit, f32) over each net's 64 x 64
+ * coarse raster (the corridor bitmap's grid).  Raster channels: 0 blocked
+ * fraction over all layers, 1 fraction blocked on every layer, 2 congestion
+ * (mean entry price / 1024, capped at 8; 0 without prices), 3 start, 4 goal,
+ * 5 inside the window, 6-9 coarse offsets to start and goal / 32, 10 distance
+ * to the start-goal segment / 8 (capped at 4), 11-15 zero.
+ * Tensors are device memory: rasters bf16 [count][64][64][16]; activations
+ * bf16 [count][64][64][32]; logits and dlogit f32 [count][64][64]; labels u8
+ * [count][64][64]; dims u32 [count] (coarse width | height << 8 | scale << 16).
+ * params f32 [apgar_b200_cnn_param_count()]: per layer l w[32][9][cin_l] then
+ * b[32], then the head w6[9][32] and b6 (tap = (dy + 1) * 3 + dx + 1);
+ * operands bf16 [apgar_b200_cnn_operand_count()] (apgar_b200_cnn_prepare). */
+enum { APGAR_B200_CNN_TIMEOUT = 1u }; /* a tensor-core completion wait ran out */
+APGAR_B200_API uint32_t apgar_b200_cnn_param_count(void);
+APGAR_B200_API uint32_t apgar_b200_cnn_operand_count(void);
+/* Coarse rasters and dims of every net of a FRONTIER plan; `cell_costs` is
+ * the plan's optional price array (device, [layers][height][width]) or NULL. */
+APGAR_B200_API int apgar_b200_corridor_rasters(void* plan, const uint32_t* cell_costs, void* rasters,
+                                uint32_t* dims, void* stream);
+/* Coarse labels (1 where the net's path of the plan's last execution has a
+ * cell) for training. */
+APGAR_B200_API int apgar_b200_corridor_labels(void* plan, const uint32_t* dims, uint8_t* labels,
+                               void* stream);
+/* The plan's corridor bitmaps (128 words per net) from logits: coarse cells
+ * with logit > threshold, dilated by `dilate` coarse cells, plus both
+ * terminals. */
+APGAR_B200_API int apgar_b200_corridor_from_logits(void* plan, const float* logits, const uint32_t* dims,
+                                    float threshold, int32_t dilate, uint32_t* bits, void* stream);
+/* bf16 operand layouts of the current params (after every update). */
+APGAR_B200_API int apgar_b200_cnn_prepare(const float* params, void* operands, void* stream);
+/* Forward pass; acts holds five activation buffers (they may alternate
+ * between two for inference).  `error` receives APGAR_B200_CNN_* bits. */
+APGAR_B200_API int apgar_b200_cnn_forward(const float* params, const void* operands, const void* rasters,
+                           const uint32_t* dims, uint32_t count, void* const acts[5], float* logits,
+                           uint32_t* error, void* stream);
+/* Backward pass of the weighted cross-entropy (positives weighted by
+ * pos_weight, mean over each net's window cells, then over nets) after a
+ * forward pass with five distinct activation buffers.  Overwrites grads
+ * (f32, params layout) and adds the loss to *loss (device f32).  scratch0 and
+ * scratch1 are activation-sized; dlogit is logits-sized. */
+APGAR_B200_API int apgar_b200_cnn_backward(const float* params, const void* operands, const void* rasters,
+                            const uint32_t* dims, uint32_t count, void* const acts[5],
+                            const float* logits, const uint8_t* labels, float pos_weight,
+                            float* dlogit, void* scratch0, void* scratch1, float* grads,
+                            float* loss, uint32_t* error, void* stream);
+/* One Adam step (step counts from 1) on params with f32 moments m and v. */
+APGAR_B200_API int apgar_b200_cnn_adam(float* params, const float* grads, float* m, float* v,
+                        uint32_t step, float lr, float beta1, float beta2, float eps,
+                        void* stream);
+
 /* ======================= C. congestion prices ======================= */
 
 /* Integer negotiated-congestion price schedule.  Combines the allocator epoch

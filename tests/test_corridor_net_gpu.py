@@ -1,0 +1,169 @@
+"""GPU corridor CNN against its numpy restatement (oracle/corridor_net.py),
+layer by layer, through the C ABI; training and what it gains.
+
+Tolerances (floating point, f32 accumulation in a different order than
+numpy): bf16 activations within one bf16 ulp (relative 2^-7) for at least
+99.9% of the elements; f32 logits and head gradients within 1e-4 relative;
+weight gradients within 1% relative Frobenius error (bf16 rounding of the
+propagated gradients differs by an ulp at some elements)."""
+
+import numpy as np
+import pytest
+import torch
+
+import apgar_b200
+import oracle
+from apgar_b200 import corridor, learned, synth
+from oracle import corridor_net as ref
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf16_to_np(t):
+    return ref.from_bf16_bits(t.view(torch.int16).cpu().numpy().view(np.uint16))
+
+
+def _u32(t):
+    return t.view(torch.int32).cpu().numpy().view(np.uint32)
+
+
+def _close_bf16(gpu, cpu, frac=0.999):
+    ok = np.isclose(gpu, cpu, rtol=2.0 ** -7, atol=1e-6)
+    assert ok.mean() >= frac, (ok.mean(), np.abs(gpu - cpu).max())
+
+
+def _setup(seed=31, count=12):
+    lat = synth.make_lattice(seed, 2, 640, 0.2, via_mask=True)
+    nets = synth.make_nets(lat, seed + 1, count, hpwl_median=120.0, hpwl_sigma=1.0, margin=32)
+    dev = apgar_b200.DeviceLattice(lat)
+    plan = dev.plan(nets, generator="frontier")
+    return lat, nets, dev, plan
+
+
+def test_rasters_match_restatement():
+    lat, nets, dev, plan = _setup()
+    try:
+        r, d = learned.rasters(plan)
+        r = _bf16_to_np(r).reshape(len(nets), 64, 64, 16)
+        d = _u32(d)
+        for i in range(len(nets)):
+            s, cw, ch = corridor.coarse_dims(nets["win_w"][i], nets["win_h"][i])
+            assert d[i] == cw | (ch << 8) | (s << 16)
+            want = _raster_cpu(lat, nets[i], s, cw, ch)
+            assert np.allclose(r[i], ref.bf16(want), rtol=2.0 ** -7, atol=1e-6), i
+    finally:
+        plan.close()
+        dev.close()
+
+
+def _raster_cpu(lat, net, s, cw, ch):
+    free = oracle._window_free(lat, net)  # [L][h][w]
+    out = np.zeros((64, 64, 16), np.float32)
+    x0, y0 = int(net["win_x0"]), int(net["win_y0"])
+    sc = ((int(net["start_x"]) - x0) >> s, (int(net["start_y"]) - y0) >> s)
+    gc = ((int(net["goal_x"]) - x0) >> s, (int(net["goal_y"]) - y0) >> s)
+    sg = np.array([gc[0] - sc[0], gc[1] - sc[1]], np.float32)
+    for cy in range(ch):
+        for cx in range(cw):
+            blk = ~free[:, cy << s:(cy + 1) << s, cx << s:(cx + 1) << s]
+            v = out[cy, cx]
+            v[0] = blk.mean()
+            v[1] = blk.all(axis=0).mean()
+            v[3] = float((cx, cy) == sc)
+            v[4] = float((cx, cy) == gc)
+            v[5] = 1.0
+            v[6:10] = [(cx - sc[0]) / 32, (cy - sc[1]) / 32, (cx - gc[0]) / 32, (cy - gc[1]) / 32]
+            seg2 = float(sg @ sg)
+            t = 0.0 if seg2 == 0 else min(max(((cx - sc[0]) * sg[0] + (cy - sc[1]) * sg[1]) / seg2, 0.0), 1.0)
+            e = np.array([cx - (sc[0] + t * sg[0]), cy - (sc[1] + t * sg[1])])
+            v[10] = min(np.sqrt(e @ e) / 8.0, 4.0)
+    return out
+
+
+def test_forward_and_backward_match_the_oracle():
+    lat, nets, dev, plan = _setup()
+    try:
+        net = learned.CorridorNet(seed=5)
+        r, d = learned.rasters(plan)
+        acts = net.activations(len(nets), distinct=True)
+        logits = net.forward(r, d, acts=acts)
+        plan.execute()
+        lab = learned.labels(plan, d)
+        loss = net.backward(r, d, acts, logits, lab, pos_weight=8.0)
+        torch.cuda.synchronize()
+        net.check_error()
+
+        params = net.params.cpu().numpy()
+        dims = _u32(d)
+        mask = ref.valid_mask(dims)
+        x = [_bf16_to_np(r).reshape(-1, 64, 64, 16)] + \
+            [_bf16_to_np(a).reshape(-1, 64, 64, 32) for a in acts]
+        for layer in range(5):
+            want = ref.conv_layer(x[layer], params, layer, mask)
+            got = np.where(mask[..., None], x[layer + 1], 0.0)
+            _close_bf16(got, want)
+        z = logits.cpu().numpy()
+        zw = ref.head(x[5], params, mask)
+        assert np.allclose(np.where(mask, z, 0), zw, rtol=1e-4, atol=1e-4)
+
+        labels = lab.cpu().numpy()
+        assert labels.sum() > 0
+        lw, dlogit = ref.loss_grad(z, labels, mask, 8.0)
+        assert abs(loss.item() - lw) <= 1e-4 * max(1.0, abs(lw))
+        grads = ref.unflatten(net.grads.cpu().numpy())
+        dpre, dw6, db6 = ref.head_backward(x[5], params, dlogit, mask)
+        assert np.allclose(grads["w6"], dw6, rtol=1e-3, atol=1e-6)
+        assert np.allclose(grads["b6"], db6, rtol=1e-3, atol=1e-6)
+        for layer in range(4, -1, -1):
+            dw, db = ref.weight_grad(x[layer], dpre, mask)
+            for got, want in ((grads[f"w{layer}"], dw), (grads[f"b{layer}"], db)):
+                err = np.linalg.norm(got - want) / max(np.linalg.norm(want), 1e-12)
+                assert err < 1e-2, (layer, err)
+            if layer > 0:
+                dpre = ref.input_grad(dpre, params, layer, x[layer], mask)
+    finally:
+        plan.close()
+        dev.close()
+
+
+def _training_set(seed, count, size=1024):
+    lat = synth.make_lattice(seed, 4, size, 0.25, pads=True)
+    nets = synth.make_nets(lat, seed + 1, count, hpwl_median=120.0, hpwl_sigma=0.8, margin=32)
+    return lat, nets
+
+
+def test_training_lowers_the_loss_and_certifies_more_nets():
+    lat, nets = _training_set(41, 1024)
+    lat_h, nets_h = _training_set(43, 256)
+    dev = apgar_b200.DeviceLattice(lat)
+    dev_h = apgar_b200.DeviceLattice(lat_h)
+    try:
+        sweep = dev.plan(nets, generator="sweep")  # optimal paths from the plain sweep
+        sweep.execute()
+        r, d = learned.rasters(sweep)
+        lab = learned.labels(sweep, d)
+        net = learned.CorridorNet(seed=7)
+        acts = net.activations(len(nets), distinct=True)
+        losses = [net.train_step(r, d, lab, lr=3e-3, acts=acts).item() for _ in range(150)]
+        net.check_error()
+        assert losses[-1] < 0.5 * losses[0], (losses[0], losses[-1])
+
+        plan = dev_h.plan(nets_h, generator="frontier")
+        rh, dh = learned.rasters(plan)
+        cost_o, _ = oracle.dijkstra_batch(lat_h, nets_h)
+
+        def certified(model):
+            bits = learned.corridors(plan, model.forward(rh, dh), dh, threshold=0.0, dilate=1)
+            plan.set_corridors(bits)
+            plan.execute()
+            res, _ = plan.readback(want_paths=False)
+            assert np.array_equal(res["cost"], cost_o)  # results never depend on the corridor
+            return (plan.corridor_status() == corridor.CERTIFIED).mean()
+
+        trained, untrained = certified(net), certified(learned.CorridorNet(seed=7))
+        assert trained > untrained + 0.2, (trained, untrained)
+        plan.close()
+        sweep.close()
+    finally:
+        dev.close()
+        dev_h.close()
