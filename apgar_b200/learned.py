@@ -146,13 +146,17 @@ class CorridorNet:
         return loss
 
 
-def rasters(plan, cell_costs=None, stream: int = 0):
-    """(rasters bf16 [n][64][64][16], dims uint32 [n]) of every net of a plan."""
+def rasters(plan, cell_costs=None, stream: int = 0, out=None):
+    """(rasters bf16 [n][64][64][16], dims uint32 [n]) of every net of a plan
+    (into `out` = (rasters, dims) when given)."""
     import torch
 
     n = len(plan.nets)
-    r = torch.empty((n, GRID, GRID, RASTER_CHANNELS), dtype=torch.bfloat16, device="cuda")
-    d = torch.empty(n, dtype=torch.uint32, device="cuda")
+    if out is not None:
+        r, d = out
+    else:
+        r = torch.empty((n, GRID, GRID, RASTER_CHANNELS), dtype=torch.bfloat16, device="cuda")
+        d = torch.empty(n, dtype=torch.uint32, device="cuda")
     costs = None if cell_costs is None else _ptr(cell_costs)
     _check(lib().apgar_b200_corridor_rasters(plan.handle, costs, _ptr(r), _ptr(d), ctypes.c_void_p(stream)))
     return r, d
@@ -178,3 +182,45 @@ def corridors(plan, logits, dims, threshold: float = 0.0, dilate: int = 1, out=N
                                                  ctypes.c_float(threshold), ctypes.c_int32(dilate),
                                                  _ptr(out), ctypes.c_void_p(stream)))
     return out
+
+
+POLICY_PATH = os.path.join(os.path.dirname(WEIGHTS_PATH), "corridor_policy.json")
+
+
+def load_policy(path: str = POLICY_PATH) -> dict:
+    """The corridor policy chosen at training time: logit threshold, dilation."""
+    import json
+
+    with open(path) as f:
+        return json.load(f)
+
+
+class LearnedRouter:
+    """The learned + persistent batched form on one frontier plan: per
+    execution, rasters -> CNN -> corridors -> corridor-mode frontier search,
+    all on one stream with buffers allocated once."""
+
+    def __init__(self, plan, net: CorridorNet | None = None, policy: dict | None = None):
+        import torch
+
+        self.plan = plan
+        self.net = net if net is not None else CorridorNet.load()
+        self.policy = policy if policy is not None else load_policy()
+        n = len(plan.nets)
+        self.rasters = torch.empty((n, GRID, GRID, RASTER_CHANNELS), dtype=torch.bfloat16,
+                                   device="cuda")
+        self.dims = torch.empty(n, dtype=torch.uint32, device="cuda")
+        self.acts = self.net.activations(n, distinct=False)
+        self.logits = torch.empty((n, GRID, GRID), dtype=torch.float32, device="cuda")
+        self.bits = torch.empty((n, 128), dtype=torch.uint32, device="cuda")
+        plan.set_corridors(self.bits)
+
+    def propose(self, stream: int = 0) -> None:
+        rasters(self.plan, stream=stream, out=(self.rasters, self.dims))
+        self.net.forward(self.rasters, self.dims, acts=self.acts, logits=self.logits, stream=stream)
+        corridors(self.plan, self.logits, self.dims, threshold=float(self.policy["threshold"]),
+                  dilate=int(self.policy["dilate"]), out=self.bits, stream=stream)
+
+    def execute(self, stream: int = 0) -> None:
+        self.propose(stream)
+        self.plan.execute(stream)

@@ -12,7 +12,9 @@ cell the canonical reverse path needs, plus that path, for every net.  A net is
 certified when its search converged (reached or proved disconnected inside its
 window).  The headline form is the persistent work-stealing frontier search
 (bucketed A*); the plain batched sweep is measured beside it on the same nets
-and reported under "plain_sweep", with the ratio of the two.
+and reported under "plain_sweep", with the ratio of the two, and so is the
+learned form (CNN corridors with the exact certificate and full-window
+fallback, trained weights under apgar_b200/weights) under "learned_corridor".
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
@@ -57,6 +59,8 @@ def parse_args():
     ap.add_argument("--ref-sample", type=int, default=512,
                     help="nets per step of the reference arm")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the learned-corridor form (reported beside the headline)")
     ap.add_argument("--workload", choices=["medium", "negotiated"], default="medium",
                     help="medium: the headline batch; negotiated: 10 rip-up/reroute rounds "
                          "on the 6 x 4096^2 lattice with multi-terminal nets (one CUDA graph)")
@@ -381,6 +385,49 @@ def main():
     same = bool(np.array_equal(front["results"]["cost"], sweep["results"]["cost"]) and
                 np.array_equal(front["results"]["completion"], sweep["results"]["completion"]))
 
+    # -------- learned corridor + persistent batched form (same nets) --------
+    learned_form = None
+    if not args.no_learned:
+        from apgar_b200 import learned
+
+        lplan = dev.plan(nets, generator="frontier")
+        router = learned.LearnedRouter(lplan)
+        for _ in range(max(args.warmup, 3)):
+            router.execute(stream.cuda_stream)
+        barrier()
+        l_start = torch.cuda.Event(enable_timing=True)
+        l_mid = torch.cuda.Event(enable_timing=True)
+        l_end = torch.cuda.Event(enable_timing=True)
+        l_start.record(stream)
+        for _ in range(args.steps):
+            router.execute(stream.cuda_stream)
+        l_end.record(stream)
+        barrier()
+        l_ms = max_over_ranks(l_start.elapsed_time(l_end))
+        # the proposal alone (rasters, CNN, corridor extraction)
+        l_start.record(stream)
+        for _ in range(args.steps):
+            router.propose(stream.cuda_stream)
+        l_mid.record(stream)
+        barrier()
+        p_ms = max_over_ranks(l_start.elapsed_time(l_mid))
+        router.net.check_error()
+        l_res, _ = lplan.readback(want_paths=False)
+        status = lplan.corridor_status()
+        l_cert = sum_over_ranks(certified(l_res))
+        learned_form = {
+            "value": l_cert * args.steps / (l_ms / 1000.0), "unit": UNIT,
+            "ms_per_step": l_ms / args.steps, "proposal_ms_per_step": p_ms / args.steps,
+            "corridor_certified": float((status == 1).mean()),
+            "fallback_exit": float((status == 2).mean()),
+            "fallback_unreached": float((status == 3).mean()),
+            "same_costs_as_frontier": bool(np.array_equal(l_res["cost"], front["results"]["cost"])),
+            "policy": router.policy,
+            "form": "6-layer 3x3 CNN (tcgen05, bf16/f32) corridors + certified corridor frontier, "
+                    "full-window fallback in the same kernel",
+        }
+        lplan.close()
+
     # ---------------- end to end through the public API (e2e) ----------------
     info = front["info"]
     pinned_nets = torch.from_numpy(nets.view(np.uint8)).pin_memory()
@@ -452,6 +499,9 @@ def main():
                 "sweeps_mean": float(sweep["results"]["sweeps"].mean()),
             },
         }
+        if learned_form is not None:
+            learned_form["learned_over_sweep"] = learned_form["value"] / sweep_value
+            line["learned_corridor"] = learned_form
         if not args.no_cpu_baseline and world == 1:
             line["cpu_baseline"], cpu_costs = cpu_baseline(lat, nets, args.cpu_sample)
             ok = results["completion"][: args.cpu_sample] != apgar_b200.COMPLETION_REJECTED
