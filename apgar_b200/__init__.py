@@ -67,14 +67,14 @@ class LatticeOptions(ctypes.Structure):
         ("generator", ctypes.c_uint32),
         ("max_iterations", ctypes.c_uint32),
         ("bucket_width", ctypes.c_uint32),
-        ("reserved", ctypes.c_uint32),
+        ("chain", ctypes.c_uint32),
     ]
 
 
-def _options(generator: str, max_iterations: int, bucket_width: int) -> LatticeOptions:
+def _options(generator: str, max_iterations: int, bucket_width: int, chain: int = 0) -> LatticeOptions:
     if generator not in GENERATORS:
         raise BackendError(1, f"unknown lattice generator {generator!r}")
-    return LatticeOptions(GENERATORS[generator], max_iterations, bucket_width, 0)
+    return LatticeOptions(GENERATORS[generator], max_iterations, bucket_width, chain)
 
 
 class PlanInfo(ctypes.Structure):
@@ -182,13 +182,16 @@ class DeviceLattice:
 
     def route(self, nets: np.ndarray, max_sweeps: int = 4096, cancel: np.ndarray | None = None,
               want_paths: bool = True, path_capacity: int | None = None, out=None,
-              generator: str = "sweep", max_rounds: int = 1 << 30, bucket_width: int = 0):
+              generator: str = "sweep", max_rounds: int = 1 << 30, bucket_width: int = 0,
+              chain: int = 0):
         """Searches every net; returns (results record array, packed paths).
 
         ``generator`` is "sweep" (budget ``max_sweeps``) or "frontier"
         (budget ``max_rounds``, key level width ``bucket_width``, 0 = twice
-        the largest move).  ``out`` may supply preallocated (results, paths)
-        host arrays (pinned memory makes the transfers faster)."""
+        the largest move; ``chain``, 0 = the default per width class, n = up
+        to n - 1 chained expansions per queued cell).  ``out`` may supply
+        preallocated (results, paths) host arrays (pinned memory makes the
+        transfers faster)."""
         nets = np.ascontiguousarray(nets)
         count = len(nets)
         if out is not None:
@@ -205,7 +208,7 @@ class DeviceLattice:
                 _vp(cancel), _vp(results), _vp(paths) if want_paths else None,
                 ctypes.c_uint64(paths.size if want_paths else 0), ctypes.byref(total)))
         else:
-            opts = _options(generator, max_rounds, bucket_width)
+            opts = _options(generator, max_rounds, bucket_width, chain)
             _check(lib().apgar_b200_lattice_route_ex(
                 self.handle, _vp(nets), ctypes.c_uint32(count), ctypes.byref(opts),
                 _vp(cancel), _vp(results), _vp(paths) if want_paths else None,
@@ -237,15 +240,16 @@ class DeviceLattice:
         return results, paths[: total.value]
 
     def plan(self, nets: np.ndarray, max_sweeps: int = 4096, generator: str = "sweep",
-             max_rounds: int = 1 << 30, bucket_width: int = 0) -> "Plan":
-        return Plan(self, nets, max_sweeps, generator, max_rounds, bucket_width)
+             max_rounds: int = 1 << 30, bucket_width: int = 0, chain: int = 0) -> "Plan":
+        return Plan(self, nets, max_sweeps, generator, max_rounds, bucket_width, chain)
 
 
 class Plan:
     """A planned batch resident on the device (execute may be graph-captured)."""
 
     def __init__(self, lattice: DeviceLattice, nets: np.ndarray, max_sweeps: int,
-                 generator: str = "sweep", max_rounds: int = 1 << 30, bucket_width: int = 0):
+                 generator: str = "sweep", max_rounds: int = 1 << 30, bucket_width: int = 0,
+                 chain: int = 0):
         self.lattice = lattice
         self.nets = np.ascontiguousarray(nets)
         self.generator = generator
@@ -255,7 +259,7 @@ class Plan:
                                                  ctypes.c_uint32(len(self.nets)),
                                                  ctypes.c_uint32(max_sweeps), ctypes.byref(handle)))
         else:
-            opts = _options(generator, max_rounds, bucket_width)
+            opts = _options(generator, max_rounds, bucket_width, chain)
             _check(lib().apgar_b200_lattice_plan_ex(lattice.handle, _vp(self.nets),
                                                     ctypes.c_uint32(len(self.nets)),
                                                     ctypes.byref(opts), ctypes.byref(handle)))

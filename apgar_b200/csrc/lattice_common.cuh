@@ -34,6 +34,11 @@ struct LatticeDeviceView {
   const uint32_t* sweep_via_cols;  // [layers-1][width][words_t + 2] or nullptr
   int32_t layers, height, width, words, words_t;
   uint32_t orth, diag, via;
+  // Move legality per cell [layers][height][width]: bit d (0-7) = the planar
+  // move in heading d is legal (target free, both side cells free for a
+  // diagonal, target inside the lattice); bit 8 / 9 = the via to the layer
+  // below / above is legal.  Built once at upload (frontier generator).
+  const uint16_t* moves;
 };
 
 // Per-net workspace record produced by the host planner.  The net is swept
@@ -116,6 +121,8 @@ struct FrontierLaunch {
   uint8_t* corridor_status;
   // optional: the class's plan count, read on the device (overrides plan_count)
   const uint32_t* plan_count_dev;
+  // chained expansions after each queued cell within a round (0 = none)
+  uint32_t chain;
 };
 
 __device__ __forceinline__ uint32_t sat(uint32_t v) { return v < kLabelInf ? v : kLabelInf; }

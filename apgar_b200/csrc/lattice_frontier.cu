@@ -71,6 +71,7 @@
 // written in the corridor pass, so only the corridor's blocks are cleared.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "lattice_common.cuh"
@@ -81,6 +82,9 @@ namespace {
 // The cancel flag lives in host-mapped memory: every read crosses the bus, so
 // each group reads it at the start of a net and then every 256 rounds.
 constexpr int kCancelPollRounds = 256;
+
+// No chained expansion follows (a packed cell never has all bits set).
+constexpr uint32_t kNoLink = 0xFFFFFFFFu;
 
 __host__ __device__ constexpr int frontier_groups_per_block(int G) { return G >= 4 ? 1 : 4 / G; }
 
@@ -160,18 +164,12 @@ __device__ __forceinline__ void fsync(int barrier_id) {
   }
 }
 
-// Blocked bits of lattice columns X-1..X+1 (bits 0..2) in a guard-padded
-// sweep-plane row (guard words read as blocked, so X = 0 needs no test).
-__device__ __forceinline__ uint32_t blocked3(const uint32_t* row, int X) {
-  const uint32_t q = static_cast<uint32_t>(X + 31);  // bit X-1, counted from the guard word
-  return __funnelshift_r(__ldg(row + (q >> 5)), __ldg(row + (q >> 5) + 1), q & 31u) & 7u;
-}
-
 // Expands one queued cell.  The memory operations are issued move-parallel in
-// two waves: the cell's label, mask bits and all in-window neighbour labels
-// together, then the 64-bit atomicMins.  Lowered neighbours whose list stamp
-// this call set are flagged in cur_mask (next round's list) or far_mask (far
-// list); ne[d] holds the packed cell.
+// three waves: the cell's label and its precomputed move legality, then the
+// labels of the legal neighbours, then their 64-bit atomicMins.  Lowered
+// neighbours whose list stamp this call set are flagged in cur_mask (next
+// round's list) or far_mask (far list); ne[d] holds the packed cell, and link
+// the least-key cell flagged in cur_mask (kNoLink if none).
 template <bool kPriced, bool kCorr>
 __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const Window& win,
                                             uint32_t e, unsigned long long* words, uint32_t thr,
@@ -179,7 +177,8 @@ __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const 
                                             const uint32_t* cell_cost, const uint32_t* cost_own,
                                             const uint32_t* own, const uint32_t* corr, int cshift,
                                             uint32_t& exit_min, uint32_t (&ne)[10],
-                                            uint32_t& cur_mask, uint32_t& far_mask, bool& overflow) {
+                                            uint32_t& cur_mask, uint32_t& far_mask, bool& overflow,
+                                            uint32_t& link) {
   const int l = static_cast<int>(e >> 28), y = static_cast<int>((e >> 14) & 0x3FFFu),
             x = static_cast<int>(e & 0x3FFFu);
   const uint32_t w = static_cast<uint32_t>(win.w);
@@ -192,19 +191,24 @@ __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const 
                           ((xl && yu) ? 8u : 0u) | (xl ? 16u : 0u) | ((xl && yd) ? 32u : 0u) |
                           (yd ? 64u : 0u) | ((xr && yd) ? 128u : 0u) | (ld ? 256u : 0u) |
                           (lu ? 512u : 0u);
-  // neighbours inside the corridor (a via keeps the cell's column); only
-  // these are read, lowered or priced
+  const int X = win.x0 + x, Y = win.y0 + y;
+  // wave 1: own label and the cell's move legality (one precomputed word)
+  const uint32_t gv = static_cast<uint32_t>(__ldcg(words + here) >> 32);
+  const uint32_t legal =
+      static_cast<uint32_t>(__ldg(lat.moves + (static_cast<size_t>(l) * lat.height + Y) * lat.width + X)) &
+      inside;
+  // legal neighbours inside the corridor (a via keeps the cell's column);
+  // only these are read, lowered or priced
   uint32_t corr_in = 0x3FFu;
   if constexpr (kCorr) {
     corr_in = 0x300u;
 #pragma unroll
     for (int d = 0; d < 8; ++d) {
-      if ((inside & (1u << d)) && corr_has(corr, cshift, x + fdx(d), y + fdy(d))) corr_in |= 1u << d;
+      if ((legal & (1u << d)) && corr_has(corr, cshift, x + fdx(d), y + fdy(d))) corr_in |= 1u << d;
     }
   }
-  const uint32_t reach = inside & corr_in;
-  // wave 1: own label, neighbour labels, mask bits
-  const uint32_t gv = static_cast<uint32_t>(__ldcg(words + here) >> 32);
+  const uint32_t reach = legal & corr_in;
+  // wave 2: the labels of the reachable neighbours
   uint32_t seen[10];
 #pragma unroll
   for (int d = 0; d < 10; ++d) {
@@ -212,7 +216,6 @@ __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const 
                               : (d == 8 ? here - plane : here + plane);
     seen[d] = (reach & (1u << d)) ? static_cast<uint32_t>(__ldcg(words + ni) >> 32) : 0u;
   }
-  const int X = win.x0 + x, Y = win.y0 + y;
   // entry prices of the neighbours (0 without a price snapshot); a cell of
   // the net's own previous path is priced without the net's own use
   uint32_t price[10];
@@ -231,41 +234,23 @@ __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const 
       price[d] = __ldg(src + (static_cast<size_t>(nl) * lat.height + py) * lat.width + px);
     }
   }
-  const size_t stride = static_cast<size_t>(lat.words) + 2;
-  const uint32_t* rowc = lat.sweep_rows + (static_cast<size_t>(l) * lat.height + Y) * stride;
-  const uint32_t edge = (xl ? 1u : 0u) | 2u | (xr ? 4u : 0u);
-  const uint32_t r1 = ~blocked3(rowc, X) & edge;
-  const uint32_t r0 = yd ? ~blocked3(rowc - stride, X) & edge : 0u;
-  const uint32_t r2 = yu ? ~blocked3(rowc + stride, X) & edge : 0u;
-  const size_t layer_stride = static_cast<size_t>(lat.height) * stride;
-  const uint32_t bit = 1u << (X & 31);
-  const uint32_t wi = static_cast<uint32_t>(X >> 5) + 1u;
-  bool down_ok = ld && (__ldg(rowc - layer_stride + wi) & bit) == 0u;
-  bool up_ok = lu && (__ldg(rowc + layer_stride + wi) & bit) == 0u;
-  if (lat.via_ok != nullptr) {
-    // via plane of layer pair (k, k + 1) is plane k
-    const size_t col = static_cast<size_t>(Y) * lat.words + (X >> 5);
-    const size_t via_layer = static_cast<size_t>(lat.height) * lat.words;
-    if (down_ok) down_ok = (__ldg(lat.via_ok + (l - 1) * via_layer + col) & bit) != 0u;
-    if (up_ok) up_ok = (__ldg(lat.via_ok + l * via_layer + col) & bit) != 0u;
-  }
-  uint32_t legal = (down_ok ? 256u : 0u) | (up_ok ? 512u : 0u);
-#pragma unroll
-  for (int d = 0; d < 8; ++d) {
-    const int dx = fdx(d), dy = fdy(d);
-    const uint32_t row = dy < 0 ? r0 : (dy == 0 ? r1 : r2);
-    bool ok = (row >> (1 + dx)) & 1u;
-    if (d & 1) ok = ok && ((r1 >> (1 + dx)) & 1u) && ((row >> 1) & 1u);
-    legal |= ok ? (1u << d) : 0u;
-  }
   // heuristic parts: |column - goal| and |row - goal| for the 3x3 neighbourhood
   const int ax[3] = {abs(x - 1 - win.gx), abs(x - win.gx), abs(x + 1 - win.gx)};
   const int ay[3] = {abs(y - 1 - win.gy), abs(y - win.gy), abs(y + 1 - win.gy)};
   const uint32_t dstep = lat.diag >= lat.orth ? min(lat.diag, 2u * lat.orth) : lat.diag;
-  // wave 2: lower the labels (all atomics issued before any result is used);
+  // wave 3: lower the labels (all atomics issued before any result is used);
   // the low half records the list the cell joins
   uint32_t cand[10], low[10];
   unsigned long long old[10];
+  // key of the neighbour reached by move m at label c
+  const auto key_of = [&](int m, uint32_t c) {
+    const int mx = m < 8 ? fdx(m) : 0, my = m < 8 ? fdy(m) : 0;
+    const int nl = m == 8 ? l - 1 : (m == 9 ? l + 1 : l);
+    const uint32_t a = static_cast<uint32_t>(ax[1 + mx]), b = static_cast<uint32_t>(ay[1 + my]);
+    const uint32_t lo = min(a, b), hi = max(a, b);
+    const uint32_t planar = lat.diag >= lat.orth ? lo * dstep + (hi - lo) * lat.orth : hi * dstep;
+    return c + planar + static_cast<uint32_t>(abs(nl - win.gl)) * lat.via;
+  };
 #pragma unroll
   for (int d = 0; d < 10; ++d) {
     const uint32_t cost = d >= 8 ? lat.via : ((d & 1) ? lat.diag : lat.orth);
@@ -278,21 +263,12 @@ __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const 
       overflow = true;
       continue;
     }
-    // key of the neighbour reached by move d at label cand[d]
-    const auto key_of = [&](int m) {
-      const int mx = m < 8 ? fdx(m) : 0, my = m < 8 ? fdy(m) : 0;
-      const int nl = m == 8 ? l - 1 : (m == 9 ? l + 1 : l);
-      const uint32_t a = static_cast<uint32_t>(ax[1 + mx]), b = static_cast<uint32_t>(ay[1 + my]);
-      const uint32_t lo = min(a, b), hi = max(a, b);
-      const uint32_t planar = lat.diag >= lat.orth ? lo * dstep + (hi - lo) * lat.orth : hi * dstep;
-      return cand[m] + planar + static_cast<uint32_t>(abs(nl - win.gl)) * lat.via;
-    };
     if constexpr (kCorr) {
-      if (legal & ~corr_in & (1u << d)) exit_min = min(exit_min, key_of(d));  // a corridor exit
+      if (legal & ~corr_in & (1u << d)) exit_min = min(exit_min, key_of(d, cand[d]));  // a corridor exit
     }
     if ((legal & (1u << d)) && cand[d] < seen[d]) {
       const int dx = d < 8 ? fdx(d) : 0, dy = d < 8 ? fdy(d) : 0;
-      const uint32_t key = key_of(d);
+      const uint32_t key = key_of(d, cand[d]);
       low[d] = key < thr ? cur_low : far_low;
       const uint32_t ni = d < 8 ? here + static_cast<uint32_t>(dy) * w + static_cast<uint32_t>(dx)
                                 : (d == 8 ? here - plane : here + plane);
@@ -301,6 +277,8 @@ __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const 
   }
   cur_mask = 0;
   far_mask = 0;
+  link = kNoLink;
+  uint32_t link_key = 0xFFFFFFFFu;
 #pragma unroll
   for (int d = 0; d < 10; ++d) {
     // old == 0 marks a move that was not attempted (label 0 is never lowered)
@@ -310,6 +288,13 @@ __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const 
       ne[d] = pack_cell(nl, x + dx, y + dy);
       if (low[d] == cur_low) {
         cur_mask |= 1u << d;
+        // the least-key cell this expansion queued for the next round: the
+        // one a chained expansion follows
+        const uint32_t k = key_of(d, cand[d]);
+        if (k < link_key) {
+          link_key = k;
+          link = ne[d];
+        }
         // its expansion next round reads rows y-1 and y+1 and the adjacent
         // layers: start those lines towards L2 now
         const uint32_t ni = d < 8 ? here + static_cast<uint32_t>(dy) * w + static_cast<uint32_t>(dx)
@@ -560,20 +545,28 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
         const uint32_t far_low = 0xFFFFFFFFu - (0x80000000u | levels);  // far list of this level
         for (uint32_t base = static_cast<uint32_t>(g) * 32u; base < n; base += T) {
           const uint32_t i = base + static_cast<uint32_t>(lane);
-          const bool valid = i < n;
+          bool valid = i < n;
+          uint32_t cell = valid ? cur[i] : 0u;
+          // the queued cell, then up to p.chain chained expansions: each
+          // follows the least-key cell the previous one queued for the next
+          // round (it stays queued, so the lists and the stop rule are
+          // unchanged; the chain only moves labels ahead within the round)
+#pragma unroll 1
+          for (uint32_t step = 0;; ++step) {
           uint32_t cur_mask = 0, far_mask = 0;
           uint32_t ne[10];
+          uint32_t link = kNoLink;
           if (valid) {
             ++expanded;
             bool overflow = false;
             if (kCorr && use_corr) {
-              expand_cell<kPriced, kCorr>(lat, win, cur[i], words, thr, cur_low, far_low,
+              expand_cell<kPriced, kCorr>(lat, win, cell, words, thr, cur_low, far_low,
                                           p.cell_cost, p.cell_cost_own, own, corr, cshift,
-                                          exit_min, ne, cur_mask, far_mask, overflow);
+                                          exit_min, ne, cur_mask, far_mask, overflow, link);
             } else {
-              expand_cell<kPriced, false>(lat, win, cur[i], words, thr, cur_low, far_low,
+              expand_cell<kPriced, false>(lat, win, cell, words, thr, cur_low, far_low,
                                           p.cell_cost, p.cell_cost_own, own, corr, cshift,
-                                          exit_min, ne, cur_mask, far_mask, overflow);
+                                          exit_min, ne, cur_mask, far_mask, overflow, link);
             }
             if (overflow) sh.overflow = 1u;
           }
@@ -615,6 +608,11 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
             }
             if (lost) sh.overflow = 1u;  // a queue list is full: the net is rejected
           }
+          if (step >= p.chain) break;  // uniform
+          valid = valid && link != kNoLink;
+          if (!__any_sync(0xFFFFFFFFu, valid)) break;
+          cell = link;
+          }  // chain
         }
         fsync<G>(barrier_id);
         n = *count;
@@ -796,6 +794,54 @@ cudaError_t launch_frontier_g(const FrontierLaunch& launch, cudaStream_t stream)
 }
 
 }  // namespace
+
+namespace {
+
+__device__ __forceinline__ bool lattice_free(const LatticeDeviceView& lat, int l, int x, int y) {
+  if (l < 0 || l >= lat.layers || x < 0 || y < 0 || x >= lat.width || y >= lat.height) return false;
+  const uint32_t word = lat.blocked[(static_cast<size_t>(l) * lat.height + y) * lat.words + (x >> 5)];
+  return ((word >> (x & 31)) & 1u) == 0u;
+}
+
+// One thread per cell: the move rule of expand_cell, evaluated once.
+__global__ void build_moves_kernel(LatticeDeviceView lat, uint16_t* __restrict__ moves) {
+  const size_t cells = static_cast<size_t>(lat.layers) * lat.height * lat.width;
+  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < cells;
+       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+    const int x = static_cast<int>(i % lat.width);
+    const int y = static_cast<int>((i / lat.width) % lat.height);
+    const int l = static_cast<int>(i / (static_cast<size_t>(lat.width) * lat.height));
+    uint32_t m = 0;
+#pragma unroll
+    for (int d = 0; d < 8; ++d) {
+      const int dx = fdx(d), dy = fdy(d);
+      bool ok = lattice_free(lat, l, x + dx, y + dy);
+      if (ok && (d & 1)) ok = lattice_free(lat, l, x + dx, y) && lattice_free(lat, l, x, y + dy);
+      if (ok) m |= 1u << d;
+    }
+    const size_t col = static_cast<size_t>(y) * lat.words + (x >> 5);
+    const size_t via_layer = static_cast<size_t>(lat.height) * lat.words;
+    if (l > 0 && lattice_free(lat, l - 1, x, y) &&
+        (lat.via_ok == nullptr || ((lat.via_ok[(l - 1) * via_layer + col] >> (x & 31)) & 1u))) {
+      m |= 256u;
+    }
+    if (l + 1 < lat.layers && lattice_free(lat, l + 1, x, y) &&
+        (lat.via_ok == nullptr || ((lat.via_ok[l * via_layer + col] >> (x & 31)) & 1u))) {
+      m |= 512u;
+    }
+    moves[i] = static_cast<uint16_t>(m);
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_build_moves(const LatticeDeviceView& lat, uint16_t* moves, cudaStream_t stream) {
+  const size_t cells = static_cast<size_t>(lat.layers) * lat.height * lat.width;
+  if (cells == 0) return cudaSuccess;
+  const unsigned blocks = static_cast<unsigned>(std::min<size_t>((cells + 255) / 256, 148 * 32));
+  build_moves_kernel<<<blocks, 256, 0, stream>>>(lat, moves);
+  return cudaGetLastError();
+}
 
 cudaError_t lattice_frontier_resident_groups(int warps_per_net, int sm_count, uint32_t* out) {
   switch (warps_per_net) {

@@ -29,6 +29,7 @@ cudaError_t launch_accumulate_cells(const apgar_b200_lattice_result* results, ui
 cudaError_t launch_lattice_frontier(int warps_per_net, const FrontierLaunch& launch, int sm_count,
                                     cudaStream_t stream);
 cudaError_t lattice_frontier_resident_groups(int warps_per_net, int sm_count, uint32_t* out);
+cudaError_t launch_build_moves(const LatticeDeviceView& lat, uint16_t* moves, cudaStream_t stream);
 cudaError_t launch_price_update(uint32_t count, const uint32_t* usage, uint64_t factor,
                                 uint64_t next_factor, uint64_t hist_inc, uint64_t capacity,
                                 uint64_t max_value, uint64_t* present, uint64_t* history,
@@ -75,6 +76,12 @@ struct ClassRange {
   uint64_t lists_offset = 0;
 };
 
+// Chained expansions per queued cell by width class (the default when the
+// plan's options leave it to the class).
+// Measured on the medium batch: the batch is bound by expansion throughput,
+// so the extra expansions of a chain cost more than the rounds it saves.
+uint32_t default_chain(int) { return 0u; }
+
 // Queue entries per list per frontier slot (a net needing more is rejected).
 constexpr uint64_t kMaxListEntries = 1ull << 22;
 // Frontier workspace above which nets share persistent slot slabs instead of
@@ -89,6 +96,7 @@ struct PlanObject {
   uint32_t max_sweeps = 0;  // sweeps (SWEEP) or rounds (FRONTIER)
   uint32_t generator = APGAR_B200_LATTICE_SWEEP;
   uint32_t bucket_width = 0;
+  uint32_t chain = 0;    // FRONTIER: apgar_b200_lattice_options::chain
   bool per_net = false;  // FRONTIER: one slab per net (else persistent slots)
   const uint32_t* cell_cost = nullptr;  // caller-owned device prices (frontier only)
   // partial rip-up (set by a negotiation): kept nets and their previous routes
@@ -145,6 +153,7 @@ struct LatticeObject {
   DeviceBuffer<uint32_t> blocked;
   DeviceBuffer<uint32_t> via_ok;
   DeviceBuffer<uint32_t> sweep_rows, sweep_cols, sweep_via_rows, sweep_via_cols;
+  DeviceBuffer<uint16_t> moves;  // LatticeDeviceView::moves
   std::mutex route_mutex;
   std::unique_ptr<PlanObject> route_plan;  // reusable workspace for route()
 };
@@ -233,7 +242,8 @@ std::vector<uint32_t> sweep_planes(const uint32_t* in, int planes, int height, i
 // Builds (or rebuilds into existing buffers) a plan for `nets`.
 int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint32_t count,
                uint32_t max_sweeps, PlanObject* plan,
-               uint32_t generator = APGAR_B200_LATTICE_SWEEP, uint32_t bucket_width = 0) {
+               uint32_t generator = APGAR_B200_LATTICE_SWEEP, uint32_t bucket_width = 0,
+               uint32_t chain = 0) {
   const LatticeDeviceView& v = lat->view;
   const bool frontier = generator == APGAR_B200_LATTICE_FRONTIER;
   plan->lattice = lat;
@@ -245,6 +255,7 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
   // falls in the next level (the frontier kernel relies on it: a cell that
   // left the far list never returns to it, so its far bit needs no clearing).
   plan->bucket_width = std::max(bucket_width, 2u * std::max(v.orth, std::max(v.diag, v.via)));
+  plan->chain = chain;
   APGAR_B200_CUDA("cudaDeviceGetAttribute",
                   cudaDeviceGetAttribute(&plan->sm_count, cudaDevAttrMultiProcessorCount,
                                          lat->device));
@@ -385,10 +396,18 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
                     cudaMemcpy(plan->plans.get(), plans.data(), plans.size() * sizeof(NetPlan),
                                cudaMemcpyHostToDevice));
   }
+  int least_priority = 0, greatest_priority = 0;
+  APGAR_B200_CUDA("cudaDeviceGetStreamPriorityRange",
+                  cudaDeviceGetStreamPriorityRange(&least_priority, &greatest_priority));
   for (int ci = 0; ci < kClassCount; ++ci) {
     if (plan->class_streams[ci] == nullptr) {
+      // wider classes (higher positions) get higher priority: their blocks
+      // need most of an SM and hold the nets with the most rounds, so they
+      // must not wait behind the narrow classes' persistent grids
+      const int priority = std::max(greatest_priority, least_priority - ci);
       APGAR_B200_CUDA("cudaStreamCreate",
-                      cudaStreamCreateWithFlags(&plan->class_streams[ci], cudaStreamNonBlocking));
+                      cudaStreamCreateWithPriority(&plan->class_streams[ci], cudaStreamNonBlocking,
+                                                   priority));
       APGAR_B200_CUDA("cudaEventCreate",
                       cudaEventCreateWithFlags(&plan->joins[ci], cudaEventDisableTiming));
     }
@@ -452,7 +471,9 @@ int execute_plan(PlanObject* plan, cudaStream_t stream) {
   base.cancel = plan->cancel_dev;
   const bool fan_out = plan->classes.size() > 1;
   if (fan_out) APGAR_B200_CUDA("cudaEventRecord(fork)", cudaEventRecord(plan->fork, stream));
-  for (size_t k = 0; k < plan->classes.size(); ++k) {
+  // widest class first (see the stream priorities above)
+  for (size_t kk = plan->classes.size(); kk-- > 0;) {
+    const size_t k = kk;
     const ClassRange& c = plan->classes[k];
     SweepLaunch launch = base;
     launch.plans = plan->plans.get() + c.begin;
@@ -479,6 +500,7 @@ int execute_plan(PlanObject* plan, cudaStream_t stream) {
         fl.own_bits = plan->own_bits;
       }
       fl.next_plan = reinterpret_cast<unsigned int*>(plan->counters.get() + 2 + k);
+      fl.chain = plan->chain != 0 ? plan->chain - 1 : default_chain(c.warps_per_net);
       APGAR_B200_CUDA("lattice frontier launch",
                       launch_lattice_frontier(c.warps_per_net, fl, plan->sm_count, s));
     } else {
@@ -602,6 +624,12 @@ extern "C" int apgar_b200_lattice_upload(const apgar_b200_lattice_desc* d, void*
     lat->view.orth = d->orth;
     lat->view.diag = d->diag;
     lat->view.via = d->via;
+    // per-cell move legality for the frontier generator
+    const size_t cells = static_cast<size_t>(d->layers) * d->height * d->width;
+    APGAR_B200_CUDA("cudaMalloc(move legality)", lat->moves.ensure(std::max<size_t>(cells, 1)));
+    APGAR_B200_CUDA("move legality launch", launch_build_moves(lat->view, lat->moves.get(), nullptr));
+    APGAR_B200_CUDA("cudaStreamSynchronize(move legality)", cudaStreamSynchronize(nullptr));
+    lat->view.moves = lat->moves.get();
     *out = lat.release();
     clear_error();
     return APGAR_B200_OK;
@@ -784,6 +812,7 @@ int check_options(const apgar_b200_lattice_options& o) {
     if (o.max_iterations == 0 || o.max_iterations > (1u << 30)) {
       return set_error(APGAR_B200_INTERNAL_INVARIANT, "frontier budget must be 1..2^30 rounds");
     }
+    if (o.chain > 16) return set_error(APGAR_B200_INTERNAL_INVARIANT, "frontier chain must be 0..16");
     return APGAR_B200_OK;
   }
   return set_error(APGAR_B200_UNSUPPORTED, "unknown lattice generator");
@@ -803,7 +832,8 @@ int route_impl(void* lattice, const apgar_b200_lattice_net* nets, uint32_t count
     std::scoped_lock lock(lat->route_mutex);
     if (lat->route_plan == nullptr) lat->route_plan = std::make_unique<PlanObject>();
     PlanObject* plan = lat->route_plan.get();
-    if (int rc = build_plan(lat, nets, count, o.max_iterations, plan, o.generator, o.bucket_width);
+    if (int rc = build_plan(lat, nets, count, o.max_iterations, plan, o.generator, o.bucket_width,
+                            o.chain);
         rc != APGAR_B200_OK) {
       return rc;
     }
@@ -864,7 +894,7 @@ extern "C" int apgar_b200_lattice_plan_ex(void* lattice, const apgar_b200_lattic
   try {
     auto plan = std::make_unique<PlanObject>();
     if (int rc = build_plan(lat, nets, count, options->max_iterations, plan.get(),
-                            options->generator, options->bucket_width);
+                            options->generator, options->bucket_width, options->chain);
         rc != APGAR_B200_OK) {
       return rc;
     }

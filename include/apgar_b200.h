@@ -419,7 +419,10 @@ typedef struct apgar_b200_lattice_options {
   uint32_t max_iterations; /* sweeps (SWEEP, 1..30000) or rounds (FRONTIER, 1..2^30) */
   uint32_t bucket_width;   /* FRONTIER: key width of a level; raised to at least twice
                               the largest move cost (0 = that minimum) */
-  uint32_t reserved;
+  uint32_t chain;          /* FRONTIER: 0 = the default per width class; n >= 1 = every
+                              queued cell is followed within its round by up to n - 1
+                              chained expansions of the least-key cell it queued
+                              (1 = none); at most 16.  Results do not depend on it. */
 } apgar_b200_lattice_options;
 
 /* Per-cell entry prices for a FRONTIER plan (no reference counterpart at this

@@ -180,3 +180,16 @@ def test_price_overflow_is_rejected_not_wrong():
     # two entries already pass 2^31: every net with a path of 2+ moves is rejected
     moved = (nets["start_x"][:8] != nets["goal_x"][:8]) | (nets["start_y"][:8] != nets["goal_y"][:8])
     assert (res["completion"][moved] == apgar_b200.COMPLETION_REJECTED).all()
+
+
+@pytest.mark.parametrize("chain", [1, 2, 4, 9, 16])
+def test_chained_expansions_do_not_change_results(chain):
+    # chain n: up to n - 1 chained expansions per queued cell in every class
+    lat, nets = synth.config_medium(10, nets=64, size=640)
+    _assert_parity(lat, nets, chain=chain)
+
+
+def test_chain_above_sixteen_is_refused():
+    lat, nets = synth.config_small(1)
+    with pytest.raises(apgar_b200.BackendError):
+        _route(lat, nets[:4].copy(), chain=17)
