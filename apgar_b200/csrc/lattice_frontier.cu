@@ -170,7 +170,11 @@ __device__ __forceinline__ void fsync(int barrier_id) {
 // neighbours whose list stamp this call set are flagged in cur_mask (next
 // round's list) or far_mask (far list); ne[d] holds the packed cell, and link
 // the least-key cell flagged in cur_mask (kNoLink if none).
-template <bool kPriced, bool kCorr>
+// kSpeculate: the neighbour labels are loaded together with the legality word
+// (one wave less per hop, for the latency-bound wide classes); otherwise only
+// the legal neighbours' labels are loaded (fewer requests, for the
+// throughput-bound narrow classes).
+template <bool kPriced, bool kCorr, bool kSpeculate>
 __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const Window& win,
                                             uint32_t e, unsigned long long* words, uint32_t thr,
                                             uint32_t cur_low, uint32_t far_low,
@@ -194,27 +198,39 @@ __device__ __forceinline__ void expand_cell(const LatticeDeviceView& lat, const 
   const int X = win.x0 + x, Y = win.y0 + y;
   // wave 1: own label and the cell's move legality (one precomputed word)
   const uint32_t gv = static_cast<uint32_t>(__ldcg(words + here) >> 32);
-  const uint32_t legal =
-      static_cast<uint32_t>(__ldg(lat.moves + (static_cast<size_t>(l) * lat.height + Y) * lat.width + X)) &
-      inside;
-  // legal neighbours inside the corridor (a via keeps the cell's column);
-  // only these are read, lowered or priced
+  const uint16_t* mv_at = lat.moves + (static_cast<size_t>(l) * lat.height + Y) * lat.width + X;
+  // neighbours inside the corridor (a via keeps the cell's column); only
+  // these are read, lowered or priced
   uint32_t corr_in = 0x3FFu;
   if constexpr (kCorr) {
     corr_in = 0x300u;
 #pragma unroll
     for (int d = 0; d < 8; ++d) {
-      if ((legal & (1u << d)) && corr_has(corr, cshift, x + fdx(d), y + fdy(d))) corr_in |= 1u << d;
+      if ((inside & (1u << d)) && corr_has(corr, cshift, x + fdx(d), y + fdy(d))) corr_in |= 1u << d;
     }
   }
-  const uint32_t reach = legal & corr_in;
-  // wave 2: the labels of the reachable neighbours
   uint32_t seen[10];
+  uint32_t legal, reach;
+  if constexpr (kSpeculate) {
+    // wave 1 also loads every in-window neighbour label
 #pragma unroll
-  for (int d = 0; d < 10; ++d) {
-    const uint32_t ni = d < 8 ? here + static_cast<uint32_t>(fdy(d)) * w + static_cast<uint32_t>(fdx(d))
-                              : (d == 8 ? here - plane : here + plane);
-    seen[d] = (reach & (1u << d)) ? static_cast<uint32_t>(__ldcg(words + ni) >> 32) : 0u;
+    for (int d = 0; d < 10; ++d) {
+      const uint32_t ni = d < 8 ? here + static_cast<uint32_t>(fdy(d)) * w + static_cast<uint32_t>(fdx(d))
+                                : (d == 8 ? here - plane : here + plane);
+      seen[d] = ((inside & corr_in) & (1u << d)) ? static_cast<uint32_t>(__ldcg(words + ni) >> 32) : 0u;
+    }
+    legal = static_cast<uint32_t>(__ldg(mv_at)) & inside;
+    reach = legal & corr_in;
+  } else {
+    legal = static_cast<uint32_t>(__ldg(mv_at)) & inside;
+    reach = legal & corr_in;
+    // wave 2: the labels of the legal neighbours only
+#pragma unroll
+    for (int d = 0; d < 10; ++d) {
+      const uint32_t ni = d < 8 ? here + static_cast<uint32_t>(fdy(d)) * w + static_cast<uint32_t>(fdx(d))
+                                : (d == 8 ? here - plane : here + plane);
+      seen[d] = (reach & (1u << d)) ? static_cast<uint32_t>(__ldcg(words + ni) >> 32) : 0u;
+    }
   }
   // entry prices of the neighbours (0 without a price snapshot); a cell of
   // the net's own previous path is priced without the net's own use
@@ -560,11 +576,11 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
             ++expanded;
             bool overflow = false;
             if (kCorr && use_corr) {
-              expand_cell<kPriced, kCorr>(lat, win, cell, words, thr, cur_low, far_low,
+              expand_cell<kPriced, kCorr, (G >= 4)>(lat, win, cell, words, thr, cur_low, far_low,
                                           p.cell_cost, p.cell_cost_own, own, corr, cshift,
                                           exit_min, ne, cur_mask, far_mask, overflow, link);
             } else {
-              expand_cell<kPriced, false>(lat, win, cell, words, thr, cur_low, far_low,
+              expand_cell<kPriced, false, (G >= 4)>(lat, win, cell, words, thr, cur_low, far_low,
                                           p.cell_cost, p.cell_cost_own, own, corr, cshift,
                                           exit_min, ne, cur_mask, far_mask, overflow, link);
             }
