@@ -297,6 +297,50 @@ struct ConvArgs {
 
 enum { kEpiRelu = 0, kEpiGate = 1 };
 
+// The input halo of a 128-cell tile (rows y0 - 1 .. y0 + 2, columns -1 .. 64
+// of one net): [4][66][cin] bf16, zero outside the window.
+template <int CIN>
+struct Halo {
+  static constexpr int kCols = kGrid + 2;
+  static constexpr int kUnits = 4 * kCols * (CIN / 8);  // 16-byte chunks
+  static constexpr int kBytes = kUnits * 16;
+};
+
+// Stages a tile's halo with every load of a thread in flight before its
+// first store (one exposed latency per tile instead of one per chunk).
+template <int CIN>
+__device__ __forceinline__ void stage_halo(const __nv_bfloat16* x, uint32_t net, int y0, int cw, int ch,
+                                           uint8_t* halo, int tid) {
+  constexpr int kUnits = Halo<CIN>::kUnits;
+  constexpr int kPer = (kUnits + 127) / 128;
+  uint4 v[kPer];
+#pragma unroll
+  for (int k = 0; k < kPer; ++k) {
+    const int u = tid + k * 128;
+    v[k] = make_uint4(0u, 0u, 0u, 0u);
+    if (u < kUnits) {
+      const int j = u % (CIN / 8), rest = u / (CIN / 8);
+      const int c = rest % Halo<CIN>::kCols, r = rest / Halo<CIN>::kCols;
+      const int sy = y0 - 1 + r, sx = c - 1;
+      if (sx >= 0 && sy >= 0 && sx < cw && sy < ch) {
+        v[k] = __ldg(reinterpret_cast<const uint4*>(x + cell_of(net, sy, sx) * CIN) + j);
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kPer; ++k) {
+    const int u = tid + k * 128;
+    if (u < kUnits) reinterpret_cast<uint4*>(halo)[u] = v[k];
+  }
+}
+
+// Halo chunk j of the input cell read by output cell m (0..127) through tap t.
+template <int CIN>
+__device__ __forceinline__ uint4 halo_chunk(const uint8_t* halo, int m, int t, int j) {
+  const int r = m / kGrid + t / 3, c = m % kGrid + t % 3;
+  return reinterpret_cast<const uint4*>(halo)[(r * Halo<CIN>::kCols + c) * (CIN / 8) + j];
+}
+
 template <int CIN>
 struct ConvSmem {
   static constexpr int K = 9 * CIN;
@@ -304,7 +348,7 @@ struct ConvSmem {
   static constexpr int kSboA = kChunks * 128;    // bytes between 8-row groups
   static constexpr int kBytesA = 16 * kSboA;     // 128 rows
   static constexpr int kBytesB = 4 * kSboA;      // 32 rows
-  static constexpr int kBytes = kBytesA + kBytesB + 16;
+  static constexpr int kBytes = kBytesA + kBytesB + Halo<CIN>::kBytes + 16;
 };
 
 // out[cell][co] = epilogue(sum_{tap, ci} x[cell + tap][ci] * w[co][tap][ci]).
@@ -314,7 +358,8 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(ConvArgs a) {
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* sa = smem;
   uint8_t* sb = smem + S::kBytesA;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S::kBytesA + S::kBytesB);
+  uint8_t* halo = smem + S::kBytesA + S::kBytesB;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S::kBytesA + S::kBytesB + Halo<CIN>::kBytes);
   __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
@@ -342,17 +387,15 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(ConvArgs a) {
     const uint32_t d = a.dims[net];
     const int cw = static_cast<int>(dims_w(d)), ch = static_cast<int>(dims_h(d));
     if (y0 >= ch) continue;  // uniform: no cell of these rows is in the window
-    // im2col: A[m][tap * CIN + ci] for the 128 cells (rows y0, y0 + 1)
+    stage_halo<CIN>(a.x, net, y0, cw, ch, halo, tid);
+    __syncthreads();
+    // im2col: A[m][tap * CIN + ci] for the 128 cells (rows y0, y0 + 1); rows
+    // of cells outside the window hold finite halo values and are not stored
     for (int u = tid; u < 128 * 9 * (CIN / 8); u += 128) {
       const int m = u % 128, r = u / 128;
       const int j = r % (CIN / 8), t = r / (CIN / 8);
-      const int py = y0 + m / kGrid, px = m % kGrid;
-      const int sy = py + t / 3 - 1, sx = px + t % 3 - 1;
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (px < cw && py < ch && sx >= 0 && sy >= 0 && sx < cw && sy < ch) {
-        v = __ldg(reinterpret_cast<const uint4*>(a.x + cell_of(net, sy, sx) * CIN) + j);
-      }
-      *reinterpret_cast<uint4*>(sa + (m % 8) * 16 + (m / 8) * S::kSboA + (t * (CIN / 8) + j) * 128) = v;
+      *reinterpret_cast<uint4*>(sa + (m % 8) * 16 + (m / 8) * S::kSboA + (t * (CIN / 8) + j) * 128) =
+          halo_chunk<CIN>(halo, m, t, j);
     }
     fence_async_smem();
     __syncthreads();
@@ -429,7 +472,7 @@ struct WgradSmem {
   static constexpr int kBytesTile = 16 * kSbo;         // 128 rows x 128 cells
   static constexpr int kBytesA = kTiles * kBytesTile;
   static constexpr int kBytesB = 4 * kSbo;             // 32 rows x 128 cells
-  static constexpr int kBytes = kBytesA + kBytesB + 16;
+  static constexpr int kBytes = kBytesA + kBytesB + Halo<CIN>::kBytes + 16;
 };
 
 // dw[co][tap * CIN + ci] += sum over cells of x[cell + tap][ci] * dy[cell][co];
@@ -441,7 +484,8 @@ __global__ void __launch_bounds__(128) conv_wgrad_tc_kernel(WgradArgs a) {
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* sa = smem;
   uint8_t* sb = smem + S::kBytesA;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S::kBytesA + S::kBytesB);
+  uint8_t* halo = smem + S::kBytesA + S::kBytesB;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S::kBytesA + S::kBytesB + Halo<CIN>::kBytes);
   __shared__ uint32_t tmem_slot;
   __shared__ float bias_part[32];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -474,16 +518,14 @@ __global__ void __launch_bounds__(128) conv_wgrad_tc_kernel(WgradArgs a) {
       if (px < cw && py < ch) v = __ldg(reinterpret_cast<const uint4*>(a.dy + cell_of(net, py, px) * kCh) + j);
       *reinterpret_cast<uint4*>(sb + (k % 8) * 16 + j * S::kSbo + (k / 8) * 128) = v;
     }
-    // A: im2col rows (tap, ci) per cell
+    // A: im2col rows (tap, ci) per cell, from the staged halo (cells outside
+    // the window carry finite halo values against a zero dy)
+    stage_halo<CIN>(a.x, net, y0, cw, ch, halo, tid);
+    __syncthreads();
     for (int u = tid; u < 128 * 9 * (CIN / 8); u += 128) {
       const int k = u % 128, r = u / 128;
       const int j = r % (CIN / 8), t = r / (CIN / 8);
-      const int py = y0 + k / kGrid, px = k % kGrid;
-      const int sy = py + t / 3 - 1, sx = px + t % 3 - 1;
-      uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (px < cw && py < ch && sx >= 0 && sy >= 0 && sx < cw && sy < ch) {
-        v = __ldg(reinterpret_cast<const uint4*>(a.x + cell_of(net, sy, sx) * CIN) + j);
-      }
+      const uint4 v = halo_chunk<CIN>(halo, k, t, j);
       const int row = t * CIN + j * 8;
       *reinterpret_cast<uint4*>(sa + (row / 128) * S::kBytesTile + (k % 8) * 16 + ((row % 128) / 8) * S::kSbo +
                                 (k / 8) * 128) = v;

@@ -183,10 +183,12 @@ int class_for_width(uint32_t width, int layers) {
 // medium batch: 4-layer windows of 10^4 to 10^7 cells) give every window
 // above 256k cells 16 warps.
 int frontier_class(uint64_t cells) {
+  // measured on the medium batch: 16-warp groups take a whole SM each, so
+  // they pay off only for the largest windows
   if (cells <= (1ull << 12)) return 0;
-  if (cells <= (1ull << 14)) return 1;
-  if (cells <= (1ull << 16)) return 2;
-  if (cells <= (1ull << 18)) return 3;
+  if (cells <= (1ull << 15)) return 1;
+  if (cells <= (1ull << 17)) return 2;
+  if (cells <= (1ull << 20)) return 3;
   return 4;
 }
 

@@ -68,8 +68,8 @@ def test_layer_counts_and_via_masks(layers):
 def test_every_warp_class():
     # windows from ~10^4 to ~10^7 cells (1 to 16 warps per net)
     lat = synth.make_lattice(41, 4, 2048, 0.18, via_mask=True)
-    nets = synth.make_nets(lat, 42, 10, hpwl_median=100.0, hpwl_sigma=0.3, margin=16)
-    sizes = [(64, 64), (300, 200), (700, 600), (1500, 1200), (2048, 1200)]
+    nets = synth.make_nets(lat, 42, 12, hpwl_median=100.0, hpwl_sigma=0.3, margin=16)
+    sizes = [(64, 64), (150, 120), (300, 200), (700, 600), (1500, 1200), (2048, 1200)]
     for i in range(len(nets)):
         w, h = sizes[i % len(sizes)]
         for axis, extent, dim in (("x", w, 2048), ("y", h, 2048)):
