@@ -285,6 +285,23 @@ class Plan:
         ptr = None if bits is None else ctypes.c_void_p(bits.data_ptr())
         _check(lib().apgar_b200_lattice_plan_set_corridors(self.handle, ptr))
 
+    def segments(self, origin_x: int = 0, origin_y: int = 0, step: int = 1, stream: int = 0):
+        """Exact-coordinate segments of the last execution's paths (GPU):
+        (segments as a CUDA int64 tensor viewed by apgar_b200.dropin.SEGMENT_DTYPE
+        after .cpu().numpy(), per-net counts as a CUDA int32 tensor); net i's
+        segments start at its result's path_offset."""
+        import torch
+
+        cap = max(int(self.info()["path_arena_capacity"]), 1)
+        segs = torch.empty(cap * 5, dtype=torch.int64, device="cuda")  # 40 B per segment
+        counts = torch.empty(max(len(self.nets), 1), dtype=torch.int32, device="cuda")
+        _check(lib().apgar_b200_lattice_segments(self.handle, ctypes.c_int64(origin_x),
+                                                 ctypes.c_int64(origin_y), ctypes.c_int64(step),
+                                                 ctypes.c_void_p(segs.data_ptr()),
+                                                 ctypes.c_void_p(counts.data_ptr()),
+                                                 ctypes.c_void_p(stream)))
+        return segs, counts
+
     def corridor_status(self) -> np.ndarray:
         """Per-net corridor outcomes of the last corridor-mode execute
         (``apgar_b200.corridor`` CERTIFIED / FALLBACK_*)."""

@@ -33,6 +33,11 @@ namespace apgar_b200 {
 
 cudaError_t launch_graph_search(const GraphLaunch& launch, cudaStream_t stream);
 cudaError_t launch_validate_paths(const PathCheckLaunch& launch, cudaStream_t stream);
+cudaError_t launch_path_segments(const apgar_b200_node_v1* nodes, uint32_t node_count, int64_t ox,
+                                 int64_t oy, int64_t step, const apgar_b200_compact_path_v1* paths,
+                                 const uint32_t* states, uint64_t state_count, uint32_t count,
+                                 apgar_b200_segment* segments, uint32_t* segment_counts,
+                                 cudaStream_t stream);
 cudaError_t launch_graph_pack(apgar_b200_compact_path_v1* compact, uint32_t count,
                               uint64_t states_per_query, const uint32_t* stage, uint32_t* packed,
                               unsigned long long* total, int sm_count, cudaStream_t stream);
@@ -754,5 +759,51 @@ extern "C" int apgar_b200_validate_compact_paths(
     return APGAR_B200_OK;
   } catch (const std::bad_alloc&) {
     return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "host allocation failed during path validation");
+  }
+}
+
+extern "C" int apgar_b200_path_segments(void* view, const apgar_b200_compact_path_v1* paths,
+                                        uint32_t path_count, const uint32_t* path_states,
+                                        uint64_t path_state_count, apgar_b200_segment* segments,
+                                        uint64_t segment_capacity, uint32_t* segment_counts) {
+  if (view == nullptr || (path_count > 0 && (paths == nullptr || segment_counts == nullptr)) ||
+      (path_state_count > 0 && (path_states == nullptr || segments == nullptr))) {
+    return invariant("path segments received a null argument");
+  }
+  if (segment_capacity < path_state_count) {
+    return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "segment output is smaller than the path states");
+  }
+  auto* v = static_cast<ViewObject*>(view);
+  if (int rc = check_device(v->device); rc != APGAR_B200_OK) return rc;
+  try {
+    DeviceBuffer<apgar_b200_compact_path_v1> d_paths;
+    DeviceBuffer<uint32_t> d_states, d_counts;
+    DeviceBuffer<apgar_b200_segment> d_segs;
+    APGAR_B200_CUDA("cudaMalloc(paths)", d_paths.ensure(std::max<uint32_t>(path_count, 1)));
+    APGAR_B200_CUDA("cudaMalloc(states)", d_states.ensure(std::max<uint64_t>(path_state_count, 1)));
+    APGAR_B200_CUDA("cudaMalloc(counts)", d_counts.ensure(std::max<uint32_t>(path_count, 1)));
+    APGAR_B200_CUDA("cudaMalloc(segments)", d_segs.ensure(std::max<uint64_t>(path_state_count, 1)));
+    if (path_count > 0) {
+      APGAR_B200_CUDA("cudaMemcpy(paths)", cudaMemcpy(d_paths.get(), paths, path_count * sizeof(*paths), cudaMemcpyHostToDevice));
+    }
+    if (path_state_count > 0) {
+      APGAR_B200_CUDA("cudaMemcpy(states)", cudaMemcpy(d_states.get(), path_states, path_state_count * 4, cudaMemcpyHostToDevice));
+    }
+    APGAR_B200_CUDA("path segments launch",
+                    launch_path_segments(v->nodes_dev.get(), static_cast<uint32_t>(v->legal.size()),
+                                         v->header.lattice_origin_x, v->header.lattice_origin_y,
+                                         v->header.lattice_step, d_paths.get(), d_states.get(),
+                                         path_state_count, path_count, d_segs.get(), d_counts.get(),
+                                         nullptr));
+    if (path_count > 0) {
+      APGAR_B200_CUDA("cudaMemcpy(counts)", cudaMemcpy(segment_counts, d_counts.get(), path_count * 4, cudaMemcpyDeviceToHost));
+    }
+    if (path_state_count > 0) {
+      APGAR_B200_CUDA("cudaMemcpy(segments)", cudaMemcpy(segments, d_segs.get(), path_state_count * sizeof(apgar_b200_segment), cudaMemcpyDeviceToHost));
+    }
+    clear_error();
+    return APGAR_B200_OK;
+  } catch (const std::bad_alloc&) {
+    return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "host allocation failed during path segments");
   }
 }

@@ -48,6 +48,10 @@ cudaError_t launch_rasters(const LatticeDeviceView& lat, const apgar_b200_lattic
 cudaError_t launch_labels(const apgar_b200_lattice_net* nets, uint32_t count, const uint32_t* dims,
                           int lat_w, int lat_h, const apgar_b200_lattice_result* results,
                           const uint32_t* paths, uint8_t* labels, cudaStream_t stream);
+cudaError_t launch_lattice_segments(const apgar_b200_lattice_result* results, const uint32_t* paths,
+                                    uint32_t count, uint32_t width, uint32_t height, int64_t ox,
+                                    int64_t oy, int64_t step, apgar_b200_segment* segments,
+                                    uint32_t* segment_counts, cudaStream_t stream);
 cudaError_t launch_corridors(const float* logits, const uint32_t* dims,
                              const apgar_b200_lattice_net* nets, uint32_t count, float threshold,
                              int dilate, uint32_t* bits, cudaStream_t stream);
@@ -776,6 +780,24 @@ extern "C" int apgar_b200_corridor_from_logits(void* plan, const float* logits, 
   if (int rc = check_device(p->device); rc != APGAR_B200_OK) return rc;
   APGAR_B200_CUDA("corridor launch", launch_corridors(logits, dims, p->nets.get(), p->count, threshold,
                                                       dilate, bits, static_cast<cudaStream_t>(stream)));
+  clear_error();
+  return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_lattice_segments(void* plan, int64_t origin_x, int64_t origin_y, int64_t step,
+                                           apgar_b200_segment* segments, uint32_t* segment_counts,
+                                           void* stream) {
+  if (plan == nullptr || segments == nullptr || segment_counts == nullptr) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "lattice segments received a null argument");
+  }
+  auto* p = static_cast<PlanObject*>(plan);
+  if (int rc = check_device(p->device); rc != APGAR_B200_OK) return rc;
+  const LatticeDeviceView& v = p->lattice->view;
+  APGAR_B200_CUDA("lattice segments launch",
+                  launch_lattice_segments(p->results.get(), p->paths.get(), p->count,
+                                          static_cast<uint32_t>(v.width), static_cast<uint32_t>(v.height),
+                                          origin_x, origin_y, step, segments, segment_counts,
+                                          static_cast<cudaStream_t>(stream)));
   clear_error();
   return APGAR_B200_OK;
 }

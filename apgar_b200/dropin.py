@@ -122,6 +122,12 @@ def make_queries(view_nodes: int, entries, batch_id: int = 7, generator: int = G
     return q, np.ascontiguousarray(edge_arr)
 
 
+# apgar_b200_segment (40 bytes)
+SEGMENT_DTYPE = np.dtype([("layer0", "<u4"), ("layer1", "<u4"), ("x0", "<i8"), ("y0", "<i8"),
+                          ("x1", "<i8"), ("y1", "<i8")])
+SEGMENT_FAILURE = 0xFFFFFFFF
+
+
 class View:
     """UploadCompiledView: the reference flattened device view on this GPU."""
 
@@ -186,6 +192,20 @@ class View:
             _vp(results), _vp(compact), _vp(states) if len(states) else None,
             ctypes.c_uint64(len(states)), _vp(out)))
         return out
+
+    def path_segments(self, compact, states):
+        """Exact-coordinate segments of read-back compact paths (GPU):
+        (segments record array indexed like the states, per-path counts;
+        path i's segments are segments[compact[i].state_offset:][:count])."""
+        compact = np.ascontiguousarray(compact)
+        states = np.ascontiguousarray(states, dtype=np.uint32)
+        segments = np.zeros(max(len(states), 1), dtype=SEGMENT_DTYPE)
+        counts = np.zeros(max(len(compact), 1), dtype=np.uint32)
+        _check(lib().apgar_b200_path_segments(
+            self.handle, _vp(compact), ctypes.c_uint32(len(compact)),
+            _vp(states) if len(states) else None, ctypes.c_uint64(len(states)), _vp(segments),
+            ctypes.c_uint64(len(segments)), _vp(counts)))
+        return segments, counts[: len(compact)]
 
     def execute_route(self, start_node, goal_node, generator=GENERATOR_SWEEP, maximum_rounds=100_000,
                       routing_profile_fingerprint=0, maximum_device_bytes=(1 << 64) - 1):

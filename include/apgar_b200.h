@@ -468,6 +468,41 @@ APGAR_B200_API int apgar_b200_lattice_route_ex(void* lattice, const apgar_b200_l
                                 uint64_t path_capacity, uint64_t* path_total);
 APGAR_B200_API int apgar_b200_lattice_plan_release(void* plan);
 
+/* =================== F. route reconstruction =================== */
+
+/* One segment of a reconstructed route, in exact board coordinates (origin +
+ * lattice index * step, LatticeIndexToExactPoint,
+ * src/geometry_compiler/compiled_board.cc:219-238).  layer0 == layer1 for a
+ * planar run (routing::LayerSegment, include/apgar/routing/planar_route.h:32);
+ * a run of vias has layer0 != layer1 and equal end points.  40 bytes. */
+typedef struct apgar_b200_segment {
+  uint32_t layer0, layer1;
+  int64_t x0, y0, x1, y1;
+} apgar_b200_segment;
+/* segment count of a path that failed reconstruction (a state outside the
+ * view, or a point outside the exact coordinate envelope |v| <= 10^12) */
+#define APGAR_B200_SEGMENT_FAILURE 0xFFFFFFFFu
+
+/* Coalesces V1 compact paths (reverse states, goal first) into segments on
+ * the GPU: a segment starts at the start point and wherever the step between
+ * consecutive points changes (routing::CoalesceSegments,
+ * src/routing/planar_route.cc:188-215, applied by the reference to every
+ * host-validated GPU path, src/gpu/planar_router.cc:1085-1105).  Host
+ * buffers: path i's segments are written at segments + paths[i].state_offset
+ * (segment_capacity >= path_state_count), its count at segment_counts[i]. */
+APGAR_B200_API int apgar_b200_path_segments(void* view, const apgar_b200_compact_path_v1* paths,
+                             uint32_t path_count, const uint32_t* path_states,
+                             uint64_t path_state_count, apgar_b200_segment* segments,
+                             uint64_t segment_capacity, uint32_t* segment_counts);
+/* The same for the packed paths of a lattice plan's last execution, on
+ * device memory and `stream`: net i's segments at segments +
+ * results[i].path_offset (capacity: the plan's packed path cells), its count
+ * at segment_counts[i] (0 when not reached).  Lattice index (x, y) maps to
+ * (origin_x + x * step, origin_y + y * step); a via run splits segments. */
+APGAR_B200_API int apgar_b200_lattice_segments(void* plan, int64_t origin_x, int64_t origin_y, int64_t step,
+                                apgar_b200_segment* segments, uint32_t* segment_counts,
+                                void* stream);
+
 /* ===================== E. learned corridor (CNN) =====================
  * No reference counterpart.  A 6-layer 3x3 CNN (layers 1-5: 16 -> 32 -> ... ->
  * 32 channels, bias, ReLU, bf16 weights and activations, f32 accumulation on

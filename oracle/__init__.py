@@ -384,3 +384,42 @@ def corridor_certificate(lat, net, mask):
         best = m if best is None else min(best, m)
     status = CORRIDOR_CERTIFIED if best is None or cost < best else CORRIDOR_FALLBACK_EXIT
     return status, int(cost), best
+
+
+# ---------------------------------------------------------------------------
+# Route reconstruction: exact points and coalesced segments.
+SEGMENT_DTYPE = np.dtype([("layer0", "<u4"), ("layer1", "<u4"), ("x0", "<i8"), ("y0", "<i8"),
+                          ("x1", "<i8"), ("y1", "<i8")])
+MAX_ABS_DB_COORD = 1_000_000_000_000  # board_ir::kMaxAbsDbCoord (include/apgar/board_ir/board.h:20)
+
+
+def exact_points(origin_x, origin_y, step, lattice_x, lattice_y):
+    """origin + index * step per axis (LatticeIndexToExactPoint,
+    src/geometry_compiler/compiled_board.cc:219-238); None if a point leaves
+    the exact coordinate envelope."""
+    xs = [int(origin_x) + int(x) * int(step) for x in lattice_x]
+    ys = [int(origin_y) + int(y) * int(step) for y in lattice_y]
+    if any(abs(v) > MAX_ABS_DB_COORD for v in xs + ys):
+        return None
+    return np.array(xs, np.int64), np.array(ys, np.int64)
+
+
+def coalesce_segments(xs, ys, layers):
+    """Segments of a forward point sequence: a new segment starts wherever the
+    step (dx, dy, dlayer) changes (routing::CoalesceSegments,
+    src/routing/planar_route.cc:188-215, with the layer step added for vias;
+    on one layer the two agree).  Fewer than two points give no segment."""
+    n = len(xs)
+    out = []
+    if n < 2:
+        return np.zeros(0, SEGMENT_DTYPE)
+    start = 0
+    prev = (xs[1] - xs[0], ys[1] - ys[0], int(layers[1]) - int(layers[0]))
+    for i in range(2, n):
+        step = (xs[i] - xs[i - 1], ys[i] - ys[i - 1], int(layers[i]) - int(layers[i - 1]))
+        if step != prev:
+            out.append((layers[start], layers[i - 1], xs[start], ys[start], xs[i - 1], ys[i - 1]))
+            start = i - 1
+            prev = step
+    out.append((layers[start], layers[n - 1], xs[start], ys[start], xs[n - 1], ys[n - 1]))
+    return np.array(out, SEGMENT_DTYPE)

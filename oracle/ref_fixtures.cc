@@ -62,6 +62,10 @@ struct QueryOut {
   uint32_t cpu_status;  // 0 reached, 1 disconnected, 2 other failure
   uint64_t cpu_cost;
   uint64_t policy_identity;
+  // reached routes: forward device nodes of the lattice path and the
+  // reference's coalesced segments (routing::CoalesceSegments)
+  std::vector<uint32_t> route_nodes;
+  std::vector<apgar::routing::LayerSegment> segments;
 };
 
 std::vector<apgar::routing::EdgeResourceKey> path_resources(
@@ -134,6 +138,13 @@ int main(int argc, char** argv) {
   std::ostringstream manifest;
   manifest << "{\n  \"cases\": [\n";
   bool first_case = true;
+  // segments.bin: per reached route, (case, query, layer, forward nodes,
+  // reference segments as layer, x0, y0, x1, y1)
+  Writer segw;
+  segw.pod<uint64_t>(0x3147455354524741ull);  // magic "AGRTSEG1"
+  uint64_t segment_records = 0;
+  Writer segbody;
+  uint32_t case_index = 0;
   for (auto& c : corpus) {
     auto dev_result = apgar::gpu::BuildDeviceCompiledBoardV1(c.board, c.compiled_board);
     if (std::holds_alternative<apgar::gpu::PlanarGpuFailure>(dev_result)) {
@@ -204,6 +215,18 @@ int main(int argc, char** argv) {
         if (auto* route = std::get_if<apgar::routing::CpuRoute>(&result)) {
           q.cpu_status = 0;
           q.cpu_cost = route->total_cost;
+          bool mapped = true;
+          for (const auto& point : route->lattice_path) {
+            const auto idx = apgar::geometry_compiler::ExactPointToLatticeIndex(profile, point);
+            const auto node = idx ? apgar::gpu::FindDeviceNodeIndex(device, req.start_layer, *idx)
+                                  : std::nullopt;
+            if (!node) {
+              mapped = false;
+              break;
+            }
+            q.route_nodes.push_back(*node);
+          }
+          if (mapped) q.segments = route->segments;
         } else {
           const auto& f = std::get<apgar::routing::RouteFailure>(result);
           q.cpu_status = f.code == apgar::routing::RouteFailureCode::kDisconnected ? 1u : 2u;
@@ -212,6 +235,25 @@ int main(int argc, char** argv) {
         queries.push_back(std::move(q));
       }
     }
+
+    for (size_t qi = 0; qi < queries.size(); ++qi) {
+      const QueryOut& q = queries[qi];
+      if (q.cpu_status != 0 || q.route_nodes.empty()) continue;
+      segbody.pod<uint32_t>(case_index);
+      segbody.pod<uint32_t>(static_cast<uint32_t>(qi));
+      segbody.array(q.route_nodes);
+      segbody.pod<uint64_t>(q.segments.size());
+      for (const auto& sgm : q.segments) {
+        segbody.pod<uint32_t>(static_cast<uint32_t>(sgm.layer));
+        segbody.pod<uint32_t>(0);
+        segbody.pod<int64_t>(sgm.centerline.start.x);
+        segbody.pod<int64_t>(sgm.centerline.start.y);
+        segbody.pod<int64_t>(sgm.centerline.end.x);
+        segbody.pod<int64_t>(sgm.centerline.end.y);
+      }
+      ++segment_records;
+    }
+    ++case_index;
 
     Writer w;
     w.pod<uint64_t>(0x3158495446524741ull);  // magic "AGRFTIX1"
@@ -257,5 +299,12 @@ int main(int argc, char** argv) {
   }
   manifest << "\n  ]\n}\n";
   std::ofstream(out_dir + "/manifest.json") << manifest.str();
+  segw.pod<uint64_t>(segment_records);
+  segw.bytes.insert(segw.bytes.end(), segbody.bytes.begin(), segbody.bytes.end());
+  {
+    std::ofstream out(out_dir + "/segments.bin", std::ios::binary);
+    out.write(reinterpret_cast<const char*>(segw.bytes.data()),
+              static_cast<std::streamsize>(segw.bytes.size()));
+  }
   return 0;
 }

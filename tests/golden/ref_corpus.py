@@ -112,7 +112,28 @@ def load_case(path: str) -> Case:
 
 
 def load_all() -> list:
-    return [load_case(p) for p in sorted(glob.glob(os.path.join(HERE, "*.bin")))]
+    return [load_case(p) for p in sorted(glob.glob(os.path.join(HERE, "*.bin")))
+            if os.path.basename(p) != "segments.bin"]
+
+
+SEGMENT_DTYPE = np.dtype([("layer", "<u4"), ("pad", "<u4"), ("x0", "<i8"), ("y0", "<i8"),
+                          ("x1", "<i8"), ("y1", "<i8")])
+
+
+def load_segments() -> list:
+    """Reference routing::CoalesceSegments outputs: one (case name, query
+    index, forward device nodes of the reference CPU A* route, segments)
+    tuple per reached route of the corpus (written by oracle/ref_fixtures.cc)."""
+    r = _Reader(open(os.path.join(HERE, "segments.bin"), "rb").read())
+    assert r.u64() == 0x3147455354524741, "bad segments magic"
+    names = [c["name"] for c in manifest()["cases"]]
+    out = []
+    for _ in range(r.u64()):
+        case, query = r.u32(), r.u32()
+        nodes = r.array("<u4")
+        segs = r.array(SEGMENT_DTYPE)
+        out.append((names[case], query, nodes, segs))
+    return out
 
 
 def manifest() -> dict:
