@@ -503,6 +503,46 @@ APGAR_B200_API int apgar_b200_lattice_segments(void* plan, int64_t origin_x, int
                                 apgar_b200_segment* segments, uint32_t* segment_counts,
                                 void* stream);
 
+/* =================== G. geometry compile (edge legality) =================== */
+
+/* An obstacle box in board units (board_ir::Obstacle, its layer and whether
+ * the routed net owns it; owned boxes never block).  40 bytes. */
+typedef struct apgar_b200_obstacle_box {
+  int64_t min_x, min_y, max_x, max_y;
+  uint32_t layer, owned_by_net;
+} apgar_b200_obstacle_box;
+
+/* The compile rules of edge legality: the routing profile's trace width and
+ * clearance, the compiler's lattice placement and heading mask (bit 0
+ * horizontal, 1 vertical, 2 diagonal 45; board_ir::Heading).  48 bytes. */
+typedef struct apgar_b200_edge_rules {
+  int64_t nominal_width, clearance;
+  int64_t lattice_origin_x, lattice_origin_y, lattice_step;
+  uint32_t heading_mask, reserved;
+} apgar_b200_edge_rules;
+
+/* Exact swept-trace clearance of one-step centrelines against boxes, on the
+ * GPU (geometry::SweptTraceClearanceAtLeast, src/geometry/exact.cc:325-360):
+ * cases are 10 int64 each (start x, y, end x, y, box min x, y, max x, y,
+ * width, clearance); out receives (error, satisfied) per case, error 0 ok,
+ * 1 coordinate out of range, 2 box not normalized, 3 width or clearance out
+ * of range (geometry::ExactGeometryErrorCode order).  Host buffers. */
+APGAR_B200_API int apgar_b200_swept_clearance(const int64_t* cases, uint64_t count, uint32_t* out);
+
+/* The legal-edge masks of the geometry compile for the given lattice nodes
+ * (CompileBoard's edge loop, src/geometry_compiler/compiled_board.cc:427-476):
+ * bit d (geometry_compiler::Direction order E, NE, N, NW, W, SW, S, SE) is set
+ * when the neighbour in direction d is one of the given nodes on the same
+ * layer, the heading is in rules->heading_mask, and the move clears every
+ * obstacle on the layer not owned by the net.  lattice_xy holds (x, y) per
+ * node.  Host buffers; the exact tests run on the GPU over per-layer
+ * obstacle bins. */
+APGAR_B200_API int apgar_b200_compile_legal_edges(const apgar_b200_edge_rules* rules,
+                                   const apgar_b200_obstacle_box* obstacles,
+                                   uint64_t obstacle_count, const int64_t* lattice_xy,
+                                   const uint32_t* layers, uint32_t node_count,
+                                   uint8_t* legal_edges);
+
 /* ===================== E. learned corridor (CNN) =====================
  * No reference counterpart.  A 6-layer 3x3 CNN (layers 1-5: 16 -> 32 -> ... ->
  * 32 channels, bias, ReLU, bf16 weights and activations, f32 accumulation on

@@ -423,3 +423,115 @@ def coalesce_segments(xs, ys, layers):
             prev = step
     out.append((layers[start], layers[n - 1], xs[start], ys[start], xs[n - 1], ys[n - 1]))
     return np.array(out, SEGMENT_DTYPE)
+
+
+# ---------------------------------------------------------------------------
+# Exact edge legality of the geometry compile (pure-Python integers; small
+# cases only).  A one-step lattice move is legal when the swept trace of
+# width w keeps clearance c from every obstacle box on its layer that the
+# routed net does not own (geometry::SweptTraceClearanceAtLeast,
+# src/geometry/exact.cc:165-216 and :325-360; CompileBoard's edge loop,
+# src/geometry_compiler/compiled_board.cc:427-476).  Coordinates are doubled
+# so that the required distance w + 2c stays integral.
+CLEARANCE_OK, CLEARANCE_OUT_OF_RANGE, CLEARANCE_BAD_BOX, CLEARANCE_BAD_DISTANCE = 0, 1, 2, 3
+
+
+def _orient(a, b, c):
+    return (b[0] - a[0]) * (c[1] - a[1]) - (b[1] - a[1]) * (c[0] - a[0])
+
+
+def _on_segment(a, b, p):
+    return (_orient(a, b, p) == 0 and min(a[0], b[0]) <= p[0] <= max(a[0], b[0])
+            and min(a[1], b[1]) <= p[1] <= max(a[1], b[1]))
+
+
+def _sign(v):
+    return (v > 0) - (v < 0)
+
+
+def _segments_touch(a, b, c, d):
+    o1, o2 = _orient(a, b, c), _orient(a, b, d)
+    o3, o4 = _orient(c, d, a), _orient(c, d, b)
+    if _sign(o1) * _sign(o2) < 0 and _sign(o3) * _sign(o4) < 0:
+        return True
+    return ((o1 == 0 and _on_segment(a, b, c)) or (o2 == 0 and _on_segment(a, b, d))
+            or (o3 == 0 and _on_segment(c, d, a)) or (o4 == 0 and _on_segment(c, d, b)))
+
+
+def _point_segment_at_least(p, a, b, req):
+    vx, vy = b[0] - a[0], b[1] - a[1]
+    wx, wy = p[0] - a[0], p[1] - a[1]
+    len2 = vx * vx + vy * vy
+    if len2 == 0:
+        return wx * wx + wy * wy >= req * req
+    proj = wx * vx + wy * vy
+    if proj <= 0:
+        return wx * wx + wy * wy >= req * req
+    if proj >= len2:
+        ex, ey = p[0] - b[0], p[1] - b[1]
+        return ex * ex + ey * ey >= req * req
+    cross = vx * wy - vy * wx
+    return cross * cross >= req * req * len2
+
+
+def swept_clearance(start, end, box_min, box_max, width, clearance):
+    """(error code, satisfied) of a centreline segment against one box."""
+    lim = MAX_ABS_DB_COORD
+    if any(abs(int(v)) > lim for v in (*start, *end, *box_min, *box_max)):
+        return CLEARANCE_OUT_OF_RANGE, False
+    if box_min[0] > box_max[0] or box_min[1] > box_max[1]:
+        return CLEARANCE_BAD_BOX, False
+    if width <= 0 or width > lim or clearance < 0 or clearance > lim:
+        return CLEARANCE_BAD_DISTANCE, False
+    req = int(width) + 2 * int(clearance)
+    s = (2 * int(start[0]), 2 * int(start[1]))
+    e = (2 * int(end[0]), 2 * int(end[1]))
+    lo = (2 * int(box_min[0]), 2 * int(box_min[1]))
+    hi = (2 * int(box_max[0]), 2 * int(box_max[1]))
+    if (max(s[0], e[0]) <= lo[0] - req or min(s[0], e[0]) >= hi[0] + req
+            or max(s[1], e[1]) <= lo[1] - req or min(s[1], e[1]) >= hi[1] + req):
+        return CLEARANCE_OK, True
+    inside = lambda p: lo[0] <= p[0] <= hi[0] and lo[1] <= p[1] <= hi[1]  # noqa: E731
+    if inside(s) or inside(e):
+        return CLEARANCE_OK, False
+    corners = [lo, (hi[0], lo[1]), hi, (lo[0], hi[1])]
+    for k in range(4):
+        c, d = corners[k], corners[(k + 1) % 4]
+        if _segments_touch(s, e, c, d):
+            return CLEARANCE_OK, False
+        if not (_point_segment_at_least(s, c, d, req) and _point_segment_at_least(e, c, d, req)
+                and _point_segment_at_least(c, s, e, req) and _point_segment_at_least(d, s, e, req)):
+            return CLEARANCE_OK, False
+    return CLEARANCE_OK, True
+
+
+_DIR = ((1, 0), (1, 1), (0, 1), (-1, 1), (-1, 0), (-1, -1), (0, -1), (1, -1))
+_HEADING = (1, 4, 2, 4, 1, 4, 2, 4)  # horizontal 1, vertical 2, diagonal 4
+
+
+def compile_legal_edges(lattice_x, lattice_y, layers, origin, step, heading_mask, width, clearance,
+                        obstacles):
+    """8-bit legal-edge masks of the given lattice nodes: a direction is legal
+    when its neighbour is a given node on the same layer, the heading is in the
+    compiler's mask, and the move clears every obstacle (minx, miny, maxx, maxy,
+    layer, owned_by_net) on the layer that the net does not own."""
+    index = {(int(l), int(x), int(y)): i for i, (x, y, l) in enumerate(zip(lattice_x, lattice_y, layers))}
+    out = np.zeros(len(lattice_x), np.uint8)
+    for i, (x, y, l) in enumerate(zip(lattice_x, lattice_y, layers)):
+        x, y, l = int(x), int(y), int(l)
+        for d, (dx, dy) in enumerate(_DIR):
+            if (l, x + dx, y + dy) not in index or not (heading_mask & _HEADING[d]):
+                continue
+            a = (origin[0] + x * step, origin[1] + y * step)
+            b = (origin[0] + (x + dx) * step, origin[1] + (y + dy) * step)
+            ok = True
+            for (minx, miny, maxx, maxy, ol, owned) in obstacles:
+                if int(ol) != l or owned:
+                    continue
+                err, sat = swept_clearance(a, b, (minx, miny), (maxx, maxy), width, clearance)
+                if err != CLEARANCE_OK or not sat:
+                    ok = False
+                    break
+            if ok:
+                out[i] |= 1 << d
+    return out

@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "apgar/benchmark/planar_corpus.h"
+#include "apgar/geometry/exact.h"
 #include "apgar/gpu/planar_router.h"
 #include "apgar/routing/candidate_policy.h"
 #include "apgar/routing/cpu_astar.h"
@@ -67,6 +68,62 @@ struct QueryOut {
   std::vector<uint32_t> route_nodes;
   std::vector<apgar::routing::LayerSegment> segments;
 };
+
+// Seeded cases for the exact swept-trace clearance predicate: one-step
+// lattice segments (8 headings) against boxes placed around them, at small
+// and at near-envelope coordinates, with widths and clearances from zero
+// clearance to several steps.  Written with the reference's verdicts.
+void write_clearance_cases(const std::string& path) {
+  uint64_t state = 0x9E3779B97F4A7C15ull;
+  const auto next = [&state]() {
+    state ^= state << 13;
+    state ^= state >> 7;
+    state ^= state << 17;
+    return state;
+  };
+  const auto pick = [&next](int64_t lo, int64_t hi) {
+    return lo + static_cast<int64_t>(next() % static_cast<uint64_t>(hi - lo + 1));
+  };
+  static const int dx[8] = {1, 1, 0, -1, -1, -1, 0, 1};
+  static const int dy[8] = {0, 1, 1, 1, 0, -1, -1, -1};
+  Writer w;
+  w.pod<uint64_t>(0x3143524c43524741ull);  // magic "AGRCLRC1"
+  const uint64_t count = 12000;
+  w.pod<uint64_t>(count);
+  for (uint64_t i = 0; i < count; ++i) {
+    const bool far = (i % 8) == 7;  // near the 10^12 envelope
+    const int64_t step = far ? pick(1, 5) * 100000 : pick(1, 12);
+    const int64_t base = far ? 999999000000ll - pick(0, 1000) * step : 0;
+    const int64_t sx = base + pick(-20, 20) * step, sy = (far ? -base : 0) + pick(-20, 20) * step;
+    const int d = static_cast<int>(next() % 8);
+    apgar::board_ir::Segment64 seg{};
+    seg.start = {sx, sy};
+    seg.end = {sx + dx[d] * step, sy + dy[d] * step};
+    const int64_t cx = sx + pick(-3, 3) * step + pick(-step, step);
+    const int64_t cy = sy + pick(-3, 3) * step + pick(-step, step);
+    const int64_t hw = pick(0, 2 * step), hh = pick(0, 2 * step);
+    apgar::board_ir::AxisAlignedBox64 box{};
+    box.min = {cx - hw, cy - hh};
+    box.max = {cx + hw, cy + hh};
+    const int64_t width = pick(1, 2 * step);
+    const int64_t clearance = pick(0, 2 * step);
+    const auto r = apgar::geometry::SweptTraceClearanceAtLeast(seg, box, width, clearance);
+    w.pod<int64_t>(seg.start.x);
+    w.pod<int64_t>(seg.start.y);
+    w.pod<int64_t>(seg.end.x);
+    w.pod<int64_t>(seg.end.y);
+    w.pod<int64_t>(box.min.x);
+    w.pod<int64_t>(box.min.y);
+    w.pod<int64_t>(box.max.x);
+    w.pod<int64_t>(box.max.y);
+    w.pod<int64_t>(width);
+    w.pod<int64_t>(clearance);
+    w.pod<uint32_t>(static_cast<uint32_t>(r.error));
+    w.pod<uint32_t>(r.clearance_satisfied ? 1u : 0u);
+  }
+  std::ofstream out(path, std::ios::binary);
+  out.write(reinterpret_cast<const char*>(w.bytes.data()), static_cast<std::streamsize>(w.bytes.size()));
+}
 
 std::vector<apgar::routing::EdgeResourceKey> path_resources(
     const apgar::geometry_compiler::CompiledBoard& compiled, apgar::board_ir::LayerId layer,
@@ -145,6 +202,13 @@ int main(int argc, char** argv) {
   uint64_t segment_records = 0;
   Writer segbody;
   uint32_t case_index = 0;
+  // geometry.bin: per case, the compile inputs of every edge's legality (the
+  // routing profile's width, clearance and net, the compiler's heading mask
+  // and lattice placement, and every obstacle box with its layer and whether
+  // the routed net owns it)
+  Writer geow;
+  geow.pod<uint64_t>(0x314f454754524741ull);  // magic "AGRTGEO1"
+  geow.pod<uint64_t>(corpus.size());
   for (auto& c : corpus) {
     auto dev_result = apgar::gpu::BuildDeviceCompiledBoardV1(c.board, c.compiled_board);
     if (std::holds_alternative<apgar::gpu::PlanarGpuFailure>(dev_result)) {
@@ -236,6 +300,29 @@ int main(int argc, char** argv) {
       }
     }
 
+    {
+      const auto& routing = c.compiled_board.prepared_routing_profile().profile();
+      geow.pod<uint32_t>(case_index);
+      geow.pod<uint32_t>(profile.heading_mask);
+      geow.pod<int64_t>(routing.nominal_width);
+      geow.pod<int64_t>(routing.clearance);
+      geow.pod<int64_t>(profile.lattice_origin.x);
+      geow.pod<int64_t>(profile.lattice_origin.y);
+      geow.pod<int64_t>(profile.lattice_step);
+      std::vector<const apgar::board_ir::Obstacle*> obstacles;
+      for (const auto& layer : c.board.data().layers) {
+        for (const auto& o : c.board.ObstaclesOnLayer(layer.routing_id)) obstacles.push_back(&o);
+      }
+      geow.pod<uint64_t>(obstacles.size());
+      for (const auto* o : obstacles) {
+        geow.pod<int64_t>(o->bounds.min.x);
+        geow.pod<int64_t>(o->bounds.min.y);
+        geow.pod<int64_t>(o->bounds.max.x);
+        geow.pod<int64_t>(o->bounds.max.y);
+        geow.pod<uint32_t>(o->layer);
+        geow.pod<uint32_t>(o->owner_net.has_value() && *o->owner_net == routing.net ? 1u : 0u);
+      }
+    }
     for (size_t qi = 0; qi < queries.size(); ++qi) {
       const QueryOut& q = queries[qi];
       if (q.cpu_status != 0 || q.route_nodes.empty()) continue;
@@ -301,6 +388,12 @@ int main(int argc, char** argv) {
   std::ofstream(out_dir + "/manifest.json") << manifest.str();
   segw.pod<uint64_t>(segment_records);
   segw.bytes.insert(segw.bytes.end(), segbody.bytes.begin(), segbody.bytes.end());
+  write_clearance_cases(out_dir + "/clearance.bin");
+  {
+    std::ofstream out(out_dir + "/geometry.bin", std::ios::binary);
+    out.write(reinterpret_cast<const char*>(geow.bytes.data()),
+              static_cast<std::streamsize>(geow.bytes.size()));
+  }
   {
     std::ofstream out(out_dir + "/segments.bin", std::ios::binary);
     out.write(reinterpret_cast<const char*>(segw.bytes.data()),

@@ -113,7 +113,11 @@ def load_case(path: str) -> Case:
 
 def load_all() -> list:
     return [load_case(p) for p in sorted(glob.glob(os.path.join(HERE, "*.bin")))
-            if os.path.basename(p) != "segments.bin"]
+            if os.path.basename(p) not in _NOT_CASES]
+
+
+# reference outputs beside the cases (not device views)
+_NOT_CASES = ("segments.bin", "clearance.bin", "geometry.bin")
 
 
 SEGMENT_DTYPE = np.dtype([("layer", "<u4"), ("pad", "<u4"), ("x0", "<i8"), ("y0", "<i8"),
@@ -139,3 +143,36 @@ def load_segments() -> list:
 def manifest() -> dict:
     with open(os.path.join(HERE, "manifest.json")) as f:
         return json.load(f)
+
+
+CLEARANCE_DTYPE = np.dtype([("start", "<i8", 2), ("end", "<i8", 2), ("box_min", "<i8", 2),
+                            ("box_max", "<i8", 2), ("width", "<i8"), ("clearance", "<i8"),
+                            ("error", "<u4"), ("satisfied", "<u4")])
+OBSTACLE_DTYPE = np.dtype([("min_x", "<i8"), ("min_y", "<i8"), ("max_x", "<i8"), ("max_y", "<i8"),
+                           ("layer", "<u4"), ("owned", "<u4")])
+
+
+def load_clearance() -> np.ndarray:
+    """Reference geometry::SweptTraceClearanceAtLeast verdicts on seeded
+    one-step segments and nearby boxes (oracle/ref_fixtures.cc)."""
+    r = _Reader(open(os.path.join(HERE, "clearance.bin"), "rb").read())
+    assert r.u64() == 0x3143524c43524741, "bad clearance magic"
+    n = r.u64()
+    return np.frombuffer(r.take(n * CLEARANCE_DTYPE.itemsize), CLEARANCE_DTYPE).copy()
+
+
+def load_geometry() -> dict:
+    """Per case name: the compile inputs of edge legality (heading mask,
+    routing width and clearance, lattice placement, obstacle boxes)."""
+    r = _Reader(open(os.path.join(HERE, "geometry.bin"), "rb").read())
+    assert r.u64() == 0x314f454754524741, "bad geometry magic"
+    names = [c["name"] for c in manifest()["cases"]]
+    out = {}
+    for _ in range(r.u64()):
+        case, heading = r.u32(), r.u32()
+        vals = np.frombuffer(r.take(40), "<i8")
+        obstacles = r.array(OBSTACLE_DTYPE)
+        out[names[case]] = dict(heading_mask=heading, width=int(vals[0]), clearance=int(vals[1]),
+                                origin=(int(vals[2]), int(vals[3])), step=int(vals[4]),
+                                obstacles=obstacles)
+    return out
