@@ -181,7 +181,13 @@ int main(int argc, char** argv) {
   check(std::get<BackendMetadata>(meta).compute_capability_major >= 10, "compute capability");
   std::vector<std::filesystem::path> files;
   for (const auto& e : std::filesystem::directory_iterator(dir)) {
-    if (e.path().extension() == ".bin") files.push_back(e.path());
+    // device-view cases only: the directory also holds reference outputs
+    // (segments, clearance verdicts, compile inputs) under other magics
+    if (e.path().extension() != ".bin") continue;
+    std::ifstream probe(e.path(), std::ios::binary);
+    std::uint64_t magic = 0;
+    probe.read(reinterpret_cast<char*>(&magic), sizeof(magic));
+    if (magic == 0x3158495446524741ull) files.push_back(e.path());
   }
   std::sort(files.begin(), files.end());
   std::size_t cases = 0, queries = 0;
