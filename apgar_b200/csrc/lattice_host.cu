@@ -91,6 +91,8 @@ constexpr uint64_t kMaxListEntries = 1ull << 22;
 // Frontier workspace above which nets share persistent slot slabs instead of
 // owning one slab each.
 constexpr uint64_t kPerNetFrontierBytes = 24ull << 30;
+// Budget of the persistent slot workspace (label words and queue lists).
+constexpr uint64_t kSlotFrontierBytes = 64ull << 30;
 
 struct PlanObject {
   LatticeObject* lattice = nullptr;
@@ -359,12 +361,35 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
       // slot slabs are spaced by the largest window plus a 4 KB skew, so that
       // equal offsets of different slots do not alias in the L2
       range.slab_cells += 512;
+    }
+    plan->classes.push_back(range);
+  }
+  if (frontier && per_net_cells * 20ull > kPerNetFrontierBytes) {
+    // Slot workspace within its budget: the class with the largest slot
+    // gives up half of its slots until the total fits (every class keeps at
+    // least one; fewer slots only means fewer of its nets in flight).
+    const auto slot_bytes = [](const ClassRange& c) { return c.slab_cells * 8ull + 12ull * c.list_cap; };
+    const auto total = [&]() {
+      uint64_t t = 0;
+      for (const ClassRange& c : plan->classes) t += c.slots * slot_bytes(c);
+      return t;
+    };
+    while (total() > kSlotFrontierBytes) {
+      ClassRange* widest = nullptr;
+      for (ClassRange& c : plan->classes) {
+        if (c.slots > 1 && (widest == nullptr || slot_bytes(c) > slot_bytes(*widest))) widest = &c;
+      }
+      if (widest == nullptr) break;
+      widest->slots = (widest->slots + 1) / 2;
+    }
+  }
+  if (frontier) {
+    for (ClassRange& range : plan->classes) {
       range.words_offset = dist_cells;
       dist_cells += static_cast<uint64_t>(range.slots) * range.slab_cells;
       range.lists_offset = arena_lists;
       arena_lists += static_cast<uint64_t>(range.slots) * 3ull * range.list_cap;
     }
-    plan->classes.push_back(range);
   }
   plan->label_cells = dist_cells;
   plan->arena_capacity = std::max<uint64_t>(arena_cells, 64);

@@ -278,6 +278,16 @@ def make_multi_terminal_nets(lat: Lattice, seed: int, count: int, hpwl_median: f
     return np.array(segs, dtype=NET_DTYPE), np.array(owner, dtype=np.int64)
 
 
+def config_full(seed: int = 5, nets: int = 32768, size: int = 8192, layers: int = 8):
+    """8 layers of 8192x8192 (30% blocked, rectangles + pad keep-outs), 32768
+    nets with 2-8 terminals split into 2-pin segments, half-perimeter
+    lognormal(400, 1.3), bbox + 32 windows; one routing resource per cell with
+    capacity 1 (the full-scale combined configuration)."""
+    lat = make_lattice(seed, layers, size, 0.30, pads=True)
+    segs, owner = make_multi_terminal_nets(lat, seed + 1000, nets, 400.0, 1.3, max_terminals=8)
+    return lat, segs, owner
+
+
 def config_negotiated(seed: int = 3, nets: int = 16384, size: int = 4096, layers: int = 6):
     """6 layers of 4096x4096 (25% blocked, rectangles + pad keep-outs as in the
     medium configuration), 16384 nets with 2-6 terminals split into 2-pin

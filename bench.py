@@ -61,10 +61,12 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-corridor form (reported beside the headline)")
-    ap.add_argument("--workload", choices=["medium", "negotiated"], default="medium",
+    ap.add_argument("--workload", choices=["medium", "negotiated", "full"], default="medium",
                     help="medium: the headline batch; negotiated: 10 rip-up/reroute rounds "
-                         "on the 6 x 4096^2 lattice with multi-terminal nets (one CUDA graph)")
-    ap.add_argument("--rounds", type=int, default=10)
+                         "on the 6 x 4096^2 lattice with multi-terminal nets (one CUDA graph); "
+                         "full: 20 rounds on the 8 x 8192^2 full-scale configuration")
+    ap.add_argument("--rounds", type=int, default=None,
+                    help="negotiated rounds (default 10, or 20 for the full workload)")
     ap.add_argument("--full-ripup", action="store_true",
                     help="negotiated: reroute every net each round (default: only nets "
                          "crossing overused cells after round 0)")
@@ -231,6 +233,10 @@ NEG_WORKLOAD = ("negotiated lattice: 6 layers x 4096x4096, 25% blocked (rectangl
                 "16384 nets with 2-6 terminals split into 2-pin segments along a Manhattan MST, "
                 "half-perimeter lognormal(median 300, sigma 1.2), bbox+32 windows, cell capacity 1, "
                 "prices 100/+100/+10 (reference defaults)")
+FULL_WORKLOAD = ("full-scale lattice: 8 layers x 8192x8192, 30% blocked (rectangles + pad keep-outs), "
+                 "32768 nets with 2-8 terminals split into 2-pin segments along a Manhattan MST, "
+                 "half-perimeter lognormal(median 400, sigma 1.3), bbox+32 windows, cell capacity 1, "
+                 "prices 100/+100/+10 (reference defaults)")
 
 
 def run_negotiated(args, rank, world, local):
@@ -242,7 +248,10 @@ def run_negotiated(args, rank, world, local):
     import apgar_b200
     from apgar_b200 import negotiate, prices, synth
 
-    lat, segs, _ = synth.config_negotiated(args.seed + 1)
+    full = args.workload == "full"
+    rounds = args.rounds if args.rounds is not None else (20 if full else 10)
+    args.rounds = rounds
+    lat, segs, _ = synth.config_full(args.seed + 3) if full else synth.config_negotiated(args.seed + 1)
     dev = apgar_b200.DeviceLattice(lat)
     plan = dev.plan(segs, generator="frontier")
     neg = negotiate.Negotiation(plan, prices.policy(capacity=1))
@@ -286,7 +295,8 @@ def run_negotiated(args, rank, world, local):
         "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic",
-        "config": {"workload": NEG_WORKLOAD, "segments": len(segs), "rounds": args.rounds,
+        "config": {"workload": FULL_WORKLOAD if full else NEG_WORKLOAD, "segments": len(segs),
+                   "rounds": args.rounds,
                    "form": "frontier search + fused snapshot prices, Jacobi rounds, one CUDA graph",
                    "rip_up": "full" if args.full_ripup else "partial (nets crossing overused cells)",
                    "workspace_bytes": plan.info()["workspace_bytes"]},
@@ -313,7 +323,7 @@ def main():
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
-    if args.workload == "negotiated":
+    if args.workload in ("negotiated", "full"):
         if world > 1 and rank > 0:
             return
         run_negotiated(args, rank, world, local)
