@@ -87,7 +87,7 @@ struct ClassRange {
 uint32_t default_chain(int) { return 0u; }
 
 // Queue entries per list per frontier slot (a net needing more is rejected).
-constexpr uint64_t kMaxListEntries = 1ull << 22;
+constexpr uint64_t kMaxListEntries = 1ull << 25;
 // Frontier workspace above which nets share persistent slot slabs instead of
 // owning one slab each.
 constexpr uint64_t kPerNetFrontierBytes = 24ull << 30;
