@@ -366,8 +366,8 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
   }
   if (frontier && per_net_cells * 20ull > kPerNetFrontierBytes) {
     // Slot workspace within its budget: the class with the largest slot
-    // gives up half of its slots until the total fits (every class keeps at
-    // least one; fewer slots only means fewer of its nets in flight).
+    // gives up an eighth of its slots until the total fits (every class keeps
+    // at least one; fewer slots only means fewer of its nets in flight).
     const auto slot_bytes = [](const ClassRange& c) { return c.slab_cells * 8ull + 12ull * c.list_cap; };
     const auto total = [&]() {
       uint64_t t = 0;
@@ -380,7 +380,7 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
         if (c.slots > 1 && (widest == nullptr || slot_bytes(c) > slot_bytes(*widest))) widest = &c;
       }
       if (widest == nullptr) break;
-      widest->slots = (widest->slots + 1) / 2;
+      widest->slots -= std::max<uint32_t>(1u, widest->slots / 8u);
     }
   }
   if (frontier) {
