@@ -3,7 +3,7 @@
 A corridor is a 64 x 64 bitmap of coarse cells over a net's window: coarse
 cell (cx, cy) covers window cells x in [cx << s, (cx + 1) << s) and y in
 [cy << s, (cy + 1) << s) on every layer, where s = coarse_shift(win_w, win_h)
-is the least value >= 2 that keeps both window sides within 64 coarse cells.
+is the least value >= 2 that keeps both window sides within 63 coarse cells.
 The device layout is 128 uint32 words per net, bit cx % 32 of word
 2 * cy + cx // 32 (``apgar_b200_lattice_plan_set_corridors``).
 
@@ -17,6 +17,7 @@ from __future__ import annotations
 import numpy as np
 
 COARSE = 64
+MAX_SPAN = 63  # coarse cells a window may span per side (the CNN's layout keeps column 63 empty)
 WORDS_PER_NET = 128
 
 NONE, CERTIFIED, FALLBACK_EXIT, FALLBACK_UNREACHED = 0, 1, 2, 3
@@ -28,7 +29,7 @@ def coarse_shift(win_w: int, win_h: int) -> int:
     """Coarse scale s of a window (the kernel's rule)."""
     span = max(int(win_w), int(win_h))
     s = 2
-    while ((span - 1) >> s) >= COARSE:
+    while ((span - 1) >> s) >= MAX_SPAN:
         s += 1
     return s
 

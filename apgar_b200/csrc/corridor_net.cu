@@ -147,8 +147,19 @@ __device__ __forceinline__ void tmem_load32(uint32_t taddr, float (&v)[32]) {
 __device__ __forceinline__ uint32_t dims_w(uint32_t d) { return d & 0xFFu; }
 __device__ __forceinline__ uint32_t dims_h(uint32_t d) { return (d >> 8) & 0xFFu; }
 
-__device__ __forceinline__ size_t cell_of(uint32_t net, int y, int x) {
+// Logits, labels: [net][64][64].
+__device__ __forceinline__ size_t grid_cell(uint32_t net, int y, int x) {
   return (static_cast<size_t>(net) * kGrid + static_cast<size_t>(y)) * kGrid + static_cast<size_t>(x);
+}
+
+// Rasters, activations and their gradients: [net][66][64][c], row y stored
+// at y + 1.  Rows -1 and 64 and, in rows 0 .. ch, the columns cw .. 63 hold
+// zeros (the producers write them), and cw <= 63, so a 3 x 3 tap that leaves
+// a row through its left or right end reads a zero or feeds an output outside
+// the window; rows and columns are then plain offsets of one 64-cell pitch.
+constexpr int kPadRows = kGrid + 2;
+__device__ __forceinline__ size_t act_cell(uint32_t net, int y, int x) {
+  return (static_cast<size_t>(net) * kPadRows + static_cast<size_t>(y + 1)) * kGrid + static_cast<size_t>(x);
 }
 
 __device__ __forceinline__ uint4 pack8(const float* v) {
@@ -183,7 +194,7 @@ __global__ void raster_kernel(LatticeDeviceView lat, const apgar_b200_lattice_ne
   const apgar_b200_lattice_net net = nets[n];
   const int w = static_cast<int>(net.win_w), h = static_cast<int>(net.win_h);
   int s = 2;
-  while ((((w > h ? w : h) - 1) >> s) >= kGrid) ++s;
+  while ((((w > h ? w : h) - 1) >> s) >= kGrid - 1) ++s;  // at most 63 coarse cells a side
   const int cw = (w + (1 << s) - 1) >> s, ch = (h + (1 << s) - 1) >> s;
   if (threadIdx.x == 0) dims[n] = static_cast<uint32_t>(cw) | (static_cast<uint32_t>(ch) << 8) |
                                   (static_cast<uint32_t>(s) << 16);
@@ -251,9 +262,15 @@ __global__ void raster_kernel(LatticeDeviceView lat, const apgar_b200_lattice_ne
       const float ex = fx - (scx + t * sgx), ey = fy - (scy + t * sgy);
       v[10] = fminf(sqrtf(ex * ex + ey * ey) / 8.f, 4.f);
     }
-    uint4* dst = reinterpret_cast<uint4*>(out + cell_of(n, cy, cx) * kCin0);
+    uint4* dst = reinterpret_cast<uint4*>(out + act_cell(n, cy, cx) * kCin0);
     dst[0] = pack8(v);
     dst[1] = pack8(v + 8);
+  }
+  // the zero pad rows above and below the grid
+  for (int c = threadIdx.x; c < 2 * kGrid; c += blockDim.x) {
+    uint4* dst = reinterpret_cast<uint4*>(out + act_cell(n, c < kGrid ? -1 : kGrid, c % kGrid) * kCin0);
+    dst[0] = make_uint4(0u, 0u, 0u, 0u);
+    dst[1] = make_uint4(0u, 0u, 0u, 0u);
   }
 }
 
@@ -323,7 +340,7 @@ __device__ __forceinline__ void stage_halo(const __nv_bfloat16* x, uint32_t net,
       const int c = rest % Halo<CIN>::kCols, r = rest / Halo<CIN>::kCols;
       const int sy = y0 - 1 + r, sx = c - 1;
       if (sx >= 0 && sy >= 0 && sx < cw && sy < ch) {
-        v[k] = __ldg(reinterpret_cast<const uint4*>(x + cell_of(net, sy, sx) * CIN) + j);
+        v[k] = __ldg(reinterpret_cast<const uint4*>(x + act_cell(net, sy, sx) * CIN) + j);
       }
     }
   }
@@ -341,25 +358,34 @@ __device__ __forceinline__ uint4 halo_chunk(const uint8_t* halo, int m, int t, i
   return reinterpret_cast<const uint4*>(halo)[(r * Halo<CIN>::kCols + c) * (CIN / 8) + j];
 }
 
+// The forward conv's operands.  A: the tile's four input rows (y0 - 1 ..
+// y0 + 2, 64 cells each) staged once as CIN / 8 planes of 16-byte chunks
+// (8 channels of one cell), one zero guard cell at each end of a plane.  The
+// A operand of tap (dy, dx) for the 128 output cells is the staged run that
+// starts at cell 1 + (1 + dy) * 64 + dx: K-major, 8-cell groups 128 bytes
+// apart (SBO), the two chunks of a K = 16 step one plane apart (LBO).  No
+// im2col copy.  B: the weights, [32 rows][9 * CIN], K-major.
 template <int CIN>
 struct ConvSmem {
   static constexpr int K = 9 * CIN;
-  static constexpr int kChunks = K / 8;          // 16-byte chunks per operand row
-  static constexpr int kSboA = kChunks * 128;    // bytes between 8-row groups
-  static constexpr int kBytesA = 16 * kSboA;     // 128 rows
-  static constexpr int kBytesB = 4 * kSboA;      // 32 rows
-  static constexpr int kBytes = kBytesA + kBytesB + Halo<CIN>::kBytes + 16;
+  static constexpr int kChunks = K / 8;                 // 16-byte chunks per B row
+  static constexpr int kSboB = kChunks * 128;           // bytes between 8-row groups of B
+  static constexpr int kBytesB = 4 * kSboB;             // 32 rows
+  static constexpr int kStageCells = 4 * kGrid + 2;     // 4 rows and two guards
+  static constexpr int kPlane = kStageCells * 16;       // bytes per channel-chunk plane
+  static constexpr int kBytesA = (CIN / 8) * kPlane;
+  static constexpr int kBytes = kBytesA + kBytesB + 16;
 };
 
 // out[cell][co] = epilogue(sum_{tap, ci} x[cell + tap][ci] * w[co][tap][ci]).
 template <int CIN, int EPI>
 __global__ void __launch_bounds__(128) conv3x3_tc_kernel(ConvArgs a) {
   using S = ConvSmem<CIN>;
+  constexpr int kPer = 4 * kGrid * (CIN / 8) / 128;  // staged chunks per thread
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* sa = smem;
   uint8_t* sb = smem + S::kBytesA;
-  uint8_t* halo = smem + S::kBytesA + S::kBytesB;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S::kBytesA + S::kBytesB + Halo<CIN>::kBytes);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S::kBytesA + S::kBytesB);
   __shared__ uint32_t tmem_slot;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
@@ -367,7 +393,13 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(ConvArgs a) {
   for (int u = tid; u < 32 * S::kChunks; u += 128) {
     const int n = u / S::kChunks, c = u % S::kChunks;
     const uint4 v = __ldg(reinterpret_cast<const uint4*>(a.w + static_cast<size_t>(n) * S::K) + c);
-    *reinterpret_cast<uint4*>(sb + (n % 8) * 16 + (n / 8) * S::kSboA + c * 128) = v;
+    *reinterpret_cast<uint4*>(sb + (n % 8) * 16 + (n / 8) * S::kSboB + c * 128) = v;
+  }
+  // the guard cells of every plane stay zero
+  if (tid < 2 * (CIN / 8)) {
+    const int j = tid >> 1;
+    *reinterpret_cast<uint4*>(sa + j * S::kPlane + ((tid & 1) ? (S::kStageCells - 1) * 16 : 0)) =
+        make_uint4(0u, 0u, 0u, 0u);
   }
   if (warp == 0) tmem_alloc(&tmem_slot, 32);
   if (tid == 0) bar_init(smem_addr(bar), 1);
@@ -386,16 +418,21 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(ConvArgs a) {
     const int y0 = static_cast<int>(item % (kGrid / 2)) * 2;
     const uint32_t d = a.dims[net];
     const int cw = static_cast<int>(dims_w(d)), ch = static_cast<int>(dims_h(d));
-    if (y0 >= ch) continue;  // uniform: no cell of these rows is in the window
-    stage_halo<CIN>(a.x, net, y0, cw, ch, halo, tid);
-    __syncthreads();
-    // im2col: A[m][tap * CIN + ci] for the 128 cells (rows y0, y0 + 1); rows
-    // of cells outside the window hold finite halo values and are not stored
-    for (int u = tid; u < 128 * 9 * (CIN / 8); u += 128) {
-      const int m = u % 128, r = u / 128;
-      const int j = r % (CIN / 8), t = r / (CIN / 8);
-      *reinterpret_cast<uint4*>(sa + (m % 8) * 16 + (m / 8) * S::kSboA + (t * (CIN / 8) + j) * 128) =
-          halo_chunk<CIN>(halo, m, t, j);
+    // rows up to ch are written (row ch as zeros: the next layer's taps read it)
+    if (y0 > ch) continue;  // uniform
+    // stage rows y0 - 1 .. y0 + 2: 256 contiguous cells of the padded tensor,
+    // every load of a thread in flight before its first store
+    {
+      const uint4* src = reinterpret_cast<const uint4*>(a.x + act_cell(net, y0 - 1, 0) * CIN);
+      uint4 v[kPer];
+#pragma unroll
+      for (int k = 0; k < kPer; ++k) v[k] = __ldg(src + tid + k * 128);
+#pragma unroll
+      for (int k = 0; k < kPer; ++k) {
+        const int u = tid + k * 128;
+        const int j = u % (CIN / 8), c = u / (CIN / 8);
+        *reinterpret_cast<uint4*>(sa + j * S::kPlane + (1 + c) * 16) = v[k];
+      }
     }
     fence_async_smem();
     __syncthreads();
@@ -403,9 +440,14 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(ConvArgs a) {
       fence_after_sync();
       const uint32_t a0 = smem_addr(sa), b0 = smem_addr(sb);
 #pragma unroll 1
-      for (int kk = 0; kk < S::K / 16; ++kk) {
-        mma_bf16(tmem, umma_desc(a0 + kk * 256, 128, S::kSboA), umma_desc(b0 + kk * 256, 128, S::kSboA),
-                 idesc, kk > 0 ? 1u : 0u);
+      for (int t = 0; t < 9; ++t) {
+        const int first = 1 + (1 + t / 3 - 1) * kGrid + (t % 3 - 1);  // staged cell of output 0
+#pragma unroll
+        for (int jj = 0; jj < CIN / 16; ++jj) {
+          const int kk = t * (CIN / 16) + jj;
+          mma_bf16(tmem, umma_desc(a0 + 2 * jj * S::kPlane + first * 16, S::kPlane, 128),
+                   umma_desc(b0 + kk * 256, 128, S::kSboB), idesc, kk > 0 ? 1u : 0u);
+        }
       }
       mma_commit(smem_addr(bar));
     }
@@ -416,13 +458,14 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(ConvArgs a) {
       break;
     }
     fence_after_sync();
-    // epilogue: thread = accumulator row = cell m
+    // epilogue: thread = accumulator row = cell m; cells outside the window
+    // are written as zeros (the layout's invariant)
     float v[32];
     tmem_load32(tmem + (static_cast<uint32_t>(warp * 32) << 16), v);
     const int m = warp * 32 + lane;
     const int py = y0 + m / kGrid, px = m % kGrid;
+    const size_t cell = act_cell(net, py, px);
     if (px < cw && py < ch) {
-      const size_t cell = cell_of(net, py, px);
       if constexpr (EPI == kEpiRelu) {
 #pragma unroll
         for (int c = 0; c < 32; ++c) v[c] = fmaxf(v[c] + __ldg(a.bias + c), 0.f);
@@ -436,9 +479,20 @@ __global__ void __launch_bounds__(128) conv3x3_tc_kernel(ConvArgs a) {
           for (int i = 0; i < 8; ++i) v[q * 8 + i] = gv[i] > 0.f ? v[q * 8 + i] : 0.f;
         }
       }
+    } else {
+#pragma unroll
+      for (int c = 0; c < 32; ++c) v[c] = 0.f;
+    }
+    if (py < kGrid) {
       uint4* dst = reinterpret_cast<uint4*>(a.y + cell * kCh);
 #pragma unroll
       for (int q = 0; q < 4; ++q) dst[q] = pack8(v + q * 8);
+    }
+    if (y0 == 0 && m < kGrid) {
+      // the zero pad row above the grid
+      uint4* pad = reinterpret_cast<uint4*>(a.y + act_cell(net, -1, m) * kCh);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) pad[q] = make_uint4(0u, 0u, 0u, 0u);
     }
     fence_before_sync();
     __syncthreads();
@@ -515,7 +569,7 @@ __global__ void __launch_bounds__(128) conv_wgrad_tc_kernel(WgradArgs a) {
       const int k = u % 128, j = u / 128;
       const int py = y0 + k / kGrid, px = k % kGrid;
       uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (px < cw && py < ch) v = __ldg(reinterpret_cast<const uint4*>(a.dy + cell_of(net, py, px) * kCh) + j);
+      if (px < cw && py < ch) v = __ldg(reinterpret_cast<const uint4*>(a.dy + act_cell(net, py, px) * kCh) + j);
       *reinterpret_cast<uint4*>(sb + (k % 8) * 16 + j * S::kSbo + (k / 8) * 128) = v;
     }
     // A: im2col rows (tap, ci) per cell, from the staged halo (cells outside
@@ -607,7 +661,7 @@ __global__ void head_forward_kernel(const __nv_bfloat16* __restrict__ act, const
       for (int t = 0; t < 9; ++t) {
         const int sy = y + t / 3 - 1, sx = x + t % 3 - 1;
         if (sx < 0 || sy < 0 || sx >= cw || sy >= ch) continue;
-        const uint4* src = reinterpret_cast<const uint4*>(act + cell_of(net, sy, sx) * kCh);
+        const uint4* src = reinterpret_cast<const uint4*>(act + act_cell(net, sy, sx) * kCh);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           float v[8];
@@ -672,7 +726,12 @@ __global__ void head_backward_kernel(const __nv_bfloat16* __restrict__ act, cons
     const int y = static_cast<int>((i / kGrid) % kGrid), x = static_cast<int>(i % kGrid);
     const uint32_t d = dims[net];
     const int cw = static_cast<int>(dims_w(d)), ch = static_cast<int>(dims_h(d));
-    if (x >= cw || y >= ch) continue;
+    if (y == 0) dact[act_cell(net, -1, x) * kCh + lane] = __float2bfloat16_rn(0.f);  // pad row
+    if (x >= cw || y >= ch) {
+      // the padded layout's zeros, through row ch (read by the next conv's taps)
+      if (y <= ch) dact[act_cell(net, y, x) * kCh + lane] = __float2bfloat16_rn(0.f);
+      continue;
+    }
     const float dl = dlogit[i];
     float da = 0.f;
 #pragma unroll
@@ -680,14 +739,14 @@ __global__ void head_backward_kernel(const __nv_bfloat16* __restrict__ act, cons
       const int dy = t / 3 - 1, dx = t % 3 - 1;
       // output cell (y - dy, x - dx) reads this cell through tap t
       const int oy = y - dy, ox = x - dx;
-      if (ox >= 0 && oy >= 0 && ox < cw && oy < ch) da = fmaf(wcol[t], dlogit[cell_of(net, oy, ox)], da);
+      if (ox >= 0 && oy >= 0 && ox < cw && oy < ch) da = fmaf(wcol[t], dlogit[grid_cell(net, oy, ox)], da);
       const int sy = y + dy, sx = x + dx;
       if (sx >= 0 && sy >= 0 && sx < cw && sy < ch) {
-        acc[t] = fmaf(dl, __bfloat162float(act[cell_of(net, sy, sx) * kCh + lane]), acc[t]);
+        acc[t] = fmaf(dl, __bfloat162float(act[act_cell(net, sy, sx) * kCh + lane]), acc[t]);
       }
     }
-    const float a = __bfloat162float(act[cell_of(net, y, x) * kCh + lane]);
-    dact[cell_of(net, y, x) * kCh + lane] = __float2bfloat16_rn(a > 0.f ? da : 0.f);
+    const float a = __bfloat162float(act[act_cell(net, y, x) * kCh + lane]);
+    dact[act_cell(net, y, x) * kCh + lane] = __float2bfloat16_rn(a > 0.f ? da : 0.f);
     bacc += dl;
   }
 #pragma unroll
@@ -828,7 +887,8 @@ cudaError_t launch_conv(const ConvArgs& a, int sm_count, cudaStream_t stream) {
                                        cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   if (e != cudaSuccess) return e;
   const uint32_t items = a.count * (kGrid / 2);
-  const uint32_t grid = min(items, static_cast<uint32_t>(max(sm_count, 1) * 2));
+  // ~35 KB of shared memory and 32 TMEM columns per CTA: four per SM
+  const uint32_t grid = min(items, static_cast<uint32_t>(max(sm_count, 1) * 4));
   if (grid == 0) return cudaSuccess;
   conv3x3_tc_kernel<CIN, EPI><<<grid, 128, bytes, stream>>>(a);
   return cudaGetLastError();

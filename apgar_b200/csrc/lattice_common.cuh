@@ -115,7 +115,7 @@ struct FrontierLaunch {
   // optional corridor mode: net n's corridor is the 64 x 64 coarse bitmap at
   // corridor + 128 * n (bit cx of word 2 * cy + cx / 32; a coarse cell covers
   // 2^s x 2^s window cells on every layer, s the least value >= 2 that keeps
-  // the window within 64 coarse cells per side); corridor_status[n] receives
+  // the window within 63 coarse cells per side); corridor_status[n] receives
   // the net's APGAR_B200_CORRIDOR_* outcome
   const uint32_t* corridor;
   uint8_t* corridor_status;

@@ -423,13 +423,13 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
     uint32_t* list_b = list_a + span;
     uint32_t* list_c = list_b + span;
 
-    // corridor: the coarse scale keeps the window within 64 x 64 coarse cells
+    // corridor: the coarse scale keeps the window within 63 x 63 coarse cells
     int cshift = 2;
     bool use_corr = false;
     uint32_t cstatus = 0;  // corridor outcome of this net (APGAR_B200_CORRIDOR_*)
     if constexpr (kCorr) {
       const int span_max = win.w > win.h ? win.w : win.h;
-      while (((span_max - 1) >> cshift) >= 64) ++cshift;
+      while (((span_max - 1) >> cshift) >= 63) ++cshift;  // at most 63 coarse cells a side
       const uint32_t* src = p.corridor + static_cast<size_t>(plan.net) * 128u;
       for (int i = tid; i < 128; i += T) corr[i] = __ldg(src + i);
       fsync<G>(barrier_id);

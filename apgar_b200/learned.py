@@ -24,6 +24,7 @@ import numpy as np
 from . import _check, lib
 
 GRID = 64
+PADDED_ROWS = GRID + 2  # rasters and activations carry a zero row above and below the grid
 RASTER_CHANNELS = 16
 CHANNELS = 32
 WEIGHTS_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "corridor_net.f32")
@@ -96,7 +97,7 @@ class CorridorNet:
     def activations(self, count: int, distinct: bool):
         t = self.torch
         n = 5 if distinct else 2
-        bufs = [t.empty((count, GRID, GRID, CHANNELS), dtype=t.bfloat16, device="cuda")
+        bufs = [t.empty((count, PADDED_ROWS, GRID, CHANNELS), dtype=t.bfloat16, device="cuda")
                 for _ in range(n)]
         return bufs if distinct else [bufs[i % 2] for i in range(5)]
 
@@ -155,7 +156,7 @@ def rasters(plan, cell_costs=None, stream: int = 0, out=None):
     if out is not None:
         r, d = out
     else:
-        r = torch.empty((n, GRID, GRID, RASTER_CHANNELS), dtype=torch.bfloat16, device="cuda")
+        r = torch.empty((n, PADDED_ROWS, GRID, RASTER_CHANNELS), dtype=torch.bfloat16, device="cuda")
         d = torch.empty(n, dtype=torch.uint32, device="cuda")
     costs = None if cell_costs is None else _ptr(cell_costs)
     _check(lib().apgar_b200_corridor_rasters(plan.handle, costs, _ptr(r), _ptr(d), ctypes.c_void_p(stream)))
@@ -207,7 +208,7 @@ class LearnedRouter:
         self.net = net if net is not None else CorridorNet.load()
         self.policy = policy if policy is not None else load_policy()
         n = len(plan.nets)
-        self.rasters = torch.empty((n, GRID, GRID, RASTER_CHANNELS), dtype=torch.bfloat16,
+        self.rasters = torch.empty((n, PADDED_ROWS, GRID, RASTER_CHANNELS), dtype=torch.bfloat16,
                                    device="cuda")
         self.dims = torch.empty(n, dtype=torch.uint32, device="cuda")
         self.acts = self.net.activations(n, distinct=False)

@@ -439,7 +439,7 @@ APGAR_B200_API int apgar_b200_lattice_plan_set_cell_costs(void* plan, const uint
  * 128 uint32 words per net of the plan: a 64 x 64 bitmap of coarse cells over
  * the net's window, bit cx of word 2 * cy + cx / 32 for coarse cell (cx, cy).
  * A coarse cell covers 2^s x 2^s window cells on every layer, where s is the
- * least value >= 2 with ceil(max(win_w, win_h) / 2^s) <= 64.  Each net first
+ * least value >= 2 with ceil(max(win_w, win_h) / 2^s) <= 63.  Each net first
  * searches its corridor only.  The result is kept when its cost is strictly
  * below the least key (label + move + admissible bound) over every legal
  * move leaving the corridor that the search expanded, which proves it equal
@@ -552,8 +552,10 @@ APGAR_B200_API int apgar_b200_compile_legal_edges(const apgar_b200_edge_rules* r
  * (mean entry price / 1024, capped at 8; 0 without prices), 3 start, 4 goal,
  * 5 inside the window, 6-9 coarse offsets to start and goal / 32, 10 distance
  * to the start-goal segment / 8 (capped at 4), 11-15 zero.
- * Tensors are device memory: rasters bf16 [count][64][64][16]; activations
- * bf16 [count][64][64][32]; logits and dlogit f32 [count][64][64]; labels u8
+ * Tensors are device memory: rasters bf16 [count][66][64][16]; activations
+ * bf16 [count][66][64][32] (grid row y stored at row y + 1, rows 0 and 65 and
+ * the cells outside each net's window zero, written by the producers);
+ * logits and dlogit f32 [count][64][64]; labels u8
  * [count][64][64]; dims u32 [count] (coarse width | height << 8 | scale << 16).
  * params f32 [apgar_b200_cnn_param_count()]: per layer l w[32][9][cin_l] then
  * b[32], then the head w6[9][32] and b6 (tap = (dy + 1) * 3 + dx + 1);

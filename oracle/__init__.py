@@ -338,7 +338,7 @@ def corridor_certificate(lat, net, mask):
     x0, y0 = int(n0["win_x0"]), int(n0["win_y0"])
     span = max(w, h)
     s = 2
-    while ((span - 1) >> s) >= 64:
+    while ((span - 1) >> s) >= 63:
         s += 1
     inside = np.asarray(mask, dtype=bool)[(np.arange(h) >> s)[:, None], (np.arange(w) >> s)[None, :]]
     sx, sy = int(n0["start_x"]) - x0, int(n0["start_y"]) - y0

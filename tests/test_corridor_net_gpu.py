@@ -23,6 +23,21 @@ def _bf16_to_np(t):
     return ref.from_bf16_bits(t.view(torch.int16).cpu().numpy().view(np.uint16))
 
 
+def _padded(t, channels, n, mask=None):
+    """A padded GPU tensor [n][66][64][c] as the grid [n][64][64][c]; checks
+    the layout's zeros (pad rows, and with a window mask the cells outside
+    the window through the row after it)."""
+    a = _bf16_to_np(t).reshape(n, 66, 64, channels)
+    assert not a[:, 0].any()
+    grid = a[:, 1:65]
+    if mask is not None:
+        below = np.zeros_like(mask)
+        below[:, 1:] = mask[:, :-1]
+        outside = ~mask & (mask.any(axis=2, keepdims=True) | below.any(axis=2, keepdims=True))
+        assert not grid[outside].any()
+    return grid
+
+
 def _u32(t):
     return t.view(torch.int32).cpu().numpy().view(np.uint32)
 
@@ -44,7 +59,7 @@ def test_rasters_match_restatement():
     lat, nets, dev, plan = _setup()
     try:
         r, d = learned.rasters(plan)
-        r = _bf16_to_np(r).reshape(len(nets), 64, 64, 16)
+        r = _padded(r, 16, len(nets))
         d = _u32(d)
         for i in range(len(nets)):
             s, cw, ch = corridor.coarse_dims(nets["win_w"][i], nets["win_h"][i])
@@ -96,8 +111,7 @@ def test_forward_and_backward_match_the_oracle():
         params = net.params.cpu().numpy()
         dims = _u32(d)
         mask = ref.valid_mask(dims)
-        x = [_bf16_to_np(r).reshape(-1, 64, 64, 16)] + \
-            [_bf16_to_np(a).reshape(-1, 64, 64, 32) for a in acts]
+        x = [_padded(r, 16, len(nets), mask)] + [_padded(a, 32, len(nets), mask) for a in acts]
         for layer in range(5):
             want = ref.conv_layer(x[layer], params, layer, mask)
             got = np.where(mask[..., None], x[layer + 1], 0.0)

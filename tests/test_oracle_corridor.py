@@ -28,11 +28,11 @@ def test_pack_roundtrip_and_layout():
     assert np.flatnonzero(w).tolist() == [2 * 7 + 1] and w[15] == 1 << (37 - 32)
 
 
-@pytest.mark.parametrize("w,h,s", [(1, 1, 2), (256, 10, 2), (257, 10, 3), (512, 600, 4),
-                                   (2048, 9, 5), (2049, 9, 6)])
+@pytest.mark.parametrize("w,h,s", [(1, 1, 2), (252, 10, 2), (253, 10, 3), (256, 10, 3),
+                                   (512, 600, 4), (2016, 9, 5), (2017, 9, 6)])
 def test_coarse_shift(w, h, s):
     assert corridor.coarse_shift(w, h) == s
-    assert -(-max(w, h) // (1 << s)) <= 64
+    assert -(-max(w, h) // (1 << s)) <= 63
 
 
 @pytest.mark.parametrize("seed", [11, 12])
