@@ -60,4 +60,19 @@ struct PathCheckLaunch {
   uint32_t query_count;
 };
 
+// Reachability of each selected query's goal under its policy bans.
+struct ReachLaunch {
+  const uint32_t* neighbors;  // [8][nodes]
+  const uint8_t* legal;       // [nodes]
+  uint32_t node_count;
+  const apgar_b200_batch_query_v1* queries;
+  const apgar_b200_policy_edge_v1* policy;
+  const uint32_t* selected;   // [count] query indices
+  uint32_t count;
+  uint32_t* visited;          // [count][ceil(nodes / 32)] scratch bits
+  uint32_t* queues;           // [count][2][nodes] scratch
+  uint32_t* reached;          // [count] 1 when the goal was reached
+  uint64_t* reach_nodes;      // [count] nodes reached
+};
+
 }  // namespace apgar_b200

@@ -33,6 +33,7 @@ namespace apgar_b200 {
 
 cudaError_t launch_graph_search(const GraphLaunch& launch, cudaStream_t stream);
 cudaError_t launch_validate_paths(const PathCheckLaunch& launch, cudaStream_t stream);
+cudaError_t launch_reach(const ReachLaunch& launch, cudaStream_t stream);
 cudaError_t launch_path_segments(const apgar_b200_node_v1* nodes, uint32_t node_count, int64_t ox,
                                  int64_t oy, int64_t step, const apgar_b200_compact_path_v1* paths,
                                  const uint32_t* states, uint64_t state_count, uint32_t count,
@@ -759,6 +760,116 @@ extern "C" int apgar_b200_validate_compact_paths(
     return APGAR_B200_OK;
   } catch (const std::bad_alloc&) {
     return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "host allocation failed during path validation");
+  }
+}
+
+// Device scratch of one reachability chunk (visited bits and two node lists
+// per query); larger batches run in several chunks.
+constexpr uint64_t kReachScratchBytes = 1ull << 30;
+
+extern "C" int apgar_b200_confirm_disconnected(
+    void* view, const apgar_b200_batch_query_v1* queries, uint32_t query_count,
+    const apgar_b200_policy_edge_v1* policy_edges, uint64_t policy_edge_count,
+    const apgar_b200_batch_result_v1* results, apgar_b200_disconnect_verdict* verdicts) {
+  if (view == nullptr || (query_count > 0 && (queries == nullptr || results == nullptr || verdicts == nullptr)) ||
+      (policy_edge_count > 0 && policy_edges == nullptr)) {
+    return invariant("disconnected confirmation received a null argument");
+  }
+  auto* v = static_cast<ViewObject*>(view);
+  if (int rc = check_device(v->device); rc != APGAR_B200_OK) return rc;
+  const uint64_t n = v->legal.size();
+  using u128 = unsigned __int128;
+  constexpr u128 kMaxFinite = static_cast<u128>(~0ull) - 1u;
+  std::vector<uint32_t> selected;
+  std::vector<u128> max_transition(query_count, 0);
+  for (uint32_t i = 0; i < query_count; ++i) {
+    verdicts[i] = apgar_b200_disconnect_verdict{APGAR_B200_DISCONNECT_NOT_CLAIMED, 0u, 0u};
+    if (results[i].completion != APGAR_B200_COMPLETION_DISCONNECTED) continue;
+    const apgar_b200_batch_query_v1& q = queries[i];
+    if (q.start_node >= n || q.goal_node >= n) {
+      return invariant("disconnected confirmation query names a node outside the view");
+    }
+    if (static_cast<uint64_t>(q.policy_offset) + q.policy_count > policy_edge_count) {
+      return invariant("disconnected confirmation query names policy edges outside the batch");
+    }
+    // the largest transition the query's CPU search can take
+    // (StepCostUnderPolicy, src/routing/candidate_policy.cc:419-438)
+    u128 penalty = 0;
+    const apgar_b200_policy_edge_v1* pol = policy_edges + q.policy_offset;
+    for (uint32_t e = 0; e < q.policy_count; ++e) {
+      if (e > 0 && pol[e].physical_edge_index <= pol[e - 1].physical_edge_index) {
+        return invariant("disconnected confirmation policy edges are not strictly sorted");
+      }
+      if (pol[e].adjustment != kGraphInf && pol[e].adjustment > penalty) penalty = pol[e].adjustment;
+    }
+    const u128 orth = static_cast<u128>(v->header.orthogonal_step) + q.orthogonal_step_surcharge;
+    const u128 diag = static_cast<u128>(v->header.diagonal_step) + q.diagonal_step_surcharge;
+    max_transition[i] = (orth > diag ? orth : diag) + v->header.bend + q.bend_surcharge + penalty;
+    selected.push_back(i);
+  }
+  if (selected.empty()) {
+    clear_error();
+    return APGAR_B200_OK;
+  }
+  try {
+    const uint64_t words = (n + 31u) / 32u;
+    const uint64_t per_query = words * 4u + 2u * n * 4u;
+    const uint64_t chunk = std::max<uint64_t>(1u, std::min<uint64_t>(selected.size(), kReachScratchBytes / per_query));
+    DeviceBuffer<apgar_b200_batch_query_v1> d_q;
+    DeviceBuffer<apgar_b200_policy_edge_v1> d_pol;
+    DeviceBuffer<uint32_t> d_sel, d_visited, d_queues, d_reached;
+    DeviceBuffer<uint64_t> d_nodes;
+    APGAR_B200_CUDA("cudaMalloc(queries)", d_q.ensure(query_count));
+    APGAR_B200_CUDA("cudaMalloc(policy)", d_pol.ensure(std::max<uint64_t>(policy_edge_count, 1)));
+    APGAR_B200_CUDA("cudaMalloc(selected)", d_sel.ensure(selected.size()));
+    APGAR_B200_CUDA("cudaMalloc(visited)", d_visited.ensure(chunk * words));
+    APGAR_B200_CUDA("cudaMalloc(queues)", d_queues.ensure(chunk * 2u * n));
+    APGAR_B200_CUDA("cudaMalloc(reached)", d_reached.ensure(selected.size()));
+    APGAR_B200_CUDA("cudaMalloc(reach nodes)", d_nodes.ensure(selected.size()));
+    APGAR_B200_CUDA("cudaMemcpy(queries)", cudaMemcpy(d_q.get(), queries, query_count * sizeof(*queries), cudaMemcpyHostToDevice));
+    if (policy_edge_count > 0) {
+      APGAR_B200_CUDA("cudaMemcpy(policy)", cudaMemcpy(d_pol.get(), policy_edges, policy_edge_count * sizeof(*policy_edges), cudaMemcpyHostToDevice));
+    }
+    APGAR_B200_CUDA("cudaMemcpy(selected)", cudaMemcpy(d_sel.get(), selected.data(), selected.size() * 4, cudaMemcpyHostToDevice));
+    for (uint64_t first = 0; first < selected.size(); first += chunk) {
+      ReachLaunch L{};
+      L.neighbors = v->neighbors.get();
+      L.legal = v->legal_dev.get();
+      L.node_count = static_cast<uint32_t>(n);
+      L.queries = d_q.get();
+      L.policy = d_pol.get();
+      L.selected = d_sel.get() + first;
+      L.count = static_cast<uint32_t>(std::min<uint64_t>(chunk, selected.size() - first));
+      L.visited = d_visited.get();
+      L.queues = d_queues.get();
+      L.reached = d_reached.get() + first;
+      L.reach_nodes = d_nodes.get() + first;
+      APGAR_B200_CUDA("reachability launch", launch_reach(L, nullptr));
+    }
+    std::vector<uint32_t> reached(selected.size());
+    std::vector<uint64_t> reach_nodes(selected.size());
+    APGAR_B200_CUDA("cudaMemcpy(reached)", cudaMemcpy(reached.data(), d_reached.get(), reached.size() * 4, cudaMemcpyDeviceToHost));
+    APGAR_B200_CUDA("cudaMemcpy(reach nodes)", cudaMemcpy(reach_nodes.data(), d_nodes.get(), reach_nodes.size() * 8, cudaMemcpyDeviceToHost));
+    for (size_t k = 0; k < selected.size(); ++k) {
+      const uint32_t i = selected[k];
+      apgar_b200_disconnect_verdict& out = verdicts[i];
+      out.reachable_nodes = reach_nodes[k];
+      if (reached[k] != 0u) {
+        out.code = APGAR_B200_DISCONNECT_REACHABLE;
+        continue;
+      }
+      // every reachable state's exact cost is at most (states - 1) transitions,
+      // so no checked add of the CPU search can leave the finite range when
+      // (8 * nodes + 1) * max transition stays finite
+      const u128 states = 8u * static_cast<u128>(reach_nodes[k]) + 1u;
+      const u128 t = max_transition[i];
+      const bool bounded = t == 0 || states <= kMaxFinite / t;
+      out.code = bounded ? APGAR_B200_DISCONNECT_CONFIRMED : APGAR_B200_DISCONNECT_UNBOUNDED;
+    }
+    clear_error();
+    return APGAR_B200_OK;
+  } catch (const std::bad_alloc&) {
+    return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "host allocation failed during disconnected confirmation");
   }
 }
 

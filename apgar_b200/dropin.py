@@ -55,6 +55,8 @@ VERDICT_DTYPE = np.dtype([("code", "<u4"), ("reserved", "<u4"), ("failing_index"
                           ("total_cost", "<u8")])
 PATH_CODES = {0: "ok", 1: "bounds", 2: "endpoint", 3: "cycle", 4: "heading", 5: "edge",
               6: "banned", 7: "not_reached"}
+DISCONNECT_VERDICT_DTYPE = np.dtype([("code", "<u4"), ("reserved", "<u4"), ("reachable_nodes", "<u8")])
+DISCONNECT_CODES = {0: "confirmed", 1: "reachable", 2: "unbounded", 3: "not_claimed"}
 ROUTE_HEADER_DTYPE = np.dtype([
     ("schema_version", "<u4"), ("compiler_version", "<u4"), ("start_node", "<u4"), ("goal_node", "<u4"),
     ("source_board_content_hash", "<u8"), ("compiler_profile_fingerprint", "<u8"),
@@ -191,6 +193,19 @@ class View:
             _vp(policy_edges) if len(policy_edges) else None, ctypes.c_uint64(len(policy_edges)),
             _vp(results), _vp(compact), _vp(states) if len(states) else None,
             ctypes.c_uint64(len(states)), _vp(out)))
+        return out
+
+    def confirm_disconnected(self, queries, policy_edges, results):
+        """Device confirmation of every DISCONNECTED result: one (code,
+        reachable nodes) record per query (codes in DISCONNECT_CODES)."""
+        queries = np.ascontiguousarray(queries)
+        policy_edges = np.ascontiguousarray(policy_edges)
+        results = np.ascontiguousarray(results)
+        out = np.zeros(len(queries), dtype=DISCONNECT_VERDICT_DTYPE)
+        _check(lib().apgar_b200_confirm_disconnected(
+            self.handle, _vp(queries), ctypes.c_uint32(len(queries)),
+            _vp(policy_edges) if len(policy_edges) else None, ctypes.c_uint64(len(policy_edges)),
+            _vp(results), _vp(out)))
         return out
 
     def path_segments(self, compact, states):

@@ -108,6 +108,7 @@ class ClockSampler:
     def __init__(self, device_index: int):
         self.device_index = device_index
         self.proc = None
+        self.skip = 0
         self.path = os.path.join("/tmp", f"apgar_b200_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
@@ -115,11 +116,25 @@ class ClockSampler:
             self.out = open(self.path, "w")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=self.out, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
+            return self
+        # nvidia-smi takes a moment to start: wait for its first row, then
+        # count only the rows written after this point (the timed region)
+        deadline = time.monotonic() + 3.0
+        while time.monotonic() < deadline and self._rows_written() == 0:
+            time.sleep(0.01)
+        self.skip = self._rows_written()
         return self
+
+    def _rows_written(self) -> int:
+        try:
+            with open(self.path) as f:
+                return sum(1 for line in f if line.count(",") >= 8)
+        except OSError:
+            return 0
 
     def __exit__(self, *exc):
         if self.proc is not None:
@@ -141,6 +156,7 @@ class ClockSampler:
                     continue
                 rows.append(parts)
         os.unlink(self.path)
+        rows = rows[self.skip:] or rows[-1:]
         if not rows:
             return None
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]

@@ -300,6 +300,39 @@ APGAR_B200_API int apgar_b200_validate_compact_paths(
     const apgar_b200_batch_result_v1* results, const apgar_b200_compact_path_v1* compact_paths,
     const uint32_t* path_states, uint64_t path_state_count, apgar_b200_path_verdict* verdicts);
 
+/* Confirmation of DISCONNECTED results on the device, in place of the CPU A*
+ * rerun of ConfirmDisconnectedWithCpuOracle (src/gpu/planar_router.cc:629-667).
+ * The CPU A* (src/routing/cpu_astar.cc:323-512) reports kDisconnected exactly
+ * when its queue empties without the goal: every state reachable from the
+ * start through compiled legal edges whose resource the query's policy does
+ * not ban has been expanded.  A per-query breadth-first search over the same
+ * edges decides that reachability.  The CPU search can instead fail with
+ * kResourceExhausted when a reachable state's cost plus a transition leaves
+ * the finite range; that cannot happen when (8 * reachable nodes + 1) times
+ * the query's largest finite transition stays below UINT64_MAX, and a query
+ * past that bound gets the code UNBOUNDED (confirm it on the CPU). */
+enum {
+  APGAR_B200_DISCONNECT_CONFIRMED = 0,   /* no path under the query's bans */
+  APGAR_B200_DISCONNECT_REACHABLE = 1,   /* gpu.disconnected.cpu_reachable.v1 */
+  APGAR_B200_DISCONNECT_UNBOUNDED = 2,   /* unreachable, but the cost bound cannot rule out
+                                            the CPU search's overflow failure */
+  APGAR_B200_DISCONNECT_NOT_CLAIMED = 3  /* the result is not DISCONNECTED: not checked */
+};
+typedef struct apgar_b200_disconnect_verdict {
+  uint32_t code;             /* APGAR_B200_DISCONNECT_* */
+  uint32_t reserved;
+  uint64_t reachable_nodes;  /* nodes reached from the start (a REACHABLE search stops at the goal) */
+} apgar_b200_disconnect_verdict;
+
+/* Confirms every DISCONNECTED result of a batch (host arrays, as read back)
+ * against an uploaded view and the batch's own queries and policy edges
+ * (each query's slice sorted by physical_edge_index); writes one verdict per
+ * query. */
+APGAR_B200_API int apgar_b200_confirm_disconnected(
+    void* view, const apgar_b200_batch_query_v1* queries, uint32_t query_count,
+    const apgar_b200_policy_edge_v1* policy_edges, uint64_t policy_edge_count,
+    const apgar_b200_batch_result_v1* results, apgar_b200_disconnect_verdict* verdicts);
+
 /* ======================= B. lattice mode ======================= */
 
 typedef struct apgar_b200_lattice_desc {

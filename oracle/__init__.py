@@ -253,6 +253,57 @@ def validate_compact(nodes, costs, start, goal, reverse_states, goal_state, comp
     return PATH_CODES[code], total.value, index.value
 
 
+DISCONNECT_CODES = {0: "confirmed", 1: "reachable", 2: "unbounded", 3: "not_claimed"}
+_U64_MAX = (1 << 64) - 1
+
+
+def disconnect_verdict(nodes, costs, start, goal, orth_s=0, diag_s=0, bend_s=0, policy=None):
+    """Confirmation of a DISCONNECTED claim for one query, restating what the
+    CPU A* rerun of ConfirmDisconnectedWithCpuOracle decides
+    (src/gpu/planar_router.cc:629-667; the search src/routing/cpu_astar.cc:
+    413-512): its queue empties without the goal exactly when the goal node
+    is unreachable over compiled legal edges whose canonical resource the
+    policy does not ban.  Level-by-level breadth-first search, stopping after
+    the level that reaches the goal.  An unreachable goal is "unbounded" when
+    (8 * reachable nodes + 1) x the largest transition (StepCostUnderPolicy,
+    src/routing/candidate_policy.cc:419-438) can leave the finite range
+    (CheckedAddFiniteRouteCost, src/routing/planar_route.cc:154-161).
+
+    Returns (code name, nodes reached)."""
+    orth, diag, bend = int(costs[0]), int(costs[1]), int(costs[2])
+    bans, penalty = set(), 0
+    if policy is not None:
+        for e in policy:
+            adj = int(e["adjustment"])
+            if adj == _U64_MAX:
+                bans.add(int(e["physical_edge_index"]))
+            else:
+                penalty = max(penalty, adj)
+    seen = {int(start)}
+    level = [int(start)]
+    found = int(start) == int(goal)
+    while level and not found:
+        nxt = []
+        for u in level:
+            legal = int(nodes[u]["legal_edges"])
+            for d in range(8):
+                if not (legal >> d) & 1:
+                    continue
+                v = int(nodes[u]["neighbors"][d])
+                edge = u * 8 + d if d < 4 else v * 8 + d - 4
+                if edge in bans or v in seen:
+                    continue
+                seen.add(v)
+                nxt.append(v)
+                found = found or v == int(goal)
+        level = nxt
+    if found:
+        return "reachable", len(seen)
+    t = max(orth + orth_s, diag + diag_s) + bend + bend_s + penalty
+    bounded = (8 * len(seen) + 1) * t <= _U64_MAX - 1
+    return ("confirmed" if bounded else "unbounded"), len(seen)
+
+
 def graph_predecessors(nodes, costs, start, labels, orth_s=0, diag_s=0, bend_s=0, policy=None):
     """Canonical predecessor of every state from exact labels."""
     L = lib()
