@@ -1257,6 +1257,7 @@ struct NegotiationObject {
   apgar_b200_price_policy policy{};
   uint64_t cells = 0;
   DeviceBuffer<uint32_t> usage, cell_cost, status;
+  uint32_t* usage_ext = nullptr;  // caller's usage buffer (multi-rank steps), or null
   DeviceBuffer<uint32_t> cell_cost_own;  // the snapshot seen from a net's own previous cells
   DeviceBuffer<uint32_t> own_bits;       // one bit per label word of the plan
   DeviceBuffer<uint64_t> history;
@@ -1272,6 +1273,10 @@ struct NegotiationObject {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   uint32_t graph_rounds = 0;
+  // split-round steps: the next (round, phase) a step may run
+  uint32_t step_round = 0, step_phase = 0;
+
+  uint32_t* usage_ptr() { return usage_ext != nullptr ? usage_ext : usage.get(); }
 
   ~NegotiationObject() {
     if (exec != nullptr) cudaGraphExecDestroy(exec);
@@ -1298,68 +1303,87 @@ bool checked_factor(const apgar_b200_price_policy& p, uint64_t epoch, uint64_t* 
   return true;
 }
 
-// Enqueues a whole negotiation (reset + `rounds` rounds) on n->work.  With
-// `partial`, round r >= 1 reroutes only the nets whose previous route did not
-// reach its goal or crosses a cell overused after round r - 1; the others
-// keep their routes.
-int enqueue_negotiation(NegotiationObject* n, uint32_t rounds, bool partial) {
-  cudaStream_t s = n->work;
+// Zero history and zero snapshot prices: the state before round 0.
+int enqueue_reset(NegotiationObject* n, cudaStream_t s) {
   APGAR_B200_CUDA("cudaMemsetAsync(history)",
                   cudaMemsetAsync(n->history.get(), 0, n->cells * sizeof(uint64_t), s));
   APGAR_B200_CUDA("cudaMemsetAsync(cell costs)",
                   cudaMemsetAsync(n->cell_cost.get(), 0, n->cells * sizeof(uint32_t), s));
   n->plan->cell_cost = n->cell_cost.get();
-  for (uint32_t r = 0; r < rounds; ++r) {
-    uint64_t factor = 0, next_factor = 0;
-    if (!checked_factor(n->policy, r, &factor) || !checked_factor(n->policy, r + 1ull, &next_factor)) {
-      return set_error(APGAR_B200_INTERNAL_INVARIANT, "present-price schedule overflowed uint64");
-    }
-    PlanObject* plan = n->plan;
-    // from round 1 on the previous round's routes drive rip-up pricing
-    plan->prev_results = r > 0 ? n->prev_results.get() : nullptr;
-    plan->prev_paths = r > 0 ? n->prev_paths.get() : nullptr;
-    plan->cell_cost_own = r > 0 ? n->cell_cost_own.get() : nullptr;
-    plan->own_bits = r > 0 ? n->own_bits.get() : nullptr;
-    if (partial && r > 0) {
-      APGAR_B200_CUDA("mark dirty launch",
-                      launch_mark_dirty(n->prev_results.get(), plan->count, n->prev_paths.get(),
-                                        n->usage.get(), n->cells,
-                                        static_cast<uint32_t>(n->policy.capacity), n->skip.get(),
-                                        plan->sm_count, s));
-      plan->skip = n->skip.get();
-    } else {
-      plan->skip = nullptr;
-    }
-    const int exec_rc = execute_plan(plan, s);
+  return APGAR_B200_OK;
+}
+
+// Steps 1-2 of round r: reroute the plan's nets against the current
+// snapshot, then count their per-cell usage.  With `partial`, round r >= 1
+// reroutes only the nets whose previous route did not reach its goal or
+// crosses a cell overused after round r - 1 (the usage buffer still holds
+// round r - 1's usage); the others keep their routes.
+int enqueue_route(NegotiationObject* n, uint32_t r, bool partial, cudaStream_t s) {
+  PlanObject* plan = n->plan;
+  if (r > 0) {
+    // the plan still holds round r - 1's routes: they drive rip-up pricing
+    APGAR_B200_CUDA("cudaMemcpyAsync(previous results)",
+                    cudaMemcpyAsync(n->prev_results.get(), plan->results.get(),
+                                    plan->count * sizeof(apgar_b200_lattice_result),
+                                    cudaMemcpyDeviceToDevice, s));
+    APGAR_B200_CUDA("cudaMemcpyAsync(previous paths)",
+                    cudaMemcpyAsync(n->prev_paths.get(), plan->paths.get(),
+                                    plan->arena_capacity * sizeof(uint32_t),
+                                    cudaMemcpyDeviceToDevice, s));
+  }
+  plan->cell_cost = n->cell_cost.get();
+  plan->prev_results = r > 0 ? n->prev_results.get() : nullptr;
+  plan->prev_paths = r > 0 ? n->prev_paths.get() : nullptr;
+  plan->cell_cost_own = r > 0 ? n->cell_cost_own.get() : nullptr;
+  plan->own_bits = r > 0 ? n->own_bits.get() : nullptr;
+  if (partial && r > 0) {
+    APGAR_B200_CUDA("mark dirty launch",
+                    launch_mark_dirty(n->prev_results.get(), plan->count, n->prev_paths.get(),
+                                      n->usage_ptr(), n->cells,
+                                      static_cast<uint32_t>(n->policy.capacity), n->skip.get(),
+                                      plan->sm_count, s));
+    plan->skip = n->skip.get();
+  } else {
     plan->skip = nullptr;
-    plan->prev_results = nullptr;
-    plan->prev_paths = nullptr;
-    plan->cell_cost_own = nullptr;
-    plan->own_bits = nullptr;
-    if (exec_rc != APGAR_B200_OK) return exec_rc;
-    if (r + 1 < rounds) {
-      APGAR_B200_CUDA("cudaMemcpyAsync(previous results)",
-                      cudaMemcpyAsync(n->prev_results.get(), plan->results.get(),
-                                      plan->count * sizeof(apgar_b200_lattice_result),
-                                      cudaMemcpyDeviceToDevice, s));
-      APGAR_B200_CUDA("cudaMemcpyAsync(previous paths)",
-                      cudaMemcpyAsync(n->prev_paths.get(), plan->paths.get(),
-                                      plan->arena_capacity * sizeof(uint32_t),
-                                      cudaMemcpyDeviceToDevice, s));
-    }
-    APGAR_B200_CUDA("cudaMemsetAsync(usage)",
-                    cudaMemsetAsync(n->usage.get(), 0, n->cells * sizeof(uint32_t), s));
-    APGAR_B200_CUDA("usage accumulation launch",
-                    launch_accumulate_cells(n->plan->results.get(), n->plan->count,
-                                            n->plan->paths.get(), n->usage.get(), n->cells,
-                                            n->plan->sm_count, s));
-    APGAR_B200_CUDA("price update launch",
-                    launch_price_update(static_cast<uint32_t>(n->cells), n->usage.get(), factor,
-                                        next_factor, n->policy.historical_price_increment,
-                                        n->policy.capacity, n->policy.maximum_value, nullptr,
-                                        n->history.get(), nullptr, nullptr, n->cell_cost.get(),
-                                        n->cell_cost_own.get(), n->status.get() + r,
-                                        n->stats.get() + 2ull * r, s));
+  }
+  const int exec_rc = execute_plan(plan, s);
+  plan->skip = nullptr;
+  plan->prev_results = nullptr;
+  plan->prev_paths = nullptr;
+  plan->cell_cost_own = nullptr;
+  plan->own_bits = nullptr;
+  if (exec_rc != APGAR_B200_OK) return exec_rc;
+  APGAR_B200_CUDA("cudaMemsetAsync(usage)",
+                  cudaMemsetAsync(n->usage_ptr(), 0, n->cells * sizeof(uint32_t), s));
+  APGAR_B200_CUDA("usage accumulation launch",
+                  launch_accumulate_cells(plan->results.get(), plan->count, plan->paths.get(),
+                                          n->usage_ptr(), n->cells, plan->sm_count, s));
+  return APGAR_B200_OK;
+}
+
+// Step 3 of round r: the fused price pass over the usage buffer.
+int enqueue_price(NegotiationObject* n, uint32_t r, cudaStream_t s) {
+  uint64_t factor = 0, next_factor = 0;
+  if (!checked_factor(n->policy, r, &factor) || !checked_factor(n->policy, r + 1ull, &next_factor)) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "present-price schedule overflowed uint64");
+  }
+  APGAR_B200_CUDA("price update launch",
+                  launch_price_update(static_cast<uint32_t>(n->cells), n->usage_ptr(), factor,
+                                      next_factor, n->policy.historical_price_increment,
+                                      n->policy.capacity, n->policy.maximum_value, nullptr,
+                                      n->history.get(), nullptr, nullptr, n->cell_cost.get(),
+                                      n->cell_cost_own.get(), n->status.get() + r,
+                                      n->stats.get() + 2ull * r, s));
+  return APGAR_B200_OK;
+}
+
+// Enqueues a whole negotiation (reset + `rounds` rounds) on n->work.
+int enqueue_negotiation(NegotiationObject* n, uint32_t rounds, bool partial) {
+  cudaStream_t s = n->work;
+  if (int rc = enqueue_reset(n, s); rc != APGAR_B200_OK) return rc;
+  for (uint32_t r = 0; r < rounds; ++r) {
+    if (int rc = enqueue_route(n, r, partial, s); rc != APGAR_B200_OK) return rc;
+    if (int rc = enqueue_price(n, r, s); rc != APGAR_B200_OK) return rc;
   }
   return APGAR_B200_OK;
 }
@@ -1456,6 +1480,79 @@ extern "C" int apgar_b200_negotiation_run_ex(void* negotiation, uint32_t rounds,
   return APGAR_B200_OK;
 }
 
+// Split-round steps cover up to this many rounds (the per-round stats are
+// sized once, at round 0).
+constexpr uint32_t kMaxStepRounds = 1000;
+
+extern "C" int apgar_b200_negotiation_set_usage_buffer(void* negotiation, uint32_t* usage_device) {
+  if (negotiation == nullptr) return set_error(APGAR_B200_INTERNAL_INVARIANT, "null negotiation");
+  auto* n = static_cast<NegotiationObject*>(negotiation);
+  if (int rc = check_device(n->plan->device); rc != APGAR_B200_OK) return rc;
+  if (usage_device != nullptr) {
+    cudaPointerAttributes attr{};
+    if (cudaPointerGetAttributes(&attr, usage_device) != cudaSuccess ||
+        attr.type != cudaMemoryTypeDevice || attr.device != n->plan->device) {
+      cudaGetLastError();
+      return set_error(APGAR_B200_INTERNAL_INVARIANT, "usage buffer is not device memory of the plan's device");
+    }
+  }
+  APGAR_B200_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(n->work));
+  n->usage_ext = usage_device;
+  if (n->exec != nullptr) {  // a captured run baked in the old buffer
+    cudaGraphExecDestroy(n->exec);
+    cudaGraphDestroy(n->graph);
+    n->exec = nullptr;
+    n->graph = nullptr;
+  }
+  clear_error();
+  return APGAR_B200_OK;
+}
+
+extern "C" int apgar_b200_negotiation_step(void* negotiation, uint32_t round, uint32_t phase,
+                                           uint32_t flags, void* stream) {
+  if (negotiation == nullptr || phase > APGAR_B200_NEGOTIATE_PRICE ||
+      (flags & ~APGAR_B200_NEGOTIATE_PARTIAL) != 0u) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "negotiation step needs a known phase and flags");
+  }
+  auto* n = static_cast<NegotiationObject*>(negotiation);
+  if (int rc = check_device(n->plan->device); rc != APGAR_B200_OK) return rc;
+  if (round >= kMaxStepRounds) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "negotiation steps cover rounds 0..999");
+  }
+  // round 0's route phase starts a new negotiation; otherwise phases alternate
+  const bool restart = round == 0 && phase == APGAR_B200_NEGOTIATE_ROUTE;
+  if (!restart && (round != n->step_round || phase != n->step_phase)) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "negotiation steps must alternate route and price in round order");
+  }
+  if (restart && n->rounds_capacity < kMaxStepRounds) {
+    APGAR_B200_CUDA("cudaMalloc(round status)", n->status.ensure(kMaxStepRounds));
+    APGAR_B200_CUDA("cudaMalloc(round stats)", n->stats.ensure(2ull * kMaxStepRounds));
+    n->rounds_capacity = kMaxStepRounds;
+  }
+  const auto caller = static_cast<cudaStream_t>(stream);
+  APGAR_B200_CUDA("cudaEventRecord(entry)", cudaEventRecord(n->entry, caller));
+  APGAR_B200_CUDA("cudaStreamWaitEvent", cudaStreamWaitEvent(n->work, n->entry, 0));
+  int rc = APGAR_B200_OK;
+  if (phase == APGAR_B200_NEGOTIATE_ROUTE) {
+    if (restart) rc = enqueue_reset(n, n->work);
+    if (rc == APGAR_B200_OK) {
+      rc = enqueue_route(n, round, (flags & APGAR_B200_NEGOTIATE_PARTIAL) != 0u, n->work);
+    }
+  } else {
+    rc = enqueue_price(n, round, n->work);
+  }
+  // the exit event is recorded even after a failed enqueue, so the caller's
+  // stream never runs ahead of work that was queued
+  const cudaError_t rec = cudaEventRecord(n->exit, n->work);
+  const cudaError_t wait = rec == cudaSuccess ? cudaStreamWaitEvent(caller, n->exit, 0) : rec;
+  if (rc != APGAR_B200_OK) return rc;
+  APGAR_B200_CUDA("cudaEventRecord(exit)", wait);
+  n->step_round = phase == APGAR_B200_NEGOTIATE_ROUTE ? round : round + 1;
+  n->step_phase = phase == APGAR_B200_NEGOTIATE_ROUTE ? APGAR_B200_NEGOTIATE_PRICE : APGAR_B200_NEGOTIATE_ROUTE;
+  clear_error();
+  return APGAR_B200_OK;
+}
+
 extern "C" int apgar_b200_negotiation_run(void* negotiation, uint32_t rounds, uint32_t use_graph,
                                           void* stream) {
   return apgar_b200_negotiation_run_ex(negotiation, rounds,
@@ -1473,7 +1570,7 @@ extern "C" int apgar_b200_negotiation_readback(void* negotiation, uint32_t* usag
     return set_error(APGAR_B200_INTERNAL_INVARIANT, "more rounds requested than were run");
   }
   APGAR_B200_CUDA("cudaStreamSynchronize", cudaStreamSynchronize(n->work));
-  if (usage) APGAR_B200_CUDA("cudaMemcpy(usage)", cudaMemcpy(usage, n->usage.get(), n->cells * 4, cudaMemcpyDeviceToHost));
+  if (usage) APGAR_B200_CUDA("cudaMemcpy(usage)", cudaMemcpy(usage, n->usage_ptr(), n->cells * 4, cudaMemcpyDeviceToHost));
   if (history) APGAR_B200_CUDA("cudaMemcpy(history)", cudaMemcpy(history, n->history.get(), n->cells * 8, cudaMemcpyDeviceToHost));
   if (cell_costs) APGAR_B200_CUDA("cudaMemcpy(cell costs)", cudaMemcpy(cell_costs, n->cell_cost.get(), n->cells * 4, cudaMemcpyDeviceToHost));
   if (rounds != nullptr && round_count > 0) {

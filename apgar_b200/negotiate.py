@@ -35,6 +35,7 @@ class Negotiation:
         self.policy = policy
         self.cells = plan.lattice.layers * plan.lattice.height * plan.lattice.width
         self.rounds = 0
+        self._usage_buffer = None
         handle = ctypes.c_void_p()
         _check(lib().apgar_b200_negotiation_create(plan.handle, ctypes.byref(policy),
                                                    ctypes.byref(handle)))
@@ -48,6 +49,44 @@ class Negotiation:
         _check(lib().apgar_b200_negotiation_run_ex(self.handle, ctypes.c_uint32(rounds),
                                                    ctypes.c_uint32(flags), ctypes.c_void_p(stream)))
         self.rounds = rounds
+
+    ROUTE, PRICE = 0, 1
+
+    def step(self, round_index: int, phase: int, stream: int = 0, partial: bool = False) -> None:
+        """One phase of one round of the split-round form: ROUTE (reroute this
+        plan's nets, count their usage; round 0 first zeroes history and
+        prices) or PRICE (the fused price pass over the usage buffer)."""
+        _check(lib().apgar_b200_negotiation_step(self.handle, ctypes.c_uint32(round_index),
+                                                 ctypes.c_uint32(phase),
+                                                 ctypes.c_uint32(2 if partial else 0),
+                                                 ctypes.c_void_p(stream)))
+        if phase == self.PRICE:
+            self.rounds = round_index + 1
+
+    def set_usage_buffer(self, usage) -> None:
+        """Counts usage into ``usage`` (a CUDA int32 tensor of one element per
+        lattice cell on the plan's device), or back into the negotiation's own
+        buffer with None."""
+        if usage is not None:
+            if (not usage.is_cuda or usage.numel() != self.cells or usage.element_size() != 4
+                    or not usage.is_contiguous()):
+                raise ValueError("usage buffer must be a contiguous 32-bit CUDA tensor of one entry per cell")
+        self._usage_buffer = usage  # kept alive while the negotiation uses it
+        _check(lib().apgar_b200_negotiation_set_usage_buffer(
+            self.handle, ctypes.c_void_p(usage.data_ptr() if usage is not None else None)))
+
+    def run_ranked(self, rounds: int, usage, sum_usage, stream: int = 0,
+                   partial: bool = False) -> None:
+        """This rank's share of a multi-GPU negotiation: the plan holds the
+        rank's segments; after each round's ROUTE, ``sum_usage(usage)`` sums
+        the usage tensor over all ranks in place (one integer all-reduce),
+        then every rank runs the same PRICE pass.  Jacobi rounds make the
+        ranks' routes exactly those of one plan over all segments."""
+        self.set_usage_buffer(usage)
+        for r in range(rounds):
+            self.step(r, self.ROUTE, stream, partial)
+            sum_usage(usage)
+            self.step(r, self.PRICE, stream, partial)
 
     def readback(self):
         """(usage, history, next snapshot prices, per-round stats list)."""

@@ -63,3 +63,18 @@ def allreduce_usage(usage, dist=None):
         return usage
     dist.all_reduce(usage)
     return usage
+
+
+def negotiate_ranked(negotiation, rounds: int, dist=None, partial: bool = True, stream: int = 0,
+                     device: str = "cuda"):
+    """Runs one rank's share of a negotiated-congestion run: ``negotiation``
+    holds this rank's segments (for example ``split_nets`` of the whole set);
+    each round sums the per-cell usage over all ranks with one all-reduce
+    (``allreduce_usage``) between the rank's ROUTE and PRICE steps."""
+    import torch
+
+    usage = torch.zeros(negotiation.cells, dtype=torch.int32, device=device)
+    negotiation.run_ranked(rounds, usage, lambda u: allreduce_usage(u, dist), stream=stream,
+                           partial=partial)
+    return usage
+

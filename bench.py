@@ -65,6 +65,9 @@ def parse_args():
                     help="medium: the headline batch; negotiated: 10 rip-up/reroute rounds "
                          "on the 6 x 4096^2 lattice with multi-terminal nets (one CUDA graph); "
                          "full: 20 rounds on the 8 x 8192^2 full-scale configuration")
+    ap.add_argument("--ranked", action="store_true",
+                    help="negotiated workloads: the multi-GPU split-round form (per-round NCCL "
+                         "all-reduce of usage) even on one GPU; it is the form used for N > 1")
     ap.add_argument("--rounds", type=int, default=None,
                     help="negotiated rounds (default 10, or 20 for the full workload)")
     ap.add_argument("--full-ripup", action="store_true",
@@ -333,6 +336,101 @@ def run_negotiated(args, rank, world, local):
         print(json.dumps(line), flush=True)
 
 
+def run_negotiated_ranked(args, rank, world, local):
+    """The negotiated workload on `world` GPUs: rank r takes every world-th
+    segment, and every round sums the per-cell usage over the ranks with one
+    NCCL all-reduce between its ROUTE and PRICE steps (strong scaling: the
+    total work is the single-GPU run's, and the routes are identical to it)."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                            device_id=torch.device("cuda", local))
+    import apgar_b200
+    from apgar_b200 import negotiate, prices, shard, synth
+
+    full = args.workload == "full"
+    rounds = args.rounds if args.rounds is not None else (20 if full else 10)
+    lat, segs, _ = synth.config_full(args.seed + 3) if full else synth.config_negotiated(args.seed + 1)
+    mine = shard.split_nets(segs, rank, world)
+    dev = apgar_b200.DeviceLattice(lat)
+    plan = dev.plan(mine, generator="frontier")
+    neg = negotiate.Negotiation(plan, prices.policy(capacity=1))
+    stream = torch.cuda.current_stream()
+    partial = not args.full_ripup
+    usage = torch.zeros(neg.cells, dtype=torch.int32, device="cuda")
+
+    def one_run(n):
+        n.run_ranked(rounds, usage, lambda u: shard.allreduce_usage(u, dist),
+                     stream=stream.cuda_stream, partial=partial)
+
+    for _ in range(max(args.warmup, 3)):
+        one_run(neg)
+    torch.cuda.synchronize()
+    dist.barrier()
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            one_run(neg)
+        end.record(stream)
+        torch.cuda.synchronize()
+    ms = shard.max_over_ranks(start.elapsed_time(end) / args.steps, dist, device="cuda")
+    _, _, _, rows = neg.readback()
+    res, _ = plan.readback()
+    # end to end: this rank's segments from the host, plan, ranked negotiation,
+    # results and paths back
+    dist.barrier()
+    e_start = torch.cuda.Event(enable_timing=True)
+    e_end = torch.cuda.Event(enable_timing=True)
+    e_runs = max(1, args.steps // 2)
+    e_start.record(stream)
+    for _ in range(e_runs):
+        p2 = dev.plan(mine, generator="frontier")
+        n2 = negotiate.Negotiation(p2, prices.policy(capacity=1))
+        one_run(n2)
+        r2, pa2 = p2.readback()
+        n2.close()
+        p2.close()
+    e_end.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = shard.max_over_ranks(e_start.elapsed_time(e_end) / e_runs, dist, device="cuda")
+    reached = shard.sum_over_ranks(int((res["completion"] == 0).sum()), dist, device="cuda")
+    d2h = shard.sum_over_ranks(int(len(mine) * apgar_b200.RESULT_DTYPE.itemsize + 4 * len(pa2)), dist,
+                               device="cuda")
+    routes = len(segs) * rounds
+    line = {
+        "metric": NEG_METRIC if world == 1 else NEG_METRIC.replace("on 1 B200", f"on {world} B200s"),
+        "value": routes / (ms / 1000.0), "unit": "routes/s", "n_gpus": world,
+        "steps": args.steps, "warmup": max(args.warmup, 3), "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u32",
+        "data": "synthetic",
+        "config": {"workload": FULL_WORKLOAD if full else NEG_WORKLOAD, "segments": len(segs),
+                   "rounds": rounds, "parallelism": f"segments split over {world} ranks",
+                   "form": "frontier search + fused snapshot prices, Jacobi rounds; one int32 "
+                           "all-reduce of per-cell usage per round (NCCL)",
+                   "rip_up": "full" if args.full_ripup else "partial (nets crossing overused cells)"},
+        "gpu_launches": rounds * (plan.info()["kernel_launches"] + 2) * args.steps,
+        "e2e": {"value": routes / (e2e_ms / 1000.0), "unit": "routes/s",
+                "h2d_bytes_per_step": int(segs.nbytes),
+                "d2h_bytes_per_step": d2h, "ms_per_step": e2e_ms},
+        "clocks": clocks.summary(),
+        "last_round_reached": reached,
+        "overuse_per_round": [[r["overused_cells"], r["total_overuse"]] for r in rows],
+    }
+    neg.close()
+    plan.close()
+    dev.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
 def main():
     args = parse_args()
     rank, world, local = dist_env()
@@ -340,9 +438,10 @@ def main():
         run_reference(args, rank, world)
         return
     if args.workload in ("negotiated", "full"):
-        if world > 1 and rank > 0:
-            return
-        run_negotiated(args, rank, world, local)
+        if world > 1 or args.ranked:
+            run_negotiated_ranked(args, rank, world, local)
+        else:
+            run_negotiated(args, rank, world, local)
         return
 
     import torch

@@ -719,6 +719,24 @@ APGAR_B200_API int apgar_b200_negotiation_run(void* negotiation, uint32_t rounds
 /* apgar_b200_negotiation_run with flags (run == run_ex with GRAPH or 0). */
 APGAR_B200_API int apgar_b200_negotiation_run_ex(void* negotiation, uint32_t rounds, uint32_t flags,
                                   void* stream);
+/* Split-round form, for one rank of a multi-GPU negotiation whose plan holds
+ * that rank's share of the segments.  Round r is two steps: ROUTE reroutes
+ * the plan's nets against the current snapshot and counts their per-cell
+ * usage (round 0's ROUTE first zeroes history and prices); the caller then
+ * sums the usage buffer over all ranks in place (one integer all-reduce);
+ * PRICE runs the fused price pass over the summed usage, identically on every
+ * rank.  Rounds are Jacobi, so R ranks give exactly the single-plan results.
+ * Steps alternate ROUTE, PRICE in round order from round 0 (rounds 0..999);
+ * flags: APGAR_B200_NEGOTIATE_PARTIAL only.  Work is ordered after `stream`
+ * and `stream` after the work. */
+enum { APGAR_B200_NEGOTIATE_ROUTE = 0, APGAR_B200_NEGOTIATE_PRICE = 1 };
+APGAR_B200_API int apgar_b200_negotiation_step(void* negotiation, uint32_t round, uint32_t phase,
+                                               uint32_t flags, void* stream);
+/* Makes the negotiation count usage into the caller's device buffer (one
+ * uint32 per lattice cell, on the plan's device), so that a collective can
+ * sum it in place between ROUTE and PRICE; NULL returns to the negotiation's
+ * own buffer. */
+APGAR_B200_API int apgar_b200_negotiation_set_usage_buffer(void* negotiation, uint32_t* usage_device);
 /* Waits for the negotiation; copies the last round's usage, the history,
  * the next snapshot prices (each optional, layers*height*width cells) and
  * per-round statistics. */

@@ -1,7 +1,8 @@
 """World-size-2 checks of the multi-GPU plumbing on CPU (gloo): net sharding,
-the timing / count reductions bench.py uses, and the usage sum of a
+the timing / count reductions bench.py uses, the usage sum of a
 negotiated-congestion round followed by identical price updates on every
-rank."""
+rank, and a whole ranked negotiation (split-round driver, CPU restatement in
+place of the GPU steps) equal to one plan over all nets."""
 
 import os
 import socket
@@ -13,7 +14,8 @@ import torch.distributed as dist
 import torch.multiprocessing as mp
 
 import oracle
-from apgar_b200 import shard, synth
+from apgar_b200 import negotiate, prices, shard, synth
+from tests.negotiation_cpu import CpuRank, cpu_rounds
 
 
 def _free_port():
@@ -80,3 +82,67 @@ def test_single_process_reductions_are_identities():
     assert shard.sum_over_ranks(7) == 7
     u = torch.arange(4)
     assert shard.allreduce_usage(u) is u
+
+
+class _CpuRankNegotiation(negotiate.Negotiation):
+    """The split-round negotiation of one rank with the CPU restatement in
+    place of the GPU steps, so the ranked driver (Negotiation.run_ranked and
+    shard.negotiate_ranked, the same code the GPU ranks run) is exercised over
+    gloo."""
+
+    def __init__(self, rank_state):
+        self.state = rank_state
+        self.cells = rank_state.cells
+        self.rounds = 0
+        self.handle = None
+        self.calls = []
+
+    def set_usage_buffer(self, usage):
+        self.buffer = usage
+
+    def step(self, round_index, phase, stream=0, partial=False):
+        self.calls.append((round_index, phase))
+        if phase == self.ROUTE:
+            self.buffer.copy_(torch.from_numpy(self.state.route(round_index, partial).astype(np.int32)))
+        else:
+            self.state.price(round_index, self.buffer.numpy().astype(np.uint64))
+            self.rounds = round_index + 1
+
+
+def _negotiation_case():
+    lat = synth.make_lattice(71, 2, 64, 0.15)
+    nets = synth.make_nets(lat, 72, 16, hpwl_median=30.0, hpwl_sigma=0.5, margin=8)
+    return lat, nets, prices.policy(initial=20, increment=20, history_increment=5, capacity=1)
+
+
+def _negotiation_worker(rank, world, port, rounds, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        lat, nets, pol = _negotiation_case()
+        state = CpuRank(lat, shard.split_nets(nets, rank, world), pol)
+        neg = _CpuRankNegotiation(state)
+        usage = shard.negotiate_ranked(neg, rounds, dist, partial=True, device="cpu")
+        out[rank] = dict(usage=usage.numpy().copy(), history=state.history.copy(),
+                         cost=state.cost.copy(), per_round=list(state.per_round),
+                         costs=np.asarray(state.costs).copy(), calls=list(neg.calls))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_negotiate_like_one_plan():
+    world, rounds = 2, 3
+    out = mp.Manager().dict()
+    mp.spawn(_negotiation_worker, args=(world, _free_port(), rounds, out), nprocs=world, join=True)
+    lat, nets, pol = _negotiation_case()
+    usage, history, cost, costs, _, per_round = cpu_rounds(lat, nets, pol, rounds, partial=True)
+    assert per_round[0][0] > 0  # congested
+    for rank in range(world):
+        r = out[rank]
+        assert np.array_equal(r["usage"].view(np.uint32), usage)
+        assert np.array_equal(r["history"], history)
+        assert np.array_equal(r["cost"], cost)
+        assert r["per_round"] == per_round
+        assert np.array_equal(r["costs"], costs[rank::world])
+        assert r["calls"] == [(i, p) for i in range(rounds) for p in (0, 1)]

@@ -14,60 +14,13 @@ import pytest
 import apgar_b200
 import oracle
 from apgar_b200 import negotiate, prices, synth
+from tests.negotiation_cpu import cpu_rounds
 
 pytestmark = pytest.mark.gpu
 
 
-def _snapshot32(usage, history, pol, epoch):
-    rc, snap = oracle.price_snapshot(usage, history, pol.capacity, epoch,
-                                     pol.initial_present_factor, pol.present_factor_increment,
-                                     pol.maximum_value)
-    assert rc == 0
-    return np.minimum(snap, 0x7FFFFFFF).astype(np.uint32)
-
-
 def _cpu_rounds(lat, nets, pol, rounds, partial=False):
-    cells = lat.layers * lat.height * lat.width
-    history = np.zeros(cells, np.uint64)
-    cost = np.zeros(cells, np.uint32)
-    cost_own = cost
-    per_round = []
-    costs = paths = usage = None
-    for r in range(rounds):
-        if r == 0:
-            costs, paths = oracle.dijkstra_batch(lat, nets, cell_cost=cost)
-        else:
-            if partial:
-                # reroute only nets that did not reach or cross an overused cell
-                idx = [i for i, (c, p) in enumerate(zip(costs, paths))
-                       if c == oracle.lo_inf() or (usage[p.astype(np.int64)] > pol.capacity).any()]
-            else:
-                idx = range(len(nets))
-            costs = costs.copy()
-            paths = list(paths)
-            for i in idx:
-                # the net's own previous cells are priced without its own use
-                mine = cost.copy()
-                if costs[i] != oracle.lo_inf():
-                    own = paths[i].astype(np.int64)
-                    mine[own] = cost_own[own]
-                c, p = oracle.dijkstra_batch(lat, nets[i:i + 1], cell_cost=mine)
-                costs[i] = c[0]
-                paths[i] = p[0]
-        usage = np.zeros(cells, np.uint64)
-        for c, p in zip(costs, paths):
-            if c != oracle.lo_inf():
-                np.add.at(usage, p.astype(np.int64), 1)
-        rc, _, history, _ = oracle.price_epoch_update(
-            usage, history, pol.capacity, r, pol.initial_present_factor,
-            pol.present_factor_increment, pol.historical_price_increment)
-        assert rc == 0
-        cost = _snapshot32(usage, history, pol, r + 1)
-        cost_own = _snapshot32(np.where(usage > 0, usage - 1, 0).astype(np.uint64), history, pol,
-                               r + 1)
-        over = np.where(usage > pol.capacity, usage - pol.capacity, 0)
-        per_round.append((int((over > 0).sum()), int(over.sum())))
-    return usage.astype(np.uint32), history, cost, costs, paths, per_round
+    return cpu_rounds(lat, nets, pol, rounds, partial)
 
 
 @pytest.mark.parametrize("partial", [False, True])
