@@ -68,13 +68,26 @@ class LatticeOptions(ctypes.Structure):
         ("max_iterations", ctypes.c_uint32),
         ("bucket_width", ctypes.c_uint32),
         ("chain", ctypes.c_uint32),
+        ("class_bounds", ctypes.c_uint32),
     ]
 
 
-def _options(generator: str, max_iterations: int, bucket_width: int, chain: int = 0) -> LatticeOptions:
+def class_bounds(*log2_limits: int) -> int:
+    """Packs the frontier width-class limits (log2 of the largest window, in
+    cells over all layers, of the 1-, 2-, 4- and 8-warp classes) into the
+    options word; no argument gives 0, the library default."""
+    if not log2_limits:
+        return 0
+    if len(log2_limits) != 4:
+        raise ValueError("four class limits (1, 2, 4 and 8 warps per net)")
+    return sum(int(b) << (8 * k) for k, b in enumerate(log2_limits))
+
+
+def _options(generator: str, max_iterations: int, bucket_width: int, chain: int = 0,
+             bounds: int = 0) -> LatticeOptions:
     if generator not in GENERATORS:
         raise BackendError(1, f"unknown lattice generator {generator!r}")
-    return LatticeOptions(GENERATORS[generator], max_iterations, bucket_width, chain)
+    return LatticeOptions(GENERATORS[generator], max_iterations, bucket_width, chain, bounds)
 
 
 class PlanInfo(ctypes.Structure):
@@ -161,6 +174,7 @@ class DeviceLattice:
 
     def __init__(self, lat):
         self.layers, self.height, self.width = lat.layers, lat.height, lat.width
+        self.orth, self.diag, self.via = int(lat.orth), int(lat.diag), int(lat.via)
         self._blocked = np.ascontiguousarray(lat.blocked, dtype=np.uint32)
         self._via = None if lat.via_ok is None else np.ascontiguousarray(lat.via_ok, np.uint32)
         desc = LatticeDesc(lat.layers, lat.height, lat.width, _vp(self._blocked), _vp(self._via),
@@ -183,13 +197,15 @@ class DeviceLattice:
     def route(self, nets: np.ndarray, max_sweeps: int = 4096, cancel: np.ndarray | None = None,
               want_paths: bool = True, path_capacity: int | None = None, out=None,
               generator: str = "sweep", max_rounds: int = 1 << 30, bucket_width: int = 0,
-              chain: int = 0):
+              chain: int = 0, class_bounds: int = 0, schedule=None):
         """Searches every net; returns (results record array, packed paths).
 
         ``generator`` is "sweep" (budget ``max_sweeps``) or "frontier"
         (budget ``max_rounds``, key level width ``bucket_width``, 0 = twice
         the largest move; ``chain``, 0 = the default per width class, n = up
-        to n - 1 chained expansions per queued cell).  ``out`` may supply
+        to n - 1 chained expansions per queued cell; ``class_bounds``, the
+        packed width-class limits of ``class_bounds()``, 0 = the default; or a
+        tuned ``schedule`` holding all three).  ``out`` may supply
         preallocated (results, paths) host arrays (pinned memory makes the
         transfers faster)."""
         nets = np.ascontiguousarray(nets)
@@ -208,7 +224,10 @@ class DeviceLattice:
                 _vp(cancel), _vp(results), _vp(paths) if want_paths else None,
                 ctypes.c_uint64(paths.size if want_paths else 0), ctypes.byref(total)))
         else:
-            opts = _options(generator, max_rounds, bucket_width, chain)
+            if schedule is not None:
+                bucket_width, chain, class_bounds = (schedule.bucket_width, schedule.chain,
+                                                     schedule.class_bounds)
+            opts = _options(generator, max_rounds, bucket_width, chain, class_bounds)
             _check(lib().apgar_b200_lattice_route_ex(
                 self.handle, _vp(nets), ctypes.c_uint32(count), ctypes.byref(opts),
                 _vp(cancel), _vp(results), _vp(paths) if want_paths else None,
@@ -240,8 +259,14 @@ class DeviceLattice:
         return results, paths[: total.value]
 
     def plan(self, nets: np.ndarray, max_sweeps: int = 4096, generator: str = "sweep",
-             max_rounds: int = 1 << 30, bucket_width: int = 0, chain: int = 0) -> "Plan":
-        return Plan(self, nets, max_sweeps, generator, max_rounds, bucket_width, chain)
+             max_rounds: int = 1 << 30, bucket_width: int = 0, chain: int = 0,
+             class_bounds: int = 0, schedule=None) -> "Plan":
+        """``schedule``: a frontier schedule (for example from
+        ``apgar_b200.autotune.tune``) whose bucket width, chain and class bounds
+        replace the three arguments."""
+        if schedule is not None:
+            bucket_width, chain, class_bounds = schedule.bucket_width, schedule.chain, schedule.class_bounds
+        return Plan(self, nets, max_sweeps, generator, max_rounds, bucket_width, chain, class_bounds)
 
 
 class Plan:
@@ -249,7 +274,7 @@ class Plan:
 
     def __init__(self, lattice: DeviceLattice, nets: np.ndarray, max_sweeps: int,
                  generator: str = "sweep", max_rounds: int = 1 << 30, bucket_width: int = 0,
-                 chain: int = 0):
+                 chain: int = 0, class_bounds: int = 0):
         self.lattice = lattice
         self.nets = np.ascontiguousarray(nets)
         self.generator = generator
@@ -259,7 +284,7 @@ class Plan:
                                                  ctypes.c_uint32(len(self.nets)),
                                                  ctypes.c_uint32(max_sweeps), ctypes.byref(handle)))
         else:
-            opts = _options(generator, max_rounds, bucket_width, chain)
+            opts = _options(generator, max_rounds, bucket_width, chain, class_bounds)
             _check(lib().apgar_b200_lattice_plan_ex(lattice.handle, _vp(self.nets),
                                                     ctypes.c_uint32(len(self.nets)),
                                                     ctypes.byref(opts), ctypes.byref(handle)))

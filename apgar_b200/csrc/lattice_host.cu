@@ -86,6 +86,10 @@ struct ClassRange {
 // so the extra expansions of a chain cost more than the rounds it saves.
 uint32_t default_chain(int) { return 0u; }
 
+// Default frontier width-class limits (log2 window cells of the 1-, 2-, 4-
+// and 8-warp classes), the autotuner's choice on the medium batch.
+constexpr uint32_t kDefaultClassBounds = 12u | (15u << 8) | (17u << 16) | (19u << 24);
+
 // Queue entries per list per frontier slot (a net needing more is rejected).
 constexpr uint64_t kMaxListEntries = 1ull << 25;
 // Frontier workspace above which nets share persistent slot slabs instead of
@@ -103,6 +107,7 @@ struct PlanObject {
   uint32_t generator = APGAR_B200_LATTICE_SWEEP;
   uint32_t bucket_width = 0;
   uint32_t chain = 0;    // FRONTIER: apgar_b200_lattice_options::chain
+  uint32_t class_bounds = kDefaultClassBounds;  // FRONTIER: log2 class limits, byte per class
   bool per_net = false;  // FRONTIER: one slab per net (else persistent slots)
   const uint32_t* cell_cost = nullptr;  // caller-owned device prices (frontier only)
   // partial rip-up (set by a negotiation): kept nets and their previous routes
@@ -188,14 +193,23 @@ int class_for_width(uint32_t width, int layers) {
 // when more warps share a round's cells; the thresholds (measured on the
 // medium batch: 4-layer windows of 10^4 to 10^7 cells) give every window
 // above 256k cells 16 warps.
-int frontier_class(uint64_t cells) {
-  // measured on the medium batch: 16-warp groups take a whole SM each, so
-  // they pay off only for the largest windows
-  if (cells <= (1ull << 12)) return 0;
-  if (cells <= (1ull << 15)) return 1;
-  if (cells <= (1ull << 17)) return 2;
-  if (cells <= (1ull << 20)) return 3;
+// `bounds` holds log2 of each class's largest window, one byte per class
+// (apgar_b200_lattice_options::class_bounds).
+int frontier_class(uint64_t cells, uint32_t bounds) {
+  for (int k = 0; k < 4; ++k) {
+    if (cells <= (1ull << ((bounds >> (8 * k)) & 0xFFu))) return k;
+  }
   return 4;
+}
+
+bool class_bounds_valid(uint32_t bounds) {
+  uint32_t prev = 0;
+  for (int k = 0; k < 4; ++k) {
+    const uint32_t b = (bounds >> (8 * k)) & 0xFFu;
+    if (b < 1 || b > 31 || b <= prev) return false;
+    prev = b;
+  }
+  return true;
 }
 
 // Guard-padded sweep planes from row-major bit planes `in`
@@ -251,7 +265,7 @@ std::vector<uint32_t> sweep_planes(const uint32_t* in, int planes, int height, i
 int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint32_t count,
                uint32_t max_sweeps, PlanObject* plan,
                uint32_t generator = APGAR_B200_LATTICE_SWEEP, uint32_t bucket_width = 0,
-               uint32_t chain = 0) {
+               uint32_t chain = 0, uint32_t class_bounds = 0) {
   const LatticeDeviceView& v = lat->view;
   const bool frontier = generator == APGAR_B200_LATTICE_FRONTIER;
   plan->lattice = lat;
@@ -264,6 +278,7 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
   // left the far list never returns to it, so its far bit needs no clearing).
   plan->bucket_width = std::max(bucket_width, 2u * std::max(v.orth, std::max(v.diag, v.via)));
   plan->chain = chain;
+  plan->class_bounds = class_bounds != 0 ? class_bounds : kDefaultClassBounds;
   APGAR_B200_CUDA("cudaDeviceGetAttribute",
                   cudaDeviceGetAttribute(&plan->sm_count, cudaDevAttrMultiProcessorCount,
                                          lat->device));
@@ -291,7 +306,7 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
     if (frontier) {
       // packed queue entries hold x and y in 14 bits each
       if (n.win_w > 16384u || n.win_h > 16384u) continue;
-      members[frontier_class(cells)].push_back(i);
+      members[frontier_class(cells, plan->class_bounds)].push_back(i);
       continue;
     }
     const uint32_t frame_width = std::max(n.win_w, n.win_h);
@@ -862,6 +877,10 @@ int check_options(const apgar_b200_lattice_options& o) {
       return set_error(APGAR_B200_INTERNAL_INVARIANT, "frontier budget must be 1..2^30 rounds");
     }
     if (o.chain > 16) return set_error(APGAR_B200_INTERNAL_INVARIANT, "frontier chain must be 0..16");
+    if (o.class_bounds != 0 && !class_bounds_valid(o.class_bounds)) {
+      return set_error(APGAR_B200_INTERNAL_INVARIANT,
+                       "frontier class bounds must be strictly increasing log2 sizes in 1..31");
+    }
     return APGAR_B200_OK;
   }
   return set_error(APGAR_B200_UNSUPPORTED, "unknown lattice generator");
@@ -882,7 +901,7 @@ int route_impl(void* lattice, const apgar_b200_lattice_net* nets, uint32_t count
     if (lat->route_plan == nullptr) lat->route_plan = std::make_unique<PlanObject>();
     PlanObject* plan = lat->route_plan.get();
     if (int rc = build_plan(lat, nets, count, o.max_iterations, plan, o.generator, o.bucket_width,
-                            o.chain);
+                            o.chain, o.class_bounds);
         rc != APGAR_B200_OK) {
       return rc;
     }
@@ -916,7 +935,7 @@ extern "C" int apgar_b200_lattice_route(void* lattice, const apgar_b200_lattice_
                                         const volatile uint32_t* cancel,
                                         apgar_b200_lattice_result* results, uint32_t* paths,
                                         uint64_t path_capacity, uint64_t* path_total) {
-  const apgar_b200_lattice_options o{APGAR_B200_LATTICE_SWEEP, max_sweeps, 0, 0};
+  const apgar_b200_lattice_options o{APGAR_B200_LATTICE_SWEEP, max_sweeps, 0, 0, 0};
   return route_impl(lattice, nets, count, o, cancel, results, paths, path_capacity, path_total);
 }
 
@@ -943,7 +962,8 @@ extern "C" int apgar_b200_lattice_plan_ex(void* lattice, const apgar_b200_lattic
   try {
     auto plan = std::make_unique<PlanObject>();
     if (int rc = build_plan(lat, nets, count, options->max_iterations, plan.get(),
-                            options->generator, options->bucket_width, options->chain);
+                            options->generator, options->bucket_width, options->chain,
+                            options->class_bounds);
         rc != APGAR_B200_OK) {
       return rc;
     }

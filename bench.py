@@ -35,6 +35,15 @@ import time
 
 import numpy as np
 
+# One hardware work queue per process (read when the CUDA context is created,
+# so before torch touches the GPU): the width classes of a plan run as
+# concurrent persistent kernels on forked streams, and with several queues
+# their CTAs can reach the SMs in any order, so narrow classes sometimes fill
+# the SMs before the 16-warp class and delay the longest nets (measured: 18 to
+# 26 ms for the same batch).  With one queue the CTAs dispatch in launch
+# order, widest class first, and the time per batch stays within 1%.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "1")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -65,6 +74,9 @@ def parse_args():
                     help="medium: the headline batch; negotiated: 10 rip-up/reroute rounds "
                          "on the 6 x 4096^2 lattice with multi-terminal nets (one CUDA graph); "
                          "full: 20 rounds on the 8 x 8192^2 full-scale configuration")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="medium workload: skip the (untimed) frontier schedule autotuner and use "
+                         "the library's default schedule")
     ap.add_argument("--ranked", action="store_true",
                     help="negotiated workloads: the multi-GPU split-round form (per-round NCCL "
                          "all-reduce of usage) even on one GPU; it is the form used for N > 1")
@@ -188,7 +200,7 @@ def certified(results):
 
 
 def algorithmic_bytes(lat, nets, results):
-    """Bytes the sweep schedule must move (see the DESIGN roofline section).
+    """Bytes the sweep schedule must move.
 
     Per processed window row: the layer rows read and written (4 B per cell of
     the window width) plus the obstacle and via bits (2 bits per cell per
@@ -474,9 +486,19 @@ def main():
     def sum_over_ranks(n):
         return shard.sum_over_ranks(n, dist, device="cuda")
 
+    # ---------------- frontier schedule (autotuned, untimed) ----------------
+    from apgar_b200 import autotune
+
+    if args.no_tune:
+        schedule, tuning = autotune.DEFAULT, []
+    else:
+        schedule, tuning = autotune.tune(dev, nets)
+    barrier()
+
     def device_resident(generator, sample_clocks):
         """K executions of a resident plan, CUDA events on torch's stream."""
-        plan = dev.plan(nets, generator=generator)
+        plan = dev.plan(nets, generator=generator,
+                        schedule=schedule if generator == "frontier" else None)
         info = plan.info()
         for _ in range(max(args.warmup, 3)):
             plan.execute(stream.cuda_stream)
@@ -515,7 +537,7 @@ def main():
     if not args.no_learned:
         from apgar_b200 import learned
 
-        lplan = dev.plan(nets, generator="frontier")
+        lplan = dev.plan(nets, generator="frontier", schedule=schedule)
         router = learned.LearnedRouter(lplan)
         for _ in range(max(args.warmup, 3)):
             router.execute(stream.cuda_stream)
@@ -562,14 +584,15 @@ def main():
     path_host = torch.empty(int(info["path_arena_capacity"]), dtype=torch.int32).pin_memory()
     path_arr = path_host.numpy().view(np.uint32)
     for _ in range(2):
-        dev.route(nets_host, out=(res_arr, path_arr), generator="frontier")
+        dev.route(nets_host, out=(res_arr, path_arr), generator="frontier", schedule=schedule)
     barrier()
     e_start = torch.cuda.Event(enable_timing=True)
     e_end = torch.cuda.Event(enable_timing=True)
     path_cells = 0
     e_start.record()
     for _ in range(args.steps):
-        r, p = dev.route(nets_host, out=(res_arr, path_arr), generator="frontier")
+        r, p = dev.route(nets_host, out=(res_arr, path_arr), generator="frontier",
+                         schedule=schedule)
         path_cells = len(p)
     e_end.record()
     barrier()
@@ -601,6 +624,9 @@ def main():
                 "seed": args.seed, "parallelism": f"weak x{world} (independent net batches)",
                 "l2": "label words (5.4 GB) larger than L2 (126 MB) and cleared every step",
                 "certified_per_step": cert_all,
+                "schedule": dict(schedule.describe(),
+                                 chosen_by="autotuner (untimed, on this batch)" if tuning else "default"),
+                "tuning_ms": [[row[0], row[1]] for row in tuning],
             },
             "gpu_launches": int(info["kernel_launches"]) * args.steps,
             "roofline": {

@@ -456,6 +456,12 @@ typedef struct apgar_b200_lattice_options {
                               queued cell is followed within its round by up to n - 1
                               chained expansions of the least-key cell it queued
                               (1 = none); at most 16.  Results do not depend on it. */
+  uint32_t class_bounds;   /* FRONTIER: width classes of 1, 2, 4, 8 and 16 warps per net;
+                              byte k (k = 0..3) is log2 of the largest window (cells over
+                              all layers) of the 2^k-warp class, strictly increasing in
+                              1..31; larger windows take 16 warps.  0 = the default
+                              0x13110F0C (2^12, 2^15, 2^17, 2^19).  Results do not
+                              depend on it. */
 } apgar_b200_lattice_options;
 
 /* Per-cell entry prices for a FRONTIER plan (no reference counterpart at this
