@@ -125,6 +125,16 @@ struct FrontierLaunch {
   uint32_t chain;
 };
 
+// Threads of a frontier CTA: one 16-warp group, which splits down to single
+// warps as the width classes drain.
+constexpr int kFrontierThreads = 512;
+
+// The width classes of one frontier execution, by warps per net 1, 2, 4, 8
+// and 16 (a class with no slots or no nets is skipped).
+struct FrontierClasses {
+  FrontierLaunch c[5];
+};
+
 __device__ __forceinline__ uint32_t sat(uint32_t v) { return v < kLabelInf ? v : kLabelInf; }
 
 // 32 bits of a bit-packed row starting at signed bit position `pos`; bits

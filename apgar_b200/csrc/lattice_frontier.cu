@@ -86,8 +86,6 @@ constexpr int kCancelPollRounds = 256;
 // No chained expansion follows (a packed cell never has all bits set).
 constexpr uint32_t kNoLink = 0xFFFFFFFFu;
 
-__host__ __device__ constexpr int frontier_groups_per_block(int G) { return G >= 4 ? 1 : 4 / G; }
-
 __device__ __forceinline__ uint32_t pack_cell(int l, int x, int y) {
   return (static_cast<uint32_t>(l) << 28) | (static_cast<uint32_t>(y) << 14) |
          static_cast<uint32_t>(x);
@@ -337,29 +335,24 @@ struct GroupShared {
   uint32_t sums[16];
 };
 
+// One warp group of G warps works through the nets of one width class until
+// the class's work-stealing cursor runs past its last net, then returns.
+// g: the warp's index within the group; barrier_id: the group's named
+// barrier (unused for G = 1); sh and corr: the group's own shared state.
 // kPriced: the plan carries per-cell entry prices (p.cell_cost != nullptr);
 // the unpriced instantiation has no price loads or overflow tests at all.
 // kCorr: corridor mode (p.corridor != nullptr), unpriced only.
 template <int G, bool kPriced, bool kCorr>
-__global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
-    lattice_frontier_kernel(FrontierLaunch p) {
+__device__ __forceinline__ void frontier_group(const FrontierLaunch& p, uint32_t slot, int g,
+                                               int barrier_id, GroupShared& sh,
+                                               uint32_t* const corr) {
   static_assert(!(kPriced && kCorr), "corridor mode is unpriced");
-  constexpr int kGroups = frontier_groups_per_block(G);
   constexpr int T = G * 32;
-  __shared__ GroupShared shared_groups[kGroups];
-  __shared__ uint32_t corridor_bits[kCorr ? kGroups * 128 : 1];
-  const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  const int gi = warp / G;
-  const int g = warp - gi * G;
   const int tid = g * 32 + lane;
-  const int barrier_id = gi + 1;
-  GroupShared& sh = shared_groups[gi];
-  uint32_t* const corr = corridor_bits + (kCorr ? gi * 128 : 0);
   const LatticeDeviceView& lat = p.lat;
   const uint32_t orth = lat.orth, diag = lat.diag, via = lat.via;
-  const uint32_t slot = blockIdx.x * kGroups + gi;
-  if (slot >= p.slots) return;  // whole group: no workspace slot of its own
+  if (slot >= p.slots) return;  // whole group: no workspace slot of its own in this class
   unsigned long long* const slot_words = p.words + static_cast<uint64_t>(slot) * p.slab_cells;
   uint32_t* const slot_lists = p.lists + static_cast<uint64_t>(slot) * 3u * p.list_cap;
   const uint32_t cap = p.list_cap;
@@ -770,43 +763,74 @@ __global__ void __launch_bounds__(frontier_groups_per_block(G) * G * 32)
   }
 }
 
-template <int G>
-cudaError_t resident_groups_g(int sm_count, uint32_t* out) {
-  // slots for the leaner instantiation: with the other, groups beyond the
-  // resident ones start as others finish (no group waits on another) and find
-  // the work-stealing queue drained
-  constexpr int kGroups = frontier_groups_per_block(G);
-  int plain = 0, priced = 0, corridor = 0;
-  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-      &plain, lattice_frontier_kernel<G, false, false>, kGroups * G * 32, 0);
-  if (e == cudaSuccess) {
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &priced, lattice_frontier_kernel<G, true, false>, kGroups * G * 32, 0);
-  }
-  if (e == cudaSuccess) {
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &corridor, lattice_frontier_kernel<G, false, true>, kGroups * G * 32, 0);
-  }
-  if (e != cudaSuccess) return e;
-  *out = static_cast<uint32_t>(max(1, max(plain, max(priced, corridor))) * max(1, sm_count) *
-                               kGroups);
-  return cudaSuccess;
+// Group state of every (width, first warp) pair a CTA can hold: the 16-warp
+// group, two 8-warp groups, four 4-warp, eight 2-warp and sixteen 1-warp
+// groups (31 in all).  A group that splits hands over to its halves while
+// they may still read its state, so no two of them share an entry.
+__host__ __device__ constexpr int group_entry(int G, int w0) {
+  return (G == 16 ? 0 : G == 8 ? 1 : G == 4 ? 3 : G == 2 ? 7 : 15) + w0 / G;
 }
 
-template <int G>
-cudaError_t launch_frontier_g(const FrontierLaunch& launch, cudaStream_t stream) {
-  constexpr int kGroups = frontier_groups_per_block(G);
-  // one group per workspace slot; the host sizes slots to the resident groups
-  const unsigned grid = (launch.slots + kGroups - 1) / kGroups;
-  if (launch.cell_cost != nullptr && launch.corridor != nullptr) return cudaErrorInvalidValue;
-  if (launch.cell_cost != nullptr) {
-    lattice_frontier_kernel<G, true, false><<<grid, kGroups * G * 32, 0, stream>>>(launch);
-  } else if (launch.corridor != nullptr) {
-    lattice_frontier_kernel<G, false, true><<<grid, kGroups * G * 32, 0, stream>>>(launch);
-  } else {
-    lattice_frontier_kernel<G, false, false><<<grid, kGroups * G * 32, 0, stream>>>(launch);
+// The whole frontier of a plan in one persistent launch of 16-warp CTAs.
+// Each CTA first serves the widest class as one 16-warp group; when that
+// class's cursor is past its last net, the group splits into two 8-warp
+// groups that serve the next class, and so on down to single warps.  So the
+// widest nets (the batch's critical path) always start first, and a finished
+// group's warps move on to narrower nets without waiting for the rest of the
+// CTA.  Named barriers: 1 for the 16-warp group, 2-3, 4-7 and 8-15 for the
+// 8-, 4- and 2-warp groups (single warps use __syncwarp).
+template <bool kPriced, bool kCorr>
+__global__ void __launch_bounds__(kFrontierThreads, 1)
+    lattice_frontier_kernel(const __grid_constant__ FrontierClasses pc) {
+  __shared__ GroupShared shared_groups[31];
+  __shared__ uint32_t corridor_bits[kCorr ? 31 * 128 : 1];
+  const int warp = threadIdx.x >> 5;
+  const auto entry = [&](int G, int w0) { return group_entry(G, w0); };
+  const auto corr_of = [&](int e) { return corridor_bits + (kCorr ? e * 128 : 0); };
+  {
+    const int e = entry(16, 0);
+    frontier_group<16, kPriced, kCorr>(pc.c[4], blockIdx.x, warp, 1, shared_groups[e], corr_of(e));
   }
-  return cudaGetLastError();
+  {
+    const int w0 = warp & ~7, e = entry(8, w0);
+    frontier_group<8, kPriced, kCorr>(pc.c[3], blockIdx.x * 2u + w0 / 8, warp - w0, 2 + w0 / 8,
+                                      shared_groups[e], corr_of(e));
+  }
+  {
+    const int w0 = warp & ~3, e = entry(4, w0);
+    frontier_group<4, kPriced, kCorr>(pc.c[2], blockIdx.x * 4u + w0 / 4, warp - w0, 4 + w0 / 4,
+                                      shared_groups[e], corr_of(e));
+  }
+  {
+    const int w0 = warp & ~1, e = entry(2, w0);
+    frontier_group<2, kPriced, kCorr>(pc.c[1], blockIdx.x * 8u + w0 / 2, warp - w0, 8 + w0 / 2,
+                                      shared_groups[e], corr_of(e));
+  }
+  {
+    const int e = entry(1, warp);
+    frontier_group<1, kPriced, kCorr>(pc.c[0], blockIdx.x * 16u + warp, 0, 0, shared_groups[e],
+                                      corr_of(e));
+  }
+}
+
+// Resident 16-warp CTAs per SM of the fullest instantiation (the others then
+// keep their extra CTAs waiting: they start as others finish, and find the
+// cursors past the end).
+cudaError_t frontier_blocks_per_sm(int* out) {
+  int plain = 0, priced = 0, corridor = 0;
+  cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+      &plain, lattice_frontier_kernel<false, false>, kFrontierThreads, 0);
+  if (e == cudaSuccess) {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &priced, lattice_frontier_kernel<true, false>, kFrontierThreads, 0);
+  }
+  if (e == cudaSuccess) {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &corridor, lattice_frontier_kernel<false, true>, kFrontierThreads, 0);
+  }
+  if (e != cudaSuccess) return e;
+  *out = max(1, max(plain, max(priced, corridor)));
+  return cudaSuccess;
 }
 
 }  // namespace
@@ -860,27 +884,39 @@ cudaError_t launch_build_moves(const LatticeDeviceView& lat, uint16_t* moves, cu
 }
 
 cudaError_t lattice_frontier_resident_groups(int warps_per_net, int sm_count, uint32_t* out) {
-  switch (warps_per_net) {
-    case 1: return resident_groups_g<1>(sm_count, out);
-    case 2: return resident_groups_g<2>(sm_count, out);
-    case 4: return resident_groups_g<4>(sm_count, out);
-    case 8: return resident_groups_g<8>(sm_count, out);
-    case 16: return resident_groups_g<16>(sm_count, out);
-    default: return cudaErrorInvalidValue;
+  if (warps_per_net < 1 || warps_per_net > 16 || (warps_per_net & (warps_per_net - 1)) != 0) {
+    return cudaErrorInvalidValue;
   }
+  int blocks = 0;
+  if (cudaError_t e = frontier_blocks_per_sm(&blocks); e != cudaSuccess) return e;
+  *out = static_cast<uint32_t>(blocks) * static_cast<uint32_t>(max(1, sm_count)) *
+         static_cast<uint32_t>(16 / warps_per_net);
+  return cudaSuccess;
 }
 
-cudaError_t launch_lattice_frontier(int warps_per_net, const FrontierLaunch& launch, int,
+cudaError_t launch_lattice_frontier(const FrontierClasses& classes, int sm_count,
                                     cudaStream_t stream) {
-  if (launch.plan_count == 0 || launch.slots == 0) return cudaSuccess;
-  switch (warps_per_net) {
-    case 1: return launch_frontier_g<1>(launch, stream);
-    case 2: return launch_frontier_g<2>(launch, stream);
-    case 4: return launch_frontier_g<4>(launch, stream);
-    case 8: return launch_frontier_g<8>(launch, stream);
-    case 16: return launch_frontier_g<16>(launch, stream);
-    default: return cudaErrorInvalidValue;
+  bool any = false, priced = false, corridor = false;
+  for (const FrontierLaunch& c : classes.c) {
+    if (c.plan_count == 0 && c.plan_count_dev == nullptr) continue;
+    any = any || c.slots > 0;
+    priced = priced || c.cell_cost != nullptr;
+    corridor = corridor || c.corridor != nullptr;
   }
+  if (!any) return cudaSuccess;
+  if (priced && corridor) return cudaErrorInvalidValue;
+  int blocks = 0;
+  if (cudaError_t e = frontier_blocks_per_sm(&blocks); e != cudaSuccess) return e;
+  // every CTA that can be resident at once; the class slots were sized to it
+  const unsigned grid = static_cast<unsigned>(blocks * max(1, sm_count));
+  if (priced) {
+    lattice_frontier_kernel<true, false><<<grid, kFrontierThreads, 0, stream>>>(classes);
+  } else if (corridor) {
+    lattice_frontier_kernel<false, true><<<grid, kFrontierThreads, 0, stream>>>(classes);
+  } else {
+    lattice_frontier_kernel<false, false><<<grid, kFrontierThreads, 0, stream>>>(classes);
+  }
+  return cudaGetLastError();
 }
 
 }  // namespace apgar_b200

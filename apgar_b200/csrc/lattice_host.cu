@@ -26,7 +26,7 @@ cudaError_t launch_lattice_sweep(int layers, int warps_per_net, const SweepLaunc
 cudaError_t launch_accumulate_cells(const apgar_b200_lattice_result* results, uint32_t count,
                                     const uint32_t* paths, uint32_t* usage, uint64_t cell_count,
                                     int sm_count, cudaStream_t stream);
-cudaError_t launch_lattice_frontier(int warps_per_net, const FrontierLaunch& launch, int sm_count,
+cudaError_t launch_lattice_frontier(const FrontierClasses& classes, int sm_count,
                                     cudaStream_t stream);
 cudaError_t lattice_frontier_resident_groups(int warps_per_net, int sm_count, uint32_t* out);
 cudaError_t launch_build_moves(const LatticeDeviceView& lat, uint16_t* moves, cudaStream_t stream);
@@ -515,22 +515,16 @@ int execute_plan(PlanObject* plan, cudaStream_t stream) {
   base.path_arena_capacity = plan->arena_capacity;
   base.arena_cursor = plan->counters.get();
   base.cancel = plan->cancel_dev;
-  const bool fan_out = plan->classes.size() > 1;
-  if (fan_out) APGAR_B200_CUDA("cudaEventRecord(fork)", cudaEventRecord(plan->fork, stream));
-  // widest class first (see the stream priorities above)
-  for (size_t kk = plan->classes.size(); kk-- > 0;) {
-    const size_t k = kk;
-    const ClassRange& c = plan->classes[k];
-    SweepLaunch launch = base;
-    launch.plans = plan->plans.get() + c.begin;
-    launch.plan_count = c.count;
-    cudaStream_t s = stream;
-    if (fan_out) {
-      s = plan->class_streams[k];
-      APGAR_B200_CUDA("cudaStreamWaitEvent", cudaStreamWaitEvent(s, plan->fork, 0));
-    }
-    if (plan->generator == APGAR_B200_LATTICE_FRONTIER) {
-      FrontierLaunch fl = fbase;
+  if (plan->generator == APGAR_B200_LATTICE_FRONTIER) {
+    // every width class in one persistent launch (the kernel serves the
+    // widest class first and splits its groups as the classes drain)
+    FrontierClasses fc{};
+    for (size_t k = 0; k < plan->classes.size(); ++k) {
+      const ClassRange& c = plan->classes[k];
+      int pos = 0;
+      while ((1 << pos) < c.warps_per_net) ++pos;
+      FrontierLaunch& fl = fc.c[pos];
+      fl = fbase;
       fl.plans = plan->plans.get() + c.begin;
       fl.plan_count = c.count;
       fl.words = plan->words.get() + c.words_offset;
@@ -547,12 +541,29 @@ int execute_plan(PlanObject* plan, cudaStream_t stream) {
       }
       fl.next_plan = reinterpret_cast<unsigned int*>(plan->counters.get() + 2 + k);
       fl.chain = plan->chain != 0 ? plan->chain - 1 : default_chain(c.warps_per_net);
-      APGAR_B200_CUDA("lattice frontier launch",
-                      launch_lattice_frontier(c.warps_per_net, fl, plan->sm_count, s));
-    } else {
-      APGAR_B200_CUDA("lattice sweep launch",
-                      launch_lattice_sweep(v.layers, c.warps_per_net, launch, c.max_rows, s));
     }
+    APGAR_B200_CUDA("lattice frontier launch", launch_lattice_frontier(fc, plan->sm_count, stream));
+    APGAR_B200_CUDA("lattice pack launch",
+                    launch_lattice_pack(plan->results.get(), plan->count, plan->counters.get() + 1,
+                                        plan->arena.get(), plan->paths.get(), plan->sm_count, stream));
+    return APGAR_B200_OK;
+  }
+  const bool fan_out = plan->classes.size() > 1;
+  if (fan_out) APGAR_B200_CUDA("cudaEventRecord(fork)", cudaEventRecord(plan->fork, stream));
+  // widest class first (see the stream priorities above)
+  for (size_t kk = plan->classes.size(); kk-- > 0;) {
+    const size_t k = kk;
+    const ClassRange& c = plan->classes[k];
+    SweepLaunch launch = base;
+    launch.plans = plan->plans.get() + c.begin;
+    launch.plan_count = c.count;
+    cudaStream_t s = stream;
+    if (fan_out) {
+      s = plan->class_streams[k];
+      APGAR_B200_CUDA("cudaStreamWaitEvent", cudaStreamWaitEvent(s, plan->fork, 0));
+    }
+    APGAR_B200_CUDA("lattice sweep launch",
+                    launch_lattice_sweep(v.layers, c.warps_per_net, launch, c.max_rows, s));
     if (fan_out) {
       APGAR_B200_CUDA("cudaEventRecord(join)", cudaEventRecord(plan->joins[k], s));
       APGAR_B200_CUDA("cudaStreamWaitEvent", cudaStreamWaitEvent(stream, plan->joins[k], 0));
@@ -850,7 +861,10 @@ extern "C" int apgar_b200_lattice_plan_info(void* plan, apgar_b200_plan_info* ou
   std::memset(out, 0, sizeof(*out));
   out->net_count = p->count;
   out->class_count = static_cast<uint32_t>(p->classes.size());
-  out->kernel_launches = out->class_count + (p->count > 0 ? 2u : 0u);
+  // the frontier runs all its classes in one launch; the sweep one per class
+  const uint32_t search_launches =
+      p->generator == APGAR_B200_LATTICE_FRONTIER ? (out->class_count > 0 ? 1u : 0u) : out->class_count;
+  out->kernel_launches = search_launches + (p->count > 0 ? 2u : 0u);
   out->workspace_bytes = p->workspace_bytes();
   out->label_cells = p->label_cells;
   out->path_arena_capacity = p->arena_capacity;

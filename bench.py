@@ -36,12 +36,10 @@ import time
 import numpy as np
 
 # One hardware work queue per process (read when the CUDA context is created,
-# so before torch touches the GPU): the width classes of a plan run as
-# concurrent persistent kernels on forked streams, and with several queues
-# their CTAs can reach the SMs in any order, so narrow classes sometimes fill
-# the SMs before the 16-warp class and delay the longest nets (measured: 18 to
-# 26 ms for the same batch).  With one queue the CTAs dispatch in launch
-# order, widest class first, and the time per batch stays within 1%.
+# so before torch touches the GPU).  The plain sweep runs its width classes as
+# concurrent kernels on forked streams; with several queues their CTAs reach
+# the SMs in any order and its time per batch varies by about 7%.  (The
+# frontier runs all its classes in one launch and does not depend on it.)
 os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "1")
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
