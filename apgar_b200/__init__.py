@@ -60,6 +60,7 @@ class LatticeDesc(ctypes.Structure):
 
 
 GENERATORS = {"sweep": 0, "frontier": 1}
+LATTICE_PATH_CODES = {0: "ok", 1: "bounds", 2: "endpoint", 5: "edge", 7: "not_reached", 8: "cost"}
 
 
 class LatticeOptions(ctypes.Structure):
@@ -233,6 +234,21 @@ class DeviceLattice:
                 _vp(cancel), _vp(results), _vp(paths) if want_paths else None,
                 ctypes.c_uint64(paths.size if want_paths else 0), ctypes.byref(total)))
         return results, (paths[: total.value] if want_paths else None)
+
+    def validate(self, nets: np.ndarray, results: np.ndarray, paths: np.ndarray) -> np.ndarray:
+        """Device validation of read-back route results (packed reverse paths):
+        one (code, reserved, failing forward index, cost sum) record per net,
+        codes as in ``LATTICE_PATH_CODES``."""
+        from .dropin import VERDICT_DTYPE
+
+        nets = np.ascontiguousarray(nets)
+        results = np.ascontiguousarray(results)
+        paths = np.ascontiguousarray(paths, dtype=np.uint32)
+        out = np.zeros(len(nets), dtype=VERDICT_DTYPE)
+        _check(lib().apgar_b200_lattice_validate(
+            self.handle, _vp(nets), ctypes.c_uint32(len(nets)), _vp(results),
+            _vp(paths) if len(paths) else None, ctypes.c_uint64(len(paths)), _vp(out)))
+        return out
 
     def route_noalloc(self, nets: np.ndarray, max_sweeps: int = 4096, stream: int = 0,
                       out=None):

@@ -28,6 +28,10 @@ cudaError_t launch_accumulate_cells(const apgar_b200_lattice_result* results, ui
                                     int sm_count, cudaStream_t stream);
 cudaError_t launch_lattice_frontier(const FrontierClasses& classes, int sm_count,
                                     cudaStream_t stream);
+cudaError_t launch_lattice_validate(const LatticeDeviceView& lat, const apgar_b200_lattice_net* nets,
+                                    const apgar_b200_lattice_result* results, const uint32_t* paths,
+                                    uint64_t path_count, uint32_t count,
+                                    apgar_b200_path_verdict* out, cudaStream_t stream);
 cudaError_t lattice_frontier_resident_groups(int warps_per_net, int sm_count, uint32_t* out);
 cudaError_t launch_build_moves(const LatticeDeviceView& lat, uint16_t* moves, cudaStream_t stream);
 cudaError_t launch_price_update(uint32_t count, const uint32_t* usage, uint64_t factor,
@@ -167,6 +171,12 @@ struct LatticeObject {
   DeviceBuffer<uint16_t> moves;  // LatticeDeviceView::moves
   std::mutex route_mutex;
   std::unique_ptr<PlanObject> route_plan;  // reusable workspace for route()
+  // reusable workspace for validate() (grown as needed, kept for later calls)
+  std::mutex validate_mutex;
+  DeviceBuffer<apgar_b200_lattice_net> val_nets;
+  DeviceBuffer<apgar_b200_lattice_result> val_results;
+  DeviceBuffer<uint32_t> val_paths;
+  DeviceBuffer<apgar_b200_path_verdict> val_out;
 };
 
 int check_device(int expected) {
@@ -987,6 +997,42 @@ extern "C" int apgar_b200_lattice_plan_ex(void* lattice, const apgar_b200_lattic
   } catch (const std::bad_alloc&) {
     return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "host allocation failed during planning");
   }
+}
+
+extern "C" int apgar_b200_lattice_validate(void* lattice, const apgar_b200_lattice_net* nets,
+                                           uint32_t count, const apgar_b200_lattice_result* results,
+                                           const uint32_t* paths, uint64_t path_count,
+                                           apgar_b200_path_verdict* verdicts) {
+  if (lattice == nullptr || (count > 0 && (nets == nullptr || results == nullptr || verdicts == nullptr)) ||
+      (path_count > 0 && paths == nullptr)) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "lattice validation received a null argument");
+  }
+  auto* lat = static_cast<LatticeObject*>(lattice);
+  if (int rc = check_device(lat->device); rc != APGAR_B200_OK) return rc;
+  if (count == 0) {
+    clear_error();
+    return APGAR_B200_OK;
+  }
+  std::scoped_lock lock(lat->validate_mutex);
+  auto& d_nets = lat->val_nets;
+  auto& d_res = lat->val_results;
+  auto& d_paths = lat->val_paths;
+  auto& d_out = lat->val_out;
+  APGAR_B200_CUDA("cudaMalloc(nets)", d_nets.ensure(count));
+  APGAR_B200_CUDA("cudaMalloc(results)", d_res.ensure(count));
+  APGAR_B200_CUDA("cudaMalloc(paths)", d_paths.ensure(std::max<uint64_t>(path_count, 1)));
+  APGAR_B200_CUDA("cudaMalloc(verdicts)", d_out.ensure(count));
+  APGAR_B200_CUDA("cudaMemcpy(nets)", cudaMemcpy(d_nets.get(), nets, count * sizeof(*nets), cudaMemcpyHostToDevice));
+  APGAR_B200_CUDA("cudaMemcpy(results)", cudaMemcpy(d_res.get(), results, count * sizeof(*results), cudaMemcpyHostToDevice));
+  if (path_count > 0) {
+    APGAR_B200_CUDA("cudaMemcpy(paths)", cudaMemcpy(d_paths.get(), paths, path_count * 4, cudaMemcpyHostToDevice));
+  }
+  APGAR_B200_CUDA("lattice validation launch",
+                  launch_lattice_validate(lat->view, d_nets.get(), d_res.get(), d_paths.get(), path_count,
+                                          count, d_out.get(), nullptr));
+  APGAR_B200_CUDA("cudaMemcpy(verdicts)", cudaMemcpy(verdicts, d_out.get(), count * sizeof(*verdicts), cudaMemcpyDeviceToHost));
+  clear_error();
+  return APGAR_B200_OK;
 }
 
 extern "C" int apgar_b200_lattice_accumulate_usage(void* plan, uint32_t* usage, uint64_t cell_count,

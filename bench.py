@@ -587,17 +587,26 @@ def main():
     e_start = torch.cuda.Event(enable_timing=True)
     e_end = torch.cuda.Event(enable_timing=True)
     path_cells = 0
+    validated = None
     e_start.record()
     for _ in range(args.steps):
+        # route from host buffers, then validate the untrusted results on the
+        # device, as a caller does before trusting them
         r, p = dev.route(nets_host, out=(res_arr, path_arr), generator="frontier",
                          schedule=schedule)
+        validated = dev.validate(nets_host, r, p)
         path_cells = len(p)
     e_end.record()
     barrier()
+    reached = r["completion"] == apgar_b200.COMPLETION_REACHED
+    if not (validated["code"][reached] == 0).all():
+        raise RuntimeError("a routed path failed validation")
     e2e_ms = max_over_ranks(e_start.elapsed_time(e_end))
     e2e_value = cert_all * args.steps / (e2e_ms / 1000.0)
-    h2d = nets.nbytes
-    d2h = len(nets) * apgar_b200.RESULT_DTYPE.itemsize + 4 * path_cells + 8
+    verdict_bytes = len(nets) * validated.dtype.itemsize
+    result_bytes = len(nets) * apgar_b200.RESULT_DTYPE.itemsize
+    h2d = 2 * nets.nbytes + result_bytes + 4 * path_cells
+    d2h = result_bytes + 4 * path_cells + 8 + verdict_bytes
     results = front["results"]
     step_ms = front["step_ms"]
     total_ms = front["total_ms"]
@@ -635,7 +644,10 @@ def main():
                 "bytes_alg_per_step": fbytes,
             },
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
-                    "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms / args.steps},
+                    "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms / args.steps,
+                    "scope": "host nets -> route (H2D, search, D2H results and paths) -> "
+                             "device validation of every path (H2D, check, D2H verdicts)",
+                    "validated_ok": int((validated["code"] == 0).sum())},
             "clocks": clocks,
             "step_ms_min_max": [min(step_ms), max(step_ms)],
             "plain_sweep": {

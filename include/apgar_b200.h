@@ -282,7 +282,8 @@ enum {
   APGAR_B200_PATH_HEADING = 4,   /* gpu.batch.compact_path.heading.v1 */
   APGAR_B200_PATH_EDGE = 5,      /* gpu.batch.compact_path.edge.v1 */
   APGAR_B200_PATH_BANNED = 6,    /* gpu.policy.banned_predecessor.v1 */
-  APGAR_B200_PATH_NOT_REACHED = 7 /* the query did not reach its goal: not validated */
+  APGAR_B200_PATH_NOT_REACHED = 7, /* the query did not reach its goal: not validated */
+  APGAR_B200_PATH_COST = 8         /* lattice mode: the move costs do not sum to the reported cost */
 };
 typedef struct apgar_b200_path_verdict {
   uint32_t code;          /* APGAR_B200_PATH_* */
@@ -361,6 +362,23 @@ typedef struct apgar_b200_lattice_result {
   uint32_t row_loads;    /* layer rows read (current and re-read predecessor rows) */
   uint32_t reserved;
 } apgar_b200_lattice_result;
+
+/* Validates lattice route results on the device, the lattice counterpart of
+ * the structural checks of ValidateAndReconstructCompactGpuPath
+ * (src/gpu/planar_router.cc:969-1067).  `results` and `paths` are untrusted
+ * host arrays as read back from a lattice route or plan (packed reverse paths
+ * of global cell ids, goal first); `nets` are the nets they answer.  Per
+ * reached net: path bounds (BOUNDS), the start and goal endpoints (ENDPOINT),
+ * every cell inside the lattice and the net's window (BOUNDS), every step one
+ * legal move re-derived from the blocked and via masks (EDGE), and the move
+ * costs summing to the reported cost (COST; unpriced costs).  One verdict per
+ * net: failing_index counts cells from the start; total_cost is the sum.
+ * Unreached nets get NOT_REACHED. */
+APGAR_B200_API int apgar_b200_lattice_validate(void* lattice, const apgar_b200_lattice_net* nets,
+                                               uint32_t count,
+                                               const apgar_b200_lattice_result* results,
+                                               const uint32_t* paths, uint64_t path_count,
+                                               apgar_b200_path_verdict* verdicts);
 
 /* Uploads the lattice masks to the current device (the prepared view). */
 APGAR_B200_API int apgar_b200_lattice_upload(const apgar_b200_lattice_desc* desc, void** out_lattice);

@@ -304,6 +304,77 @@ def disconnect_verdict(nodes, costs, start, goal, orth_s=0, diag_s=0, bend_s=0, 
     return ("confirmed" if bounded else "unbounded"), len(seen)
 
 
+LATTICE_PATH_CODES = {0: "ok", 1: "bounds", 2: "endpoint", 5: "edge", 7: "not_reached", 8: "cost"}
+
+
+def validate_lattice_path(lat, net, result, path):
+    """Structural validation of one lattice route result, restating the checks
+    a host applies to an untrusted GPU path (src/gpu/planar_router.cc:969-1067)
+    for lattice paths: bounds, endpoints (start first, goal last in forward
+    order), every cell inside the lattice and the net's window, every step a
+    legal move by the lattice rule (orthogonal: both cells free; diagonal: both
+    cells and both side cells free; via: same column, adjacent layer, both
+    cells free, via bit set), and the move costs summing to the reported cost.
+    ``path`` is the reverse path of global cell ids (goal first).  Returns
+    (code name, failing forward index, cost sum)."""
+    if int(result["completion"]) != 0:
+        return "not_reached", 0, 0
+    path = [int(c) for c in path]
+    if not path:
+        return "bounds", 0, 0
+    free = ~lat.blocked_dense()
+    via_ok = None if lat.via_ok is None else unpack_bits_dense(lat.via_ok, lat.width)
+    L, H, W = lat.layers, lat.height, lat.width
+
+    def cell(c):
+        return c // (W * H), c % W, (c // W) % H
+
+    fwd = path[::-1]
+    start = (int(net["start_layer"]) * H + int(net["start_y"])) * W + int(net["start_x"])
+    goal = (int(net["goal_layer"]) * H + int(net["goal_y"])) * W + int(net["goal_x"])
+    if fwd[0] != start:
+        return "endpoint", 0, 0
+    if fwd[-1] != goal:
+        return "endpoint", len(fwd) - 1, 0
+    x0, y0 = int(net["win_x0"]), int(net["win_y0"])
+    x1, y1 = x0 + int(net["win_w"]), y0 + int(net["win_h"])
+    total = 0
+    for f, c in enumerate(fwd):
+        if c >= L * H * W:
+            return "bounds", f, 0
+        l, x, y = cell(c)
+        if not (x0 <= x < x1 and y0 <= y < y1):
+            return "bounds", f, 0
+        if f == 0:
+            continue
+        pl, px, py = cell(fwd[f - 1])
+        dx, dy, dl = x - px, y - py, l - pl
+        cost = 0
+        if dl != 0:
+            if dx == 0 and dy == 0 and abs(dl) == 1 and free[pl, py, px] and free[l, y, x] and \
+                    (via_ok is None or via_ok[min(l, pl), y, x]):
+                cost = lat.via
+        elif max(abs(dx), abs(dy)) == 1 and free[pl, py, px] and free[l, y, x]:
+            if dx != 0 and dy != 0:
+                if free[l, py, x] and free[l, y, px]:
+                    cost = lat.diag
+            else:
+                cost = lat.orth
+        if cost == 0:
+            return "edge", f, 0
+        total += cost
+    if total != int(result["cost"]):
+        return "cost", 0, total
+    return "ok", 0, total
+
+
+def unpack_bits_dense(words, width):
+    """uint32 [..., width // 32] -> bool [..., width] (bit x % 32 of word x // 32)."""
+    shifts = np.arange(32, dtype=np.uint32)
+    bits = (np.asarray(words)[..., None] >> shifts) & np.uint32(1)
+    return bits.reshape(np.asarray(words).shape[:-1] + (width,)).astype(bool)
+
+
 def graph_predecessors(nodes, costs, start, labels, orth_s=0, diag_s=0, bend_s=0, policy=None):
     """Canonical predecessor of every state from exact labels."""
     L = lib()
