@@ -835,13 +835,21 @@ __global__ void adam_kernel(float* __restrict__ params, const float* __restrict_
 
 // One block per net: coarse cells with logit > threshold, dilated by
 // `dilate` coarse cells (Chebyshev), plus both terminals, as the 128-word
-// corridor bitmap (bit cx % 32 of word 2 * cy + cx / 32).
+// corridor bitmap (bit cx % 32 of word 2 * cy + cx / 32).  A net whose window
+// holds more than max_cells cells (all layers; 0 = no limit) gets an empty
+// bitmap: no corridor, its whole window is searched at once.
 __global__ void corridor_kernel(const float* __restrict__ logits, const uint32_t* __restrict__ dims,
                                 const apgar_b200_lattice_net* __restrict__ nets, uint32_t count,
-                                float threshold, int dilate, uint32_t* __restrict__ bits) {
+                                float threshold, int dilate, uint64_t max_cells, int layers,
+                                uint32_t* __restrict__ bits) {
   __shared__ uint8_t hot[kCells];
   const uint32_t n = blockIdx.x;
   if (n >= count) return;
+  if (max_cells != 0 &&
+      static_cast<uint64_t>(layers) * nets[n].win_w * nets[n].win_h > max_cells) {
+    for (int wd = threadIdx.x; wd < 128; wd += blockDim.x) bits[static_cast<size_t>(n) * 128 + wd] = 0u;
+    return;  // uniform: the whole block
+  }
   const uint32_t d = dims[n];
   const int cw = static_cast<int>(dims_w(d)), ch = static_cast<int>(dims_h(d));
   const int s = static_cast<int>(d >> 16);
@@ -1026,9 +1034,11 @@ cudaError_t launch_adam(float* params, const float* grads, float* m, float* v, u
 
 cudaError_t launch_corridors(const float* logits, const uint32_t* dims,
                              const apgar_b200_lattice_net* nets, uint32_t count, float threshold,
-                             int dilate, uint32_t* bits, cudaStream_t stream) {
+                             int dilate, uint64_t max_cells, int layers, uint32_t* bits,
+                             cudaStream_t stream) {
   if (count == 0) return cudaSuccess;
-  corridor_kernel<<<count, 256, 0, stream>>>(logits, dims, nets, count, threshold, dilate, bits);
+  corridor_kernel<<<count, 256, 0, stream>>>(logits, dims, nets, count, threshold, dilate, max_cells,
+                                             layers, bits);
   return cudaGetLastError();
 }
 

@@ -332,6 +332,7 @@ struct GroupShared {
   uint32_t cancel[2];
   uint32_t overflow;
   uint32_t bound;  // corridor pass: least expanded exit key
+  uint32_t corr_any;  // the net's corridor bitmap has a bit set
   uint32_t sums[16];
 };
 
@@ -358,7 +359,10 @@ __device__ __forceinline__ void frontier_group(const FrontierLaunch& p, uint32_t
   const uint32_t cap = p.list_cap;
 
   for (;;) {
-    if (tid == 0) sh.plan = atomicAdd(p.next_plan, 1u);
+    if (tid == 0) {
+      sh.plan = atomicAdd(p.next_plan, 1u);
+      sh.corr_any = 0u;
+    }
     fsync<G>(barrier_id);
     const uint32_t plan_index = sh.plan;
     if (plan_index >= (p.plan_count_dev != nullptr ? *p.plan_count_dev : p.plan_count)) {
@@ -424,10 +428,17 @@ __device__ __forceinline__ void frontier_group(const FrontierLaunch& p, uint32_t
       const int span_max = win.w > win.h ? win.w : win.h;
       while (((span_max - 1) >> cshift) >= 63) ++cshift;  // at most 63 coarse cells a side
       const uint32_t* src = p.corridor + static_cast<size_t>(plan.net) * 128u;
-      for (int i = tid; i < 128; i += T) corr[i] = __ldg(src + i);
+      for (int i = tid; i < 128; i += T) {
+        const uint32_t word = __ldg(src + i);
+        corr[i] = word;
+        if (word != 0u) sh.corr_any = 1u;
+      }
       fsync<G>(barrier_id);
       use_corr = corr_has(corr, cshift, sx, sy) && corr_has(corr, cshift, win.gx, win.gy);
-      cstatus = use_corr ? APGAR_B200_CORRIDOR_CERTIFIED : APGAR_B200_CORRIDOR_FALLBACK_UNREACHED;
+      // an empty bitmap proposes no corridor: the window is searched at once
+      cstatus = use_corr ? APGAR_B200_CORRIDOR_CERTIFIED
+                         : (sh.corr_any != 0u ? APGAR_B200_CORRIDOR_FALLBACK_UNREACHED
+                                              : APGAR_B200_CORRIDOR_NONE);
     }
     const bool endpoints_free = cell_free_w(lat, win, sl, sx, sy) &&
                                 cell_free_w(lat, win, win.gl, win.gx, win.gy);

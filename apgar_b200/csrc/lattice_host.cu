@@ -58,7 +58,8 @@ cudaError_t launch_lattice_segments(const apgar_b200_lattice_result* results, co
                                     uint32_t* segment_counts, cudaStream_t stream);
 cudaError_t launch_corridors(const float* logits, const uint32_t* dims,
                              const apgar_b200_lattice_net* nets, uint32_t count, float threshold,
-                             int dilate, uint32_t* bits, cudaStream_t stream);
+                             int dilate, uint64_t max_cells, int layers, uint32_t* bits,
+                             cudaStream_t stream);
 
 namespace {
 
@@ -831,7 +832,8 @@ extern "C" int apgar_b200_corridor_labels(void* plan, const uint32_t* dims, uint
 }
 
 extern "C" int apgar_b200_corridor_from_logits(void* plan, const float* logits, const uint32_t* dims,
-                                               float threshold, int32_t dilate, uint32_t* bits,
+                                               float threshold, int32_t dilate,
+                                               uint64_t max_window_cells, uint32_t* bits,
                                                void* stream) {
   if (plan == nullptr || logits == nullptr || dims == nullptr || bits == nullptr || dilate < 0 ||
       dilate > 64) {
@@ -839,8 +841,10 @@ extern "C" int apgar_b200_corridor_from_logits(void* plan, const float* logits, 
   }
   auto* p = static_cast<PlanObject*>(plan);
   if (int rc = check_device(p->device); rc != APGAR_B200_OK) return rc;
-  APGAR_B200_CUDA("corridor launch", launch_corridors(logits, dims, p->nets.get(), p->count, threshold,
-                                                      dilate, bits, static_cast<cudaStream_t>(stream)));
+  APGAR_B200_CUDA("corridor launch",
+                  launch_corridors(logits, dims, p->nets.get(), p->count, threshold, dilate,
+                                   max_window_cells, p->lattice->view.layers, bits,
+                                   static_cast<cudaStream_t>(stream)));
   clear_error();
   return APGAR_B200_OK;
 }

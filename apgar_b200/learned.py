@@ -173,15 +173,17 @@ def labels(plan, dims, stream: int = 0):
 
 
 def corridors(plan, logits, dims, threshold: float = 0.0, dilate: int = 1, out=None,
-              stream: int = 0):
-    """Corridor bitmaps uint32 [n][128] from logits."""
+              stream: int = 0, max_window_cells: int = 0):
+    """Corridor bitmaps uint32 [n][128] from logits; nets whose window holds
+    more than ``max_window_cells`` cells (0 = no limit) get no corridor."""
     import torch
 
     if out is None:
         out = torch.empty((len(plan.nets), 128), dtype=torch.uint32, device="cuda")
     _check(lib().apgar_b200_corridor_from_logits(plan.handle, _ptr(logits), _ptr(dims),
                                                  ctypes.c_float(threshold), ctypes.c_int32(dilate),
-                                                 _ptr(out), ctypes.c_void_p(stream)))
+                                                 ctypes.c_uint64(max_window_cells), _ptr(out),
+                                                 ctypes.c_void_p(stream)))
     return out
 
 
@@ -189,7 +191,9 @@ POLICY_PATH = os.path.join(os.path.dirname(WEIGHTS_PATH), "corridor_policy.json"
 
 
 def load_policy(path: str = POLICY_PATH) -> dict:
-    """The corridor policy chosen at training time: logit threshold, dilation."""
+    """The corridor policy: logit threshold and dilation (chosen at training
+    time) and the largest window that gets a corridor (0 = all; chosen by
+    measuring the learned form)."""
     import json
 
     with open(path) as f:
@@ -220,7 +224,8 @@ class LearnedRouter:
         rasters(self.plan, stream=stream, out=(self.rasters, self.dims))
         self.net.forward(self.rasters, self.dims, acts=self.acts, logits=self.logits, stream=stream)
         corridors(self.plan, self.logits, self.dims, threshold=float(self.policy["threshold"]),
-                  dilate=int(self.policy["dilate"]), out=self.bits, stream=stream)
+                  dilate=int(self.policy["dilate"]), out=self.bits, stream=stream,
+                  max_window_cells=int(self.policy.get("max_window_cells", 0)))
 
     def execute(self, stream: int = 0) -> None:
         self.propose(stream)

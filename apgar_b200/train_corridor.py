@@ -31,6 +31,12 @@ import apgar_b200
 from apgar_b200 import corridor, learned, synth
 
 POLICY_PATH = os.path.join(os.path.dirname(learned.WEIGHTS_PATH), "corridor_policy.json")
+# Windows above 2^19 cells get no corridor: measured on the medium batch, a
+# corridor never shortens a frontier search's rounds, and the widest nets
+# (the batch's critical path) fall back more often (18% of them), which
+# searches them twice (32.1 ms per batch with corridors on every net, 25.6
+# ms without them above 2^19 cells).
+MAX_WINDOW_CELLS = 1 << 19
 
 
 def training_batches(paths: int, nets_per_batch: int = 4096, batches_per_lattice: int = 7,
@@ -130,7 +136,8 @@ def evaluate(net, policies, log=print):
     cw, ch = (dims & 0xFF).astype(np.float64), ((dims >> 8) & 0xFF).astype(np.float64)
     rows = []
     for threshold, dilate in policies:
-        bits = learned.corridors(plan, logits, d, threshold=threshold, dilate=dilate)
+        bits = learned.corridors(plan, logits, d, threshold=threshold, dilate=dilate,
+                                 max_window_cells=MAX_WINDOW_CELLS)
         plan.set_corridors(bits)
         ms = timed()
         st = plan.corridor_status()
@@ -178,7 +185,8 @@ def main(argv=None):
     best = min(ok, key=lambda row: row["ms"]) if ok else None
     if best is not None:
         with open(os.path.join(os.path.dirname(args.out), "corridor_policy.json"), "w") as f:
-            json.dump({"threshold": best["threshold"], "dilate": best["dilate"]}, f)
+            json.dump({"threshold": best["threshold"], "dilate": best["dilate"],
+                       "max_window_cells": MAX_WINDOW_CELLS}, f)
     report = {
         "paths": int(rasters.shape[0]), "epochs": args.epochs, "batch": args.batch, "lr": args.lr,
         "dataset_s": round(t1 - t0, 1), "train_s": round(t2 - t1, 1), "loss": history,

@@ -566,10 +566,12 @@ def main():
             "corridor_certified": float((status == 1).mean()),
             "fallback_exit": float((status == 2).mean()),
             "fallback_unreached": float((status == 3).mean()),
+            "no_corridor": float((status == 0).mean()),  # windows above the policy's limit
             "same_costs_as_frontier": bool(np.array_equal(l_res["cost"], front["results"]["cost"])),
             "policy": router.policy,
             "form": "6-layer 3x3 CNN (tcgen05, bf16/f32) corridors + certified corridor frontier, "
-                    "full-window fallback in the same kernel",
+                    "full-window fallback in the same kernel; windows above the policy's "
+                    "max_window_cells get no corridor",
         }
         lplan.close()
 

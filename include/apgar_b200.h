@@ -504,7 +504,7 @@ APGAR_B200_API int apgar_b200_lattice_plan_set_cell_costs(void* plan, const uint
  * again over the whole window, so results never depend on the corridor.
  * NULL detaches the corridors.  Not combined with per-cell prices. */
 enum {
-  APGAR_B200_CORRIDOR_NONE = 0,
+  APGAR_B200_CORRIDOR_NONE = 0,               /* no corridors, or the net's bitmap is empty */
   APGAR_B200_CORRIDOR_CERTIFIED = 1,          /* the corridor result, certified */
   APGAR_B200_CORRIDOR_FALLBACK_EXIT = 2,      /* reached, but an exit key was <= its cost */
   APGAR_B200_CORRIDOR_FALLBACK_UNREACHED = 3  /* a terminal outside, or goal not reached */
@@ -630,9 +630,12 @@ APGAR_B200_API int apgar_b200_corridor_labels(void* plan, const uint32_t* dims, 
                                void* stream);
 /* The plan's corridor bitmaps (128 words per net) from logits: coarse cells
  * with logit > threshold, dilated by `dilate` coarse cells, plus both
- * terminals. */
+ * terminals.  A net whose window holds more than `max_window_cells` cells
+ * (all layers; 0 = no limit) gets an empty bitmap: no corridor is proposed,
+ * its whole window is searched at once, and its status is NONE. */
 APGAR_B200_API int apgar_b200_corridor_from_logits(void* plan, const float* logits, const uint32_t* dims,
-                                    float threshold, int32_t dilate, uint32_t* bits, void* stream);
+                                    float threshold, int32_t dilate, uint64_t max_window_cells,
+                                    uint32_t* bits, void* stream);
 /* bf16 operand layouts of the current params (after every update). */
 APGAR_B200_API int apgar_b200_cnn_prepare(const float* params, void* operands, void* stream);
 /* Forward pass; acts holds five activation buffers (they may alternate

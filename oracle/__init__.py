@@ -437,7 +437,7 @@ def accumulate_cells(offsets, lengths, cells, cell_count):
 # reached corridor cell u to a window cell v outside the corridor is an exit
 # with key d(u) + move + h(v), h the octile-plus-via bound.  The corridor
 # result is certified when its cost is strictly below every exit key.
-CORRIDOR_CERTIFIED, CORRIDOR_FALLBACK_EXIT, CORRIDOR_FALLBACK_UNREACHED = 1, 2, 3
+CORRIDOR_NONE, CORRIDOR_CERTIFIED, CORRIDOR_FALLBACK_EXIT, CORRIDOR_FALLBACK_UNREACHED = 0, 1, 2, 3
 _STEPS = ((1, 0), (1, 1), (0, 1), (-1, 1), (-1, 0), (-1, -1), (0, -1), (1, -1))
 
 
@@ -466,6 +466,8 @@ def corridor_certificate(lat, net, mask):
     sx, sy = int(n0["start_x"]) - x0, int(n0["start_y"]) - y0
     gx, gy = int(n0["goal_x"]) - x0, int(n0["goal_y"]) - y0
     sl, gl = int(n0["start_layer"]), int(n0["goal_layer"])
+    if not np.asarray(mask).any():
+        return CORRIDOR_NONE, None, None  # no corridor proposed: the window is searched
     if not (inside[sy, sx] and inside[gy, gx]):
         return CORRIDOR_FALLBACK_UNREACHED, None, None
     free = _window_free(lat, n0)

@@ -56,9 +56,19 @@ def test_full_corridor_certifies_everything():
     assert (status == corridor.CERTIFIED).all()
 
 
-def test_empty_corridor_falls_back_everywhere():
+def test_empty_corridor_is_no_proposal():
     lat, nets = _case(22, 24)
     status = _check(lat, nets, np.zeros((len(nets), 64, 64), bool))
+    assert (status == corridor.NONE).all()
+
+
+def test_corridor_missing_a_terminal_falls_back():
+    lat, nets = _case(27, 24)
+    masks = corridor.full_corridor(len(nets))
+    for i, n in enumerate(nets):  # drop the start's coarse cell only
+        s = corridor.coarse_shift(int(n["win_w"]), int(n["win_h"]))
+        masks[i, (int(n["start_y"]) - int(n["win_y0"])) >> s, (int(n["start_x"]) - int(n["win_x0"])) >> s] = False
+    status = _check(lat, nets, masks)
     assert (status == corridor.FALLBACK_UNREACHED).all()
 
 

@@ -181,3 +181,33 @@ def test_training_lowers_the_loss_and_certifies_more_nets():
     finally:
         dev.close()
         dev_h.close()
+
+
+def test_window_limit_proposes_no_corridor():
+    import torch
+
+    lat, nets = _training_set(45, 96, size=512)
+    cost_o, _ = oracle.dijkstra_batch(lat, nets)
+    dev = apgar_b200.DeviceLattice(lat)
+    try:
+        plan = dev.plan(nets, generator="frontier")
+        _, dims = learned.rasters(plan)
+        logits = torch.full((len(nets), learned.GRID, learned.GRID), 5.0, dtype=torch.float32,
+                            device="cuda")  # every coarse cell hot: a whole-window corridor
+        cells = nets["win_w"].astype(np.int64) * nets["win_h"].astype(np.int64) * lat.layers
+        limit = int(np.median(cells))
+        bits = learned.corridors(plan, logits, dims, threshold=0.0, dilate=0,
+                                 max_window_cells=limit)
+        plan.set_corridors(bits)
+        plan.execute()
+        res, _ = plan.readback(want_paths=False)
+        assert np.array_equal(res["cost"], cost_o)
+        status = plan.corridor_status()
+        over = cells > limit
+        assert over.any() and (~over).any()
+        assert (status[over] == corridor.NONE).all()
+        assert (bits.view(torch.int32).cpu().numpy()[over] == 0).all()
+        assert (status[~over] == corridor.CERTIFIED).all()
+        plan.close()
+    finally:
+        dev.close()

@@ -65,10 +65,15 @@ def test_full_corridor_always_certifies():
         assert status == oracle.CORRIDOR_CERTIFIED and bound is None
 
 
-def test_empty_corridor_falls_back():
+def test_empty_corridor_is_no_proposal_and_a_missing_terminal_falls_back():
     lat, nets = _case(14, 8)
     masks = np.zeros((len(nets), 64, 64), bool)
     for i in range(len(nets)):
+        assert oracle.corridor_certificate(lat, nets[i], masks[i])[0] == oracle.CORRIDOR_NONE
+    masks = np.ones((len(nets), 64, 64), bool)
+    for i, n in enumerate(nets):
+        s = corridor.coarse_shift(int(n["win_w"]), int(n["win_h"]))
+        masks[i, (int(n["goal_y"]) - int(n["win_y0"])) >> s, (int(n["goal_x"]) - int(n["win_x0"])) >> s] = False
         assert oracle.corridor_certificate(lat, nets[i], masks[i])[0] == \
             oracle.CORRIDOR_FALLBACK_UNREACHED
 
