@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -102,6 +103,16 @@ constexpr uint64_t kMaxListEntries = 1ull << 25;
 constexpr uint64_t kPerNetFrontierBytes = 24ull << 30;
 // Budget of the persistent slot workspace (label words and queue lists).
 constexpr uint64_t kSlotFrontierBytes = 64ull << 30;
+
+// A workspace budget, overridable from the environment (bytes, decimal), for
+// callers with less device memory to give the frontier.
+uint64_t budget_from_env(const char* name, uint64_t fallback) {
+  const char* v = std::getenv(name);
+  if (v == nullptr || *v == '\0') return fallback;
+  char* end = nullptr;
+  const unsigned long long b = std::strtoull(v, &end, 10);
+  return (end != nullptr && *end == '\0' && b > 0) ? static_cast<uint64_t>(b) : fallback;
+}
 
 struct PlanObject {
   LatticeObject* lattice = nullptr;
@@ -390,7 +401,9 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
     }
     plan->classes.push_back(range);
   }
-  if (frontier && per_net_cells * 20ull > kPerNetFrontierBytes) {
+  const uint64_t per_net_budget = budget_from_env("APGAR_B200_FRONTIER_PER_NET_BYTES", kPerNetFrontierBytes);
+  const uint64_t slot_budget = budget_from_env("APGAR_B200_FRONTIER_SLOT_BYTES", kSlotFrontierBytes);
+  if (frontier && per_net_cells * 20ull > per_net_budget) {
     // Slot workspace within its budget: the class with the largest slot
     // gives up an eighth of its slots until the total fits (every class keeps
     // at least one; fewer slots only means fewer of its nets in flight).
@@ -400,7 +413,7 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
       for (const ClassRange& c : plan->classes) t += c.slots * slot_bytes(c);
       return t;
     };
-    while (total() > kSlotFrontierBytes) {
+    while (total() > slot_budget) {
       ClassRange* widest = nullptr;
       for (ClassRange& c : plan->classes) {
         if (c.slots > 1 && (widest == nullptr || slot_bytes(c) > slot_bytes(*widest))) widest = &c;
@@ -426,7 +439,7 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
     // Every net gets its own slab (8 B words + 3 x 4 B list entries per
     // cell) when that fits the per-net budget; otherwise the persistent
     // groups reuse their slot slabs net after net.
-    plan->per_net = per_net_cells * 20ull <= kPerNetFrontierBytes;
+    plan->per_net = per_net_cells * 20ull <= per_net_budget;
     if (plan->per_net) {
       dist_cells = per_net_cells;
       arena_lists = 3ull * per_net_cells;

@@ -193,3 +193,39 @@ def test_chain_above_sixteen_is_refused():
     lat, nets = synth.config_small(1)
     with pytest.raises(apgar_b200.BackendError):
         _route(lat, nets[:4].copy(), chain=17)
+
+
+def test_slot_workspace_gives_the_per_net_results(monkeypatch):
+    """The persistent slot workspace (used when per-net slabs exceed their
+    budget), with its full slot count and with slots cut to fit a small
+    budget, gives exactly the per-net workspace's (and the oracle's) costs
+    and paths."""
+    lat = synth.make_lattice(51, 2, 512, 0.2, pads=True)
+    nets = synth.make_nets(lat, 52, 300, hpwl_median=120.0, hpwl_sigma=1.0)
+    cost_o, paths_o = oracle.dijkstra_batch(lat, nets)
+    dev = apgar_b200.DeviceLattice(lat)
+    try:
+        outs = []
+        for per_net, slot in ((None, None), ("1", None), ("1", str(64 << 20))):
+            if per_net is not None:
+                monkeypatch.setenv("APGAR_B200_FRONTIER_PER_NET_BYTES", per_net)
+            if slot is not None:
+                monkeypatch.setenv("APGAR_B200_FRONTIER_SLOT_BYTES", slot)
+            plan = dev.plan(nets, generator="frontier")
+            plan.execute()
+            res, paths = plan.readback()
+            outs.append((res, paths, plan.info()["workspace_bytes"]))
+            plan.close()
+        monkeypatch.delenv("APGAR_B200_FRONTIER_PER_NET_BYTES")
+        monkeypatch.delenv("APGAR_B200_FRONTIER_SLOT_BYTES")
+        assert len({w for _, _, w in outs}) == 3  # three different workspaces
+        assert outs[2][2] < outs[1][2]
+        for res, paths, _ in outs:
+            assert (res["completion"] != apgar_b200.COMPLETION_REJECTED).all()
+            assert np.array_equal(res["cost"], cost_o)
+            per = apgar_b200.split_paths(res, paths)
+            for i in range(len(nets)):
+                if cost_o[i] != oracle.lo_inf():
+                    assert np.array_equal(per[i], paths_o[i]), i
+    finally:
+        dev.close()
