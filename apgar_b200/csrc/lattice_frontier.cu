@@ -72,6 +72,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 
 #include "lattice_common.cuh"
@@ -827,7 +828,20 @@ __global__ void __launch_bounds__(kFrontierThreads, 1)
 // Resident 16-warp CTAs per SM of the fullest instantiation (the others then
 // keep their extra CTAs waiting: they start as others finish, and find the
 // cursors past the end).
+// Per device ordinal: resident CTAs per SM, 0 until first queried.
+std::atomic<int> g_frontier_blocks[64];
+
 cudaError_t frontier_blocks_per_sm(int* out) {
+  int device = 0;
+  if (cudaError_t e = cudaGetDevice(&device); e != cudaSuccess) return e;
+  const bool cacheable = device >= 0 && device < 64;
+  if (cacheable) {
+    const int cached = g_frontier_blocks[device].load(std::memory_order_acquire);
+    if (cached > 0) {
+      *out = cached;
+      return cudaSuccess;
+    }
+  }
   int plain = 0, priced = 0, corridor = 0;
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
       &plain, lattice_frontier_kernel<false, false>, kFrontierThreads, 0);
@@ -841,6 +855,7 @@ cudaError_t frontier_blocks_per_sm(int* out) {
   }
   if (e != cudaSuccess) return e;
   *out = max(1, max(plain, max(priced, corridor)));
+  if (cacheable) g_frontier_blocks[device].store(*out, std::memory_order_release);
   return cudaSuccess;
 }
 
