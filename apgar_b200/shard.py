@@ -34,6 +34,28 @@ def split_nets(nets: np.ndarray, rank: int, world: int) -> np.ndarray:
     return np.ascontiguousarray(nets[rank::world])
 
 
+def window_work(nets: np.ndarray, layers: int) -> np.ndarray:
+    """Estimated search work of each net: its window cells over all layers
+    (W x L)."""
+    return nets["win_w"].astype(np.int64) * nets["win_h"].astype(np.int64) * int(layers)
+
+
+def balanced_split(nets: np.ndarray, world: int, layers: int) -> list:
+    """Static partition of one batch over ranks by estimated window work:
+    longest-processing-time first, each net to the rank with the least work
+    so far (ties to the lower rank).  Returns each rank's net indices,
+    ascending; every rank computes the same partition."""
+    work = window_work(nets, layers)
+    order = np.lexsort((np.arange(len(nets)), -work))  # largest first, stable
+    loads = np.zeros(world, dtype=np.int64)
+    owner = np.empty(len(nets), dtype=np.int64)
+    for i in order:
+        r = int(np.argmin(loads))
+        owner[i] = r
+        loads[r] += work[i]
+    return [np.flatnonzero(owner == r) for r in range(world)]
+
+
 def max_over_ranks(value: float, dist=None, device=None) -> float:
     """Maximum of a per-rank value (step time) over all ranks."""
     if dist is None or not dist.is_initialized() or dist.get_world_size() == 1:

@@ -365,7 +365,8 @@ def run_negotiated_ranked(args, rank, world, local):
     full = args.workload == "full"
     rounds = args.rounds if args.rounds is not None else (20 if full else 10)
     lat, segs, _ = synth.config_full(args.seed + 3) if full else synth.config_negotiated(args.seed + 1)
-    mine = shard.split_nets(segs, rank, world)
+    # static partition by estimated window work (every rank computes the same)
+    mine = np.ascontiguousarray(segs[shard.balanced_split(segs, world, lat.layers)[rank]])
     dev = apgar_b200.DeviceLattice(lat)
     plan = dev.plan(mine, generator="frontier")
     neg = negotiate.Negotiation(plan, prices.policy(capacity=1))
@@ -420,7 +421,8 @@ def run_negotiated_ranked(args, rank, world, local):
         "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic",
         "config": {"workload": FULL_WORKLOAD if full else NEG_WORKLOAD, "segments": len(segs),
-                   "rounds": rounds, "parallelism": f"segments split over {world} ranks",
+                   "rounds": rounds,
+                   "parallelism": f"segments split over {world} ranks, balanced by window work",
                    "form": "frontier search + fused snapshot prices, Jacobi rounds; one int32 "
                            "all-reduce of per-cell usage per round (NCCL)",
                    "rip_up": "full" if args.full_ripup else "partial (nets crossing overused cells)"},

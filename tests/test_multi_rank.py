@@ -146,3 +146,20 @@ def test_two_ranks_negotiate_like_one_plan():
         assert r["per_round"] == per_round
         assert np.array_equal(r["costs"], costs[rank::world])
         assert r["calls"] == [(i, p) for i in range(rounds) for p in (0, 1)]
+
+
+def test_balanced_split_covers_the_batch_and_balances_work():
+    lat = synth.make_lattice(5, 2, 256, 0.2)
+    nets = synth.make_nets(lat, 6, 500, hpwl_median=40.0, hpwl_sigma=1.0, margin=16)
+    work = shard.window_work(nets, lat.layers)
+    for world in (1, 2, 3, 8):
+        parts = shard.balanced_split(nets, world, lat.layers)
+        assert len(parts) == world
+        allidx = np.concatenate(parts)
+        assert np.array_equal(np.sort(allidx), np.arange(len(nets)))
+        loads = np.array([work[p].sum() for p in parts])
+        # LPT: no rank exceeds the mean by more than the largest single net
+        assert loads.max() - loads.mean() <= work.max()
+        again = shard.balanced_split(nets.copy(), world, lat.layers)  # deterministic
+        assert all(np.array_equal(a, b) for a, b in zip(parts, again))
+

@@ -24,17 +24,21 @@ def _case():
     return lat, nets, pol
 
 
+@pytest.mark.parametrize("split", ["round_robin", "balanced"])
 @pytest.mark.parametrize("partial", [False, True])
 @pytest.mark.parametrize("world", [1, 2, 3])
-def test_emulated_ranks_match_one_plan(world, partial):
+def test_emulated_ranks_match_one_plan(world, partial, split):
     lat, nets, pol = _case()
     rounds = 4
     usage_c, history_c, cost_c, costs_c, paths_c, per_round_c = _cpu_rounds(lat, nets, pol, rounds,
                                                                             partial)
     dev = apgar_b200.DeviceLattice(lat)
     try:
-        shares = [np.arange(len(nets))[r::world] for r in range(world)]
-        plans = [dev.plan(shard.split_nets(nets, r, world), generator="frontier")
+        if split == "balanced":
+            shares = shard.balanced_split(nets, world, lat.layers)
+        else:
+            shares = [np.arange(len(nets))[r::world] for r in range(world)]
+        plans = [dev.plan(np.ascontiguousarray(nets[shares[r]]), generator="frontier")
                  for r in range(world)]
         negs = [negotiate.Negotiation(p, pol) for p in plans]
         usages = [torch.zeros(negs[0].cells, dtype=torch.int32, device="cuda") for _ in range(world)]
