@@ -1,5 +1,7 @@
 // Lattice-mode frontier search: bucketed, label-correcting A* per net window,
-// one warp group per net, persistent work stealing over the nets of a class.
+// one warp group per net, persistent work stealing over the nets of a width
+// class, all classes in one launch of 16-warp CTAs that split into narrower
+// groups as the classes drain (lattice_frontier_kernel, at the end).
 //
 // A cell is keyed by f = g + h, with h the admissible, consistent
 // octile-plus-via bound to the goal.  The search works through key levels
