@@ -4,7 +4,10 @@
 // The exact-geometry stage that follows them in the reference (lattice points,
 // coalesced segments, obstacle clearance) stays on the host.
 //
-// Per query: a reached completion and a path of 1..9N states; the goal state
+// Per query: first the compact path's envelope (schema version 1, the
+// query's id and workspace owner, a slice inside the state array, non-empty
+// exactly when reached; src/gpu/planar_router.cc:1789-1805), then a reached
+// completion and a path of 1..9N states; the goal state
 // first and the canonical start state (start node, heading 8) last; every
 // state below 9N; then in forward order: no repeated state (a visited bit per
 // state), the start-only heading sentinel, one adjacent compiled legal edge
@@ -55,7 +58,14 @@ __global__ void validate_paths_kernel(PathCheckLaunch p) {
     const uint32_t start_state = q.start_node * 9u + 8u;
     const uint32_t* rev = p.states + c.state_offset;
     const uint64_t len = c.state_count;
-    if (r.completion != APGAR_B200_COMPLETION_REACHED) {
+    const bool reached = r.completion == APGAR_B200_COMPLETION_REACHED;
+    const uint64_t end = c.state_offset + static_cast<uint64_t>(c.state_count);
+    if (c.schema_version != 1u || c.query_id != q.query_id ||
+        c.workspace_owner != q.workspace_owner || end < c.state_offset || end > p.state_count ||
+        (reached ? c.state_count == 0u : c.state_count != 0u)) {
+      // the compact path envelope (src/gpu/planar_router.cc:1789-1805)
+      v.code = APGAR_B200_PATH_BOUNDS;
+    } else if (!reached) {
       v.code = APGAR_B200_PATH_NOT_REACHED;
     } else if (len == 0 || len > states || c.state_offset > p.state_count ||
                len > p.state_count - c.state_offset) {

@@ -269,9 +269,11 @@ APGAR_B200_API int apgar_b200_readback_route(void* pending,
 APGAR_B200_API int apgar_b200_release_route(void* pending);
 
 /* Structural validation of untrusted compact paths on the device: the
- * device-view checks of ValidateAndReconstructCompactGpuPath
- * (src/gpu/planar_router.cc:969-1067), in the reference's order, for every
- * query of a batch at once.  The exact-geometry stage that follows them in
+ * compact path envelope of the readback (schema version, query id, workspace
+ * owner, slice bounds, non-empty exactly when reached;
+ * src/gpu/planar_router.cc:1789-1805), then the device-view checks of
+ * ValidateAndReconstructCompactGpuPath (src/gpu/planar_router.cc:969-1067),
+ * in the reference's order, for every query of a batch at once.  The exact-geometry stage that follows them in
  * the reference (src/gpu/planar_router.cc:1069-1111) stays with the host.
  * Codes name the reference's invariant ids. */
 enum {
