@@ -60,6 +60,21 @@ struct PathCheckLaunch {
   uint32_t query_count;
 };
 
+// Full-workspace predecessor validation of a batch (labels and predecessors
+// [query][9 * nodes], as read back).
+struct PredCheckLaunch {
+  const apgar_b200_node_v1* nodes;
+  uint32_t node_count;
+  uint32_t orth, diag, bend;
+  const apgar_b200_batch_query_v1* queries;
+  const apgar_b200_policy_edge_v1* policy;
+  const uint64_t* labels;
+  const uint32_t* predecessors;
+  const uint8_t* partial;  // [query] 1 = partial (lower-bound) cost validation, or nullptr
+  unsigned long long* first;  // [query] least (state + 1) << 32 | code; ~0 when valid
+  uint32_t query_count;
+};
+
 // Reachability of each selected query's goal under its policy bans.
 struct ReachLaunch {
   const uint32_t* neighbors;  // [8][nodes]

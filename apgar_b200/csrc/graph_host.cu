@@ -34,6 +34,7 @@ namespace apgar_b200 {
 cudaError_t launch_graph_search(const GraphLaunch& launch, cudaStream_t stream);
 cudaError_t launch_validate_paths(const PathCheckLaunch& launch, cudaStream_t stream);
 cudaError_t launch_reach(const ReachLaunch& launch, cudaStream_t stream);
+cudaError_t launch_validate_predecessors(const PredCheckLaunch& launch, cudaStream_t stream);
 cudaError_t launch_path_segments(const apgar_b200_node_v1* nodes, uint32_t node_count, int64_t ox,
                                  int64_t oy, int64_t step, const apgar_b200_compact_path_v1* paths,
                                  const uint32_t* states, uint64_t state_count, uint32_t count,
@@ -761,6 +762,80 @@ extern "C" int apgar_b200_validate_compact_paths(
   } catch (const std::bad_alloc&) {
     return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "host allocation failed during path validation");
   }
+}
+
+extern "C" int apgar_b200_validate_predecessors(
+    void* view, const apgar_b200_batch_query_v1* queries, uint32_t query_count,
+    const apgar_b200_policy_edge_v1* policy_edges, uint64_t policy_edge_count, const uint8_t* partial,
+    const uint64_t* labels, const uint32_t* predecessors, apgar_b200_path_verdict* verdicts) {
+  if (view == nullptr ||
+      (query_count > 0 && (queries == nullptr || labels == nullptr || predecessors == nullptr ||
+                           verdicts == nullptr)) ||
+      (policy_edge_count > 0 && policy_edges == nullptr)) {
+    return invariant("predecessor validation received a null argument");
+  }
+  auto* v = static_cast<ViewObject*>(view);
+  if (int rc = check_device(v->device); rc != APGAR_B200_OK) return rc;
+  for (uint32_t i = 0; i < query_count; ++i) {
+    if (static_cast<uint64_t>(queries[i].policy_offset) + queries[i].policy_count > policy_edge_count) {
+      return invariant("predecessor validation query names policy edges outside the batch");
+    }
+  }
+  if (query_count == 0) {
+    clear_error();
+    return APGAR_B200_OK;
+  }
+  const uint64_t n = v->legal.size();
+  const uint64_t states = 9u * n * query_count;
+  DeviceBuffer<apgar_b200_batch_query_v1> d_q;
+  DeviceBuffer<apgar_b200_policy_edge_v1> d_pol;
+  DeviceBuffer<uint64_t> d_labels;
+  DeviceBuffer<uint32_t> d_preds;
+  DeviceBuffer<uint8_t> d_partial;
+  DeviceBuffer<unsigned long long> d_first;
+  APGAR_B200_CUDA("cudaMalloc(queries)", d_q.ensure(query_count));
+  APGAR_B200_CUDA("cudaMalloc(policy)", d_pol.ensure(std::max<uint64_t>(policy_edge_count, 1)));
+  APGAR_B200_CUDA("cudaMalloc(labels)", d_labels.ensure(std::max<uint64_t>(states, 1)));
+  APGAR_B200_CUDA("cudaMalloc(predecessors)", d_preds.ensure(std::max<uint64_t>(states, 1)));
+  APGAR_B200_CUDA("cudaMalloc(partial)", d_partial.ensure(query_count));
+  APGAR_B200_CUDA("cudaMalloc(first failures)", d_first.ensure(query_count));
+  APGAR_B200_CUDA("cudaMemcpy(queries)", cudaMemcpy(d_q.get(), queries, query_count * sizeof(*queries), cudaMemcpyHostToDevice));
+  if (policy_edge_count > 0) {
+    APGAR_B200_CUDA("cudaMemcpy(policy)", cudaMemcpy(d_pol.get(), policy_edges, policy_edge_count * sizeof(*policy_edges), cudaMemcpyHostToDevice));
+  }
+  APGAR_B200_CUDA("cudaMemcpy(labels)", cudaMemcpy(d_labels.get(), labels, states * 8, cudaMemcpyHostToDevice));
+  APGAR_B200_CUDA("cudaMemcpy(predecessors)", cudaMemcpy(d_preds.get(), predecessors, states * 4, cudaMemcpyHostToDevice));
+  if (partial != nullptr) {
+    APGAR_B200_CUDA("cudaMemcpy(partial)", cudaMemcpy(d_partial.get(), partial, query_count, cudaMemcpyHostToDevice));
+  }
+  APGAR_B200_CUDA("cudaMemset(first failures)", cudaMemset(d_first.get(), 0xFF, query_count * 8));
+  PredCheckLaunch L{};
+  L.nodes = v->nodes_dev.get();
+  L.node_count = static_cast<uint32_t>(n);
+  L.orth = v->header.orthogonal_step;
+  L.diag = v->header.diagonal_step;
+  L.bend = v->header.bend;
+  L.queries = d_q.get();
+  L.policy = d_pol.get();
+  L.labels = d_labels.get();
+  L.predecessors = d_preds.get();
+  L.partial = partial != nullptr ? d_partial.get() : nullptr;
+  L.first = d_first.get();
+  L.query_count = query_count;
+  APGAR_B200_CUDA("predecessor validation launch", launch_validate_predecessors(L, nullptr));
+  std::vector<unsigned long long> first(query_count);
+  APGAR_B200_CUDA("cudaMemcpy(first failures)", cudaMemcpy(first.data(), d_first.get(), query_count * 8, cudaMemcpyDeviceToHost));
+  for (uint32_t i = 0; i < query_count; ++i) {
+    apgar_b200_path_verdict out{};
+    if (first[i] != ~0ull) {
+      out.code = static_cast<uint32_t>(first[i] & 0xFFFFFFFFull);
+      const uint64_t key_state = first[i] >> 32;
+      out.failing_index = key_state == 0 ? 9ull * queries[i].start_node + 8u : key_state - 1u;
+    }
+    verdicts[i] = out;
+  }
+  clear_error();
+  return APGAR_B200_OK;
 }
 
 // Device scratch of one reachability chunk (visited bits and two node lists

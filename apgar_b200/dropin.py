@@ -55,6 +55,8 @@ VERDICT_DTYPE = np.dtype([("code", "<u4"), ("reserved", "<u4"), ("failing_index"
                           ("total_cost", "<u8")])
 PATH_CODES = {0: "ok", 1: "bounds", 2: "endpoint", 3: "cycle", 4: "heading", 5: "edge",
               6: "banned", 7: "not_reached"}
+PRED_CODES = {0: "ok", 1: "start", 2: "no_heading", 3: "unreachable", 4: "bounds",
+              5: "self_reference", 6: "edge", 7: "sentinel", 8: "infinite", 9: "banned", 10: "cost"}
 DISCONNECT_VERDICT_DTYPE = np.dtype([("code", "<u4"), ("reserved", "<u4"), ("reachable_nodes", "<u8")])
 DISCONNECT_CODES = {0: "confirmed", 1: "reachable", 2: "unbounded", 3: "not_claimed"}
 ROUTE_HEADER_DTYPE = np.dtype([
@@ -193,6 +195,22 @@ class View:
             _vp(policy_edges) if len(policy_edges) else None, ctypes.c_uint64(len(policy_edges)),
             _vp(results), _vp(compact), _vp(states) if len(states) else None,
             ctypes.c_uint64(len(states)), _vp(out)))
+        return out
+
+    def validate_predecessors(self, queries, policy_edges, labels, predecessors, partial=None):
+        """Device validation of full-workspace results (labels [Q][9N] uint64,
+        predecessors [Q][9N] uint32): one (code, reserved, first failing
+        state, 0) record per query, codes in PRED_CODES."""
+        queries = np.ascontiguousarray(queries)
+        policy_edges = np.ascontiguousarray(policy_edges)
+        labels = np.ascontiguousarray(labels, dtype=np.uint64)
+        predecessors = np.ascontiguousarray(predecessors, dtype=np.uint32)
+        part = None if partial is None else np.ascontiguousarray(partial, dtype=np.uint8)
+        out = np.zeros(len(queries), dtype=VERDICT_DTYPE)
+        _check(lib().apgar_b200_validate_predecessors(
+            self.handle, _vp(queries), ctypes.c_uint32(len(queries)),
+            _vp(policy_edges) if len(policy_edges) else None, ctypes.c_uint64(len(policy_edges)),
+            _vp(part) if part is not None else None, _vp(labels), _vp(predecessors), _vp(out)))
         return out
 
     def confirm_disconnected(self, queries, policy_edges, results):

@@ -303,6 +303,33 @@ APGAR_B200_API int apgar_b200_validate_compact_paths(
     const apgar_b200_batch_result_v1* results, const apgar_b200_compact_path_v1* compact_paths,
     const uint32_t* path_states, uint64_t path_state_count, apgar_b200_path_verdict* verdicts);
 
+/* Validation of untrusted full-workspace results on the device: the checks of
+ * ValidateAllPredecessors (src/gpu/planar_router.cc:492-611) over every
+ * heading state of every query, in the reference's order, reporting each
+ * query's first failure (state index in failing_index).  `labels` [query][9N]
+ * uint64 and `predecessors` [query][9N] uint32 are host arrays as read back
+ * (apgar_b200_readback_batch_workspace, or one query of
+ * apgar_b200_readback_route); `partial` [query] selects the lower-bound cost
+ * check of bounded results (1) instead of the exact one (0), or is NULL (all
+ * exact).  Codes: */
+enum {
+  APGAR_B200_PRED_OK = 0,
+  APGAR_B200_PRED_START = 1,          /* start state not labelled 0 without predecessor */
+  APGAR_B200_PRED_NO_HEADING = 2,     /* a heading-8 state away from the start is reachable */
+  APGAR_B200_PRED_UNREACHABLE = 3,    /* an unreachable state carries a predecessor */
+  APGAR_B200_PRED_BOUNDS = 4,         /* predecessor index out of bounds */
+  APGAR_B200_PRED_SELF_REFERENCE = 5, /* gpu.predecessor.self_reference.v1 */
+  APGAR_B200_PRED_EDGE = 6,           /* not one adjacent compiled legal edge */
+  APGAR_B200_PRED_SENTINEL = 7,       /* predecessor uses heading 8 away from the start */
+  APGAR_B200_PRED_INFINITE = 8,       /* reachable state after an unreachable predecessor */
+  APGAR_B200_PRED_BANNED = 9,         /* gpu.policy.banned_predecessor.v1 */
+  APGAR_B200_PRED_COST = 10           /* label does not reconstruct the scalar cost */
+};
+APGAR_B200_API int apgar_b200_validate_predecessors(
+    void* view, const apgar_b200_batch_query_v1* queries, uint32_t query_count,
+    const apgar_b200_policy_edge_v1* policy_edges, uint64_t policy_edge_count, const uint8_t* partial,
+    const uint64_t* labels, const uint32_t* predecessors, apgar_b200_path_verdict* verdicts);
+
 /* Confirmation of DISCONNECTED results on the device, in place of the CPU A*
  * rerun of ConfirmDisconnectedWithCpuOracle (src/gpu/planar_router.cc:629-667).
  * The CPU A* (src/routing/cpu_astar.cc:323-512) reports kDisconnected exactly

@@ -375,6 +375,77 @@ def unpack_bits_dense(words, width):
     return bits.reshape(np.asarray(words).shape[:-1] + (width,)).astype(bool)
 
 
+PRED_CODES = {0: "ok", 1: "start", 2: "no_heading", 3: "unreachable", 4: "bounds",
+              5: "self_reference", 6: "edge", 7: "sentinel", 8: "infinite", 9: "banned", 10: "cost"}
+
+
+def validate_predecessors(nodes, costs, start, labels, preds, orth_s=0, diag_s=0, bend_s=0,
+                          policy=None, partial=False):
+    """The checks of ValidateAllPredecessors (src/gpu/planar_router.cc:492-611)
+    over one query's heading-state labels and predecessors, in state order;
+    returns (code name, failing state) of the first failure, ("ok", 0) if
+    none."""
+    U64 = (1 << 64) - 1
+    INV = 0xFFFFFFFF
+    orth, diag, bend = (int(c) for c in costs)
+    n = len(nodes)
+    S = 9 * n
+    labels = [int(x) for x in labels]
+    preds = [int(x) for x in preds]
+    adj = {}
+    if policy is not None:
+        for e in policy:
+            adj[int(e["physical_edge_index"])] = int(e["adjustment"])
+    if start >= n:
+        return "start", 9 * start + 8
+    start_state = 9 * start + 8
+    if labels[start_state] != 0 or preds[start_state] != INV:
+        return "start", start_state
+    dxs = (1, 1, 0, -1, -1, -1, 0, 1)
+    dys = (0, 1, 1, 1, 0, -1, -1, -1)
+    for state in range(S):
+        if state == start_state:
+            continue
+        label, pred, inc = labels[state], preds[state], state % 9
+        if inc == 8:
+            if label != U64 or pred != INV:
+                return "no_heading", state
+            continue
+        if label == U64:
+            if pred != INV:
+                return "unreachable", state
+            continue
+        if pred == INV and partial:
+            continue
+        if pred >= S:
+            return "bounds", state
+        if pred == state:
+            return "self_reference", state
+        node, pnode = state // 9, pred // 9
+        a, b = nodes[pnode], nodes[node]
+        if (int(a["layer"]) != int(b["layer"]) or int(b["lattice_x"]) - int(a["lattice_x"]) != dxs[inc]
+                or int(b["lattice_y"]) - int(a["lattice_y"]) != dys[inc]
+                or int(a["neighbors"][inc]) != node or not (int(a["legal_edges"]) >> inc) & 1):
+            return "edge", state
+        ph = pred % 9
+        if ph == 8 and pred != start_state:
+            return "sentinel", state
+        if labels[pred] == U64:
+            return "infinite", state
+        edge = pnode * 8 + inc if inc < 4 else node * 8 + inc - 4
+        pen = adj.get(edge, 0)
+        if pen == U64:
+            return "banned", state
+        t = (diag + diag_s) if inc & 1 else (orth + orth_s)
+        if ph != 8 and ph != inc:
+            t += bend + bend_s
+        t += pen
+        expected = labels[pred] + t if t < U64 else None
+        if expected is None or expected > U64 - 1 or (expected > label if partial else expected != label):
+            return "cost", state
+    return "ok", 0
+
+
 def graph_predecessors(nodes, costs, start, labels, orth_s=0, diag_s=0, bend_s=0, policy=None):
     """Canonical predecessor of every state from exact labels."""
     L = lib()
