@@ -50,3 +50,53 @@ def test_save_and_load(tmp_path):
     autotune.load(path)
     assert autotune._CACHE[key][0] == autotune.Schedule(200, 2, apgar_b200.class_bounds(12, 15, 18, 21))
     del autotune._CACHE[key]
+
+
+class _FakeLattice:
+    layers, height, width = 4, 512, 512
+    orth, diag, via = 10, 14, 50
+
+
+def _fake_timer(table):
+    """time_schedule stand-in: ms from `table` keyed by the schedule's
+    describe(), the same costs for every schedule."""
+    def timer(lattice, nets, s, warmup=1, reps=5):
+        d = s.describe()
+        key = (d["bucket_width"], d["chain"], tuple(d["class_log2_limits"] or ()))
+        return table.get(key, 20.0), np.arange(len(nets), dtype=np.uint32)
+    return timer
+
+
+def test_coordinate_descent_keeps_gains_above_the_noise(monkeypatch):
+    lat = synth.make_lattice(3, 2, 256, 0.2)
+    nets = synth.make_nets(lat, 4, 50, hpwl_median=40.0, hpwl_sigma=1.0, margin=16)
+    table = {
+        (0, 0, ()): 20.0,
+        (200, 0, ()): 19.9,                 # 0.5% better: noise, not taken
+        (400, 0, ()): 25.0,
+        (0, 0, (12, 15, 18, 21)): 18.0,     # 10% better: taken
+        (0, 0, (12, 15, 18, 20)): 17.0,     # one refinement step further
+        (0, 2, (12, 15, 18, 20)): 16.9,     # chaining within the noise: not taken
+    }
+    monkeypatch.setattr(autotune, "time_schedule", _fake_timer(table))
+    best, rows = autotune.tune(_FakeLattice, nets, use_cache=False)
+    assert best == autotune.Schedule(0, 0, apgar_b200.class_bounds(12, 15, 18, 20))
+    assert rows[0][0] == autotune.DEFAULT.describe()
+    assert len(rows) >= 1 + 3 + len(autotune.BOUND_SETS) - 1 + 1
+
+
+def test_a_schedule_that_changes_a_result_raises(monkeypatch):
+    lat = synth.make_lattice(3, 2, 256, 0.2)
+    nets = synth.make_nets(lat, 4, 20, hpwl_median=40.0, hpwl_sigma=1.0, margin=16)
+    calls = []
+
+    def timer(lattice, nets_, s, warmup=1, reps=5):
+        calls.append(s)
+        cost = np.zeros(len(nets_), np.uint32)
+        if len(calls) == 3:
+            cost[0] = 1  # the third candidate disagrees
+        return 20.0, cost
+
+    monkeypatch.setattr(autotune, "time_schedule", timer)
+    with pytest.raises(RuntimeError):
+        autotune.tune(_FakeLattice, nets, use_cache=False)
