@@ -69,3 +69,26 @@ def test_view_upload_rejects_corrupt_views_without_gpu():
         assert e.code == 4 and "upload rejected" in e.detail
     else:
         raise AssertionError("corrupt view accepted")
+
+
+def test_new_entry_points_refuse_null_handles_on_the_host():
+    """Each refuses a null handle or argument with INTERNAL_INVARIANT (4) and a
+    'null' detail, before any device call."""
+    lib = apgar_b200.lib()
+    calls = [
+        lambda: lib.apgar_b200_lattice_validate(None, None, ctypes.c_uint32(1), None, None,
+                                                ctypes.c_uint64(0), None),
+        lambda: lib.apgar_b200_confirm_disconnected(None, None, ctypes.c_uint32(1), None,
+                                                    ctypes.c_uint64(0), None, None),
+        lambda: lib.apgar_b200_validate_predecessors(None, None, ctypes.c_uint32(1), None,
+                                                     ctypes.c_uint64(0), None, None, None, None),
+        lambda: lib.apgar_b200_negotiation_set_usage_buffer(None, None),
+    ]
+    buf = ctypes.create_string_buffer(256)
+    for call in calls:
+        assert call() == 4
+        lib.apgar_b200_last_error(buf, ctypes.c_size_t(256))
+        assert b"null" in buf.value, buf.value
+    # a negotiation step without a negotiation, and with an unknown phase
+    assert lib.apgar_b200_negotiation_step(None, ctypes.c_uint32(0), ctypes.c_uint32(0),
+                                           ctypes.c_uint32(0), None) == 4
