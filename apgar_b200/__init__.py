@@ -213,6 +213,14 @@ class DeviceLattice:
         count = len(nets)
         if out is not None:
             results, paths = out
+            # the C side writes count records and up to paths.size cells
+            if not (isinstance(results, np.ndarray) and results.dtype == RESULT_DTYPE
+                    and results.flags.c_contiguous and results.size >= count):
+                raise ValueError("out[0] must be a C-contiguous RESULT_DTYPE array of at least "
+                                 f"{count} records")
+            if not (isinstance(paths, np.ndarray) and paths.dtype == np.uint32
+                    and paths.flags.c_contiguous):
+                raise ValueError("out[1] must be a C-contiguous uint32 array")
         else:
             results = np.empty(count, dtype=RESULT_DTYPE)
             cap = path_capacity or int(8 * (nets["win_w"].astype(np.int64)
@@ -254,14 +262,22 @@ class DeviceLattice:
                       out=None):
         """``route`` without device allocation: the library's fixed scratch
         (``NOALLOC_SCRATCH_BYTES`` per device, at most ``NOALLOC_MAX_NETS``
-        nets) holds the workspace, and work goes to ``stream``.  Calls that
-        overlap in time share that scratch and must be serialised by the
-        caller.  ``out`` may supply preallocated (results, paths) host arrays
-        so that the call allocates nothing in Python either."""
+        nets) holds the workspace, and work goes to ``stream``.  Calls share
+        that scratch and take one process-wide lock, so concurrent calls run
+        one after another.  ``out`` may supply preallocated (results, paths)
+        host arrays so that the call allocates nothing in Python either."""
         nets = np.ascontiguousarray(nets)
         count = len(nets)
         if out is not None:
             results, paths = out
+            # the C side writes count records and up to paths.size cells
+            if not (isinstance(results, np.ndarray) and results.dtype == RESULT_DTYPE
+                    and results.flags.c_contiguous and results.size >= count):
+                raise ValueError("out[0] must be a C-contiguous RESULT_DTYPE array of at least "
+                                 f"{count} records")
+            if not (isinstance(paths, np.ndarray) and paths.dtype == np.uint32
+                    and paths.flags.c_contiguous):
+                raise ValueError("out[1] must be a C-contiguous uint32 array")
         else:
             results = np.empty(count, dtype=RESULT_DTYPE)
             cap = int(8 * (nets["win_w"].astype(np.int64) + nets["win_h"].astype(np.int64)).sum()

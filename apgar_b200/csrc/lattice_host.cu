@@ -1079,22 +1079,27 @@ extern "C" int apgar_b200_lattice_accumulate_usage(void* plan, uint32_t* usage, 
 // plan in fixed file-scope host arrays.  It creates no stream, event or pinned
 // buffer; every copy and launch goes to the caller's stream.
 //
-// The scratch is shared by every call on a device: two calls whose work
-// overlaps in time (two host threads, or calls on different streams) race on
-// it and on the host staging arrays, and corrupt each other's results.
-// Callers serialise them.
+// The scratch is shared by every call on a device, and the host staging
+// arrays by every call of the process.  One process-wide mutex is held from
+// the admission pass to the final stream synchronisation, so calls from
+// several host threads (on one device or on several) run one after another.
+// Without it, overlapping calls would race: one call's plan records could be
+// uploaded beside another call's nets, and the sweep would then index label
+// slabs laid out for the other batch, which can write out of bounds and fault
+// the GPU rather than only corrupt results.  Work that another process or
+// a caller's own kernels put on the same scratch cannot exist: the array is
+// private to this library and this process.
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[APGAR_B200_NOALLOC_SCRATCH_BYTES];
 
 namespace apgar_b200 {
 namespace {
 
-constexpr int kNoallocMaxDevices = 64;
 constexpr uint64_t kNoallocAlign = 256;
 
-// Device address of g_noalloc_scratch per device ordinal; 0 until the first
-// call on that device looks it up (with that device current).
-std::atomic<uintptr_t> g_noalloc_base[kNoallocMaxDevices];
+// Serialises allocation-free calls (host staging, uploads, launches and the
+// final synchronisation).  A std::mutex allocates nothing.
+std::mutex g_noalloc_mutex;
 
 struct NoallocStaging {
   NetPlan plans[APGAR_B200_NOALLOC_MAX_NETS];
@@ -1104,20 +1109,16 @@ struct NoallocStaging {
 };
 NoallocStaging g_noalloc_host;
 
-int noalloc_scratch(int device, unsigned char** out) {
-  if (device < 0 || device >= kNoallocMaxDevices) {
-    return set_error(APGAR_B200_UNSUPPORTED,
-                     "allocation-free route supports device ordinals below 64");
-  }
-  uintptr_t base = g_noalloc_base[device].load(std::memory_order_acquire);
-  if (base == 0) {
-    void* ptr = nullptr;
-    APGAR_B200_CUDA("cudaGetSymbolAddress(allocation-free scratch)",
-                    cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
-    base = reinterpret_cast<uintptr_t>(ptr);
-    g_noalloc_base[device].store(base, std::memory_order_release);
-  }
-  *out = reinterpret_cast<unsigned char*>(base);
+// Device address of g_noalloc_scratch on the current device.  In host code
+// the array's name is only a host-side stand-in, so every call looks the
+// address up again (with the lattice's device current, which the entry point
+// has checked): the lookup allocates nothing, and a module reloaded after a
+// device reset may sit at another address.
+int noalloc_scratch(unsigned char** out) {
+  void* ptr = nullptr;
+  APGAR_B200_CUDA("cudaGetSymbolAddress(allocation-free scratch)",
+                  cudaGetSymbolAddress(&ptr, g_noalloc_scratch));
+  *out = static_cast<unsigned char*>(ptr);
   return APGAR_B200_OK;
 }
 
@@ -1226,7 +1227,7 @@ int route_noalloc(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, u
                          " bytes; split the batch or use apgar_b200_lattice_route");
   }
   unsigned char* base = nullptr;
-  if (int rc = noalloc_scratch(lat->device, &base); rc != APGAR_B200_OK) return rc;
+  if (int rc = noalloc_scratch(&base); rc != APGAR_B200_OK) return rc;
   auto* d_nets = reinterpret_cast<apgar_b200_lattice_net*>(base + nets_at);
   auto* d_plans = reinterpret_cast<NetPlan*>(base + plans_at);
   auto* d_results = reinterpret_cast<apgar_b200_lattice_result*>(base + results_at);
@@ -1291,6 +1292,9 @@ int route_noalloc(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, u
   if (path_total != nullptr) *path_total = total;
   if (paths != nullptr && total > 0) {
     if (total > path_capacity) {
+      // A pinned results buffer makes the copy above asynchronous: finish it
+      // before returning, so the stream is synchronised on every return.
+      APGAR_B200_CUDA("cudaStreamSynchronize(route)", cudaStreamSynchronize(stream));
       return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "path output buffer is too small");
     }
     APGAR_B200_CUDA("cudaMemcpyAsync(paths)",
@@ -1316,6 +1320,7 @@ extern "C" int apgar_b200_lattice_route_noalloc(void* lattice, const apgar_b200_
   }
   auto* lat = static_cast<LatticeObject*>(lattice);
   if (int rc = check_device(lat->device); rc != APGAR_B200_OK) return rc;
+  std::lock_guard<std::mutex> hold(g_noalloc_mutex);
   const int rc = route_noalloc(lat, nets, count, max_sweeps, static_cast<cudaStream_t>(stream),
                                results, paths, path_capacity, path_total);
   if (rc == APGAR_B200_OK) clear_error();

@@ -86,8 +86,21 @@ APGAR_B200_API int apgar_b200_query_metadata(apgar_b200_metadata* out);
 /* =================== A. drop-in seam (reference V1 records) =================== */
 
 /* Generator values of PlanarGenerator (planar_router.h:42-45) plus the value
- * this backend adds for its own persistent engine; the descriptor of the new
- * value is described in INTEGRATION.md. */
+ * this backend adds for its own persistent engine.
+ *
+ * APGAR_B200_GENERATOR_B200_PERSISTENT searches a whole batch in one launch
+ * with no host round trips and returns compact paths.  Its generator
+ * descriptor (the reference's DescribePlanarGenerator, planar_router.h:56-100)
+ * is: workspace kSweep (compact-path readback), chunk_rounds = the request's
+ * maximum_rounds, fixed_launches = 3 (search, offset scan, pack),
+ * kernels_per_round = 0, launches_once_per_chunk = false, and host_chunked =
+ * false, a flag the descriptor gains with this value.  For host_chunked ==
+ * false the telemetry check expects 0 blocking status readbacks,
+ * fixed_launches + finalization launches, and device bytes
+ * Q*(120 + 120 + 32) + E*16 + Q*S*8 + Q*N*12 + Q*S*4 + 16 for Q queries,
+ * E policy edges, N nodes and S = 9N states.  The two stock generators keep
+ * their descriptors; this engine serves them with the same single launch and
+ * reports its own counts. */
 enum {
   APGAR_B200_GENERATOR_BUCKETED_FRONTIER = 0, /* PlanarGenerator::kBucketedFrontier */
   APGAR_B200_GENERATOR_HEADING_SWEEP = 1,     /* PlanarGenerator::kHeadingAwareSweep */
@@ -444,12 +457,24 @@ APGAR_B200_API int apgar_b200_lattice_route(void* lattice, const apgar_b200_latt
  *    stream).  Width classes run one after another on that stream.  The call
  *    synchronises only that stream before it returns.
  *  - It takes no cancel flag.
- *  - The first call on a device looks up the array's device address with that
- *    device current.  That call should come before any stream capture on the
- *    device.
- *  - The scratch is shared: calls whose work overlaps in time race on it and
- *    corrupt each other's results.  This includes two host threads, or calls
- *    on different streams.  Callers serialise them. */
+ *  - Every call looks up the array's device address (cudaGetSymbolAddress,
+ *    which allocates nothing) with the lattice's device current.  The first
+ *    call on a device also loads the module there, so it should come before
+ *    any stream capture on that device.  Do not call it across a device
+ *    reset of the lattice's device.
+ *  - The array is part of the library's device image: every process that
+ *    loads the library holds APGAR_B200_NOALLOC_SCRATCH_BYTES on each device
+ *    where it uses the library, until exit, whether or not it calls this
+ *    entry point.
+ *  - The scratch is shared by every call on a device and the host staging by
+ *    every call of the process.  Calls therefore take one process-wide lock
+ *    from admission to the final stream synchronisation, so calls from
+ *    several host threads, on one device or several, run one after another.
+ *    Overlapping calls would race on the scratch and the staging; a plan
+ *    uploaded beside another call's nets could make the sweep write outside
+ *    its slabs and fault the GPU, not just corrupt results.  The scratch
+ *    keeps the last call's contents; each call clears what must start at
+ *    zero. */
 #define APGAR_B200_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 #define APGAR_B200_NOALLOC_MAX_NETS 4096u
 APGAR_B200_API int apgar_b200_lattice_route_noalloc(void* lattice, const apgar_b200_lattice_net* nets,
