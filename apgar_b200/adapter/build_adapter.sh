@@ -13,7 +13,7 @@
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
 ROOT="$(cd "$HERE/../.." && pwd)"
-REF="${APGAR_REFERENCE:-/root/reference}"
+REF="${APGAR_REFERENCE:-$(cat "$ROOT/oracle/_ref/reference_root.txt" 2>/dev/null || echo /root/reference)}"
 OUT="$HERE/_build"
 CXX="${CXX:-g++}"
 FLAGS=(-std=c++20 -O2 -Wall -Wextra -fPIC -I"$REF/include" -I"$REF" -I"$ROOT/include")

@@ -70,6 +70,24 @@ def lo_inf() -> int:
     return 0xFFFFFFFF
 
 
+def reference_root():
+    """Root of the reference source tree, or None where it is absent.
+
+    ``APGAR_REFERENCE`` names it; otherwise the tree that ``oracle/build_ref.sh``
+    last compiled into ``oracle/_ref`` (recorded there in
+    ``reference_root.txt``).  Tests that read reference sources or run the
+    compiled reference skip with a message when this is None."""
+    root = os.environ.get("APGAR_REFERENCE")
+    if not root:
+        stamp = os.path.join(_HERE, "_ref", "reference_root.txt")
+        if os.path.exists(stamp):
+            with open(stamp) as f:
+                root = f.read().strip()
+    if root and os.path.isdir(os.path.join(root, "src")):
+        return root
+    return None
+
+
 def build() -> str:
     """Compile the oracle with make (gcc); returns the library path."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)
@@ -165,6 +183,22 @@ def dijkstra_batch(lat, nets, threads=None, path_cap_per_net=None, cell_cost=Non
             o = int(offsets[i])
             out.append(paths[o:o + n].copy())
     return costs, out
+
+
+def astar_path(lat, net_row, path_cap=1 << 22):
+    """(cost, expanded states, forward A* path as global cell ids or None) of
+    the restatement of RouteWithCpuAStar for one net."""
+    L = lib()
+    ref = LatticeRef(lat)
+    net = np.ascontiguousarray(np.asarray(net_row).reshape(1))
+    path = np.empty(path_cap, dtype=np.uint32)
+    plen = ctypes.c_uint32(0)
+    expanded = ctypes.c_uint64(0)
+    L.lo_astar_path.restype = ctypes.c_uint32
+    cost = L.lo_astar_path(ctypes.byref(ref.c), _net_ptr(net), ctypes.byref(expanded), _ptr(path),
+                           ctypes.c_uint32(path_cap), ctypes.byref(plen))
+    n = plen.value
+    return cost, expanded.value, (path[:n].copy() if 0 < n != 0xFFFFFFFF else None)
 
 
 def astar_batch(lat, nets, threads=None):

@@ -5,6 +5,7 @@
 #                                (CPU A*), device-view flattening, host GPU
 #                                dispatch/validation, corpus + KiCad adapter
 #   oracle/_ref/ref_fixtures     driver that writes tests/golden fixtures
+#   oracle/_ref/ref_lattice      compile + CPU A* on box-obstacle lattices
 # TEST INFRASTRUCTURE ONLY.  Needs the reference tree (REF, default
 # /root/reference) and g++ with C++20; the GPU box only uses prebuilt outputs.
 set -euo pipefail
@@ -44,4 +45,7 @@ done
 rm -f "$OUT/libapgar_ref.a"
 ar rcs "$OUT/libapgar_ref.a" "${OBJS[@]}"
 "$CXX" "${FLAGS[@]}" "$HERE/ref_fixtures.cc" "$OUT/libapgar_ref.a" -o "$OUT/ref_fixtures"
+"$CXX" "${FLAGS[@]}" "$HERE/ref_lattice.cc" "$OUT/libapgar_ref.a" -o "$OUT/ref_lattice"
+# where the checker was built from, for the tests that read reference files
+(cd "$REF" && pwd) > "$OUT/reference_root.txt"
 echo "$OUT"

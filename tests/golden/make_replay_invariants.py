@@ -31,4 +31,13 @@ def main(root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) > 1:
+        root = sys.argv[1]
+    else:
+        sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
+        import oracle
+
+        root = oracle.reference_root()
+        if root is None:
+            sys.exit("usage: make_replay_invariants.py REFERENCE_ROOT (or set APGAR_REFERENCE)")
+    main(root)

@@ -16,12 +16,13 @@ import pytest
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 BUILD = os.path.join(ROOT, "apgar_b200", "adapter", "build_adapter.sh")
 CHECK = os.path.join(ROOT, "apgar_b200", "adapter", "_build", "adapter_check")
-REF = os.environ.get("APGAR_REFERENCE", "/root/reference")
 
 
 def test_shim_compiles_against_the_reference_interface():
-    if not os.path.isdir(os.path.join(REF, "include", "apgar")):
-        pytest.skip("reference headers are absent")
+    import oracle
+
+    if oracle.reference_root() is None:
+        pytest.skip("reference sources are absent (set APGAR_REFERENCE or run oracle/build_ref.sh)")
     out = subprocess.run(["bash", BUILD, "--check"], capture_output=True, text=True)
     assert out.returncode == 0, out.stderr[-2000:]
 

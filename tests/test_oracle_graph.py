@@ -84,10 +84,11 @@ def test_fixtures_regenerate_from_the_reference(tmp_path):
 
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     exe = os.path.join(root, "oracle", "_ref", "ref_fixtures")
-    ref = os.environ.get("APGAR_REFERENCE", "/root/reference")
+    ref = oracle.reference_root()
+    if ref is None or not os.path.exists(exe):
+        pytest.skip("reference sources or the compiled reference checker are absent "
+                    "(set APGAR_REFERENCE or run oracle/build_ref.sh)")
     pcb = os.path.join(ref, "tests", "fixtures", "m1_exactness.kicad_pcb")
-    if not (os.path.exists(exe) and os.path.exists(pcb)):
-        pytest.skip("reference sources or the compiled reference checker are absent")
     subprocess.run([exe, pcb, str(tmp_path)], check=True, stdout=subprocess.DEVNULL)
     committed = os.path.join(root, "tests", "golden", "ref_corpus")
     names = sorted(os.listdir(committed))
