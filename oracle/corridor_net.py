@@ -17,9 +17,35 @@ GRID = 64
 CIN0 = 16
 CH = 32
 
+# Exact mode (``exact()``): every rounding point is the identity and the
+# arithmetic is float64, so the backward can be checked against central finite
+# differences of the forward.  The kernels' arithmetic is the default mode.
+_EXACT = False
+
+
+class exact:
+    """Context manager: run the restatement in float64 without bf16 rounding."""
+
+    def __enter__(self):
+        global _EXACT
+        self._prev, _EXACT = _EXACT, True
+        return self
+
+    def __exit__(self, *exc):
+        global _EXACT
+        _EXACT = self._prev
+        return False
+
+
+def _ft():
+    return np.float64 if _EXACT else np.float32
+
 
 def bf16(x):
-    """Round float32 to bfloat16 (nearest even), returned as float32."""
+    """Round float32 to bfloat16 (nearest even), returned as float32 (in
+    exact mode: the value itself, as float64)."""
+    if _EXACT:
+        return np.asarray(x, dtype=np.float64)
     u = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
     u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
     return u.astype(np.uint32).view(np.float32)
@@ -52,7 +78,7 @@ def unflatten(params):
 
 def flatten(parts):
     o, total = offsets()
-    out = np.zeros(total, np.float32)
+    out = np.zeros(total, _ft())
     for k, (a, s) in o.items():
         out[a:a + int(np.prod(s))] = parts[k].reshape(-1)
     return out
@@ -80,8 +106,8 @@ def _shift(x, dy, dx):
 def conv(x, w, mask):
     """acc[cell][co] = sum_{tap, ci} x[cell + tap][ci] * w[co][tap][ci] over
     window cells (x zero outside the window), f32; zero outside the window."""
-    x = np.where(mask[..., None], x, 0.0).astype(np.float32)
-    acc = np.zeros(x.shape[:3] + (w.shape[0],), np.float32)
+    x = np.where(mask[..., None], x, 0.0).astype(_ft())
+    acc = np.zeros(x.shape[:3] + (w.shape[0],), _ft())
     for t in range(9):
         dy, dx = t // 3 - 1, t % 3 - 1
         acc += np.einsum("nyxc,oc->nyxo", _shift(x, dy, dx), w[:, t, :], optimize=True)
@@ -97,7 +123,7 @@ def conv_layer(x, params, layer, mask):
 def head(a5, params, mask):
     p = unflatten(params)
     a5 = np.where(mask[..., None], a5, 0.0)
-    z = np.zeros(a5.shape[:3], np.float32)
+    z = np.zeros(a5.shape[:3], _ft())
     for t in range(9):
         dy, dx = t // 3 - 1, t % 3 - 1
         z += _shift(a5, dy, dx) @ p["w6"][t]
@@ -107,15 +133,15 @@ def head(a5, params, mask):
 def loss_grad(logits, labels, mask, pos_weight):
     """(loss, dlogit) of the kernels' weighted cross-entropy."""
     n = logits.shape[0]
-    cells = mask.reshape(n, -1).sum(axis=1).astype(np.float32)
+    cells = mask.reshape(n, -1).sum(axis=1).astype(_ft())
     norm = (1.0 / (cells * n))[:, None, None]
-    t = labels.astype(np.float32)
-    wgt = np.where(labels != 0, pos_weight, 1.0).astype(np.float32)
-    z = logits.astype(np.float32)
+    t = labels.astype(_ft())
+    wgt = np.where(labels != 0, pos_weight, 1.0).astype(_ft())
+    z = logits.astype(_ft())
     sig = 1.0 / (1.0 + np.exp(-z))
     g = np.where(mask, wgt * (sig - t) * norm, 0.0)
     l = np.where(mask, wgt * (np.maximum(z, 0) - z * t + np.log1p(np.exp(-np.abs(z)))) * norm, 0.0)
-    return float(l.sum()), g.astype(np.float32)
+    return float(l.sum()), g.astype(_ft())
 
 
 def head_backward(a5, params, dlogit, mask):
@@ -123,13 +149,13 @@ def head_backward(a5, params, dlogit, mask):
     p = unflatten(params)
     a5 = np.where(mask[..., None], a5, 0.0)
     da = np.zeros_like(a5)
-    dw6 = np.zeros((9, CH), np.float32)
+    dw6 = np.zeros((9, CH), _ft())
     for t in range(9):
         dy, dx = t // 3 - 1, t % 3 - 1
         da += _shift(dlogit, -dy, -dx)[..., None] * p["w6"][t][None, None, None, :]
         dw6[t] = np.einsum("nyx,nyxc->c", dlogit, _shift(a5, dy, dx))
     dpre = np.where(mask[..., None] & (a5 > 0), bf16(da), 0.0)
-    return dpre, dw6, np.array([dlogit.sum()], np.float32)
+    return dpre, dw6, np.array([dlogit.sum()], _ft())
 
 
 def input_grad(dpre, params, layer, gate, mask):
@@ -147,8 +173,8 @@ def weight_grad(x, dpre, mask):
     """(dw[co][tap][ci], db[co]) = sums over window cells."""
     x = np.where(mask[..., None], x, 0.0)
     dpre = np.where(mask[..., None], dpre, 0.0)
-    dw = np.zeros((CH, 9, x.shape[-1]), np.float32)
+    dw = np.zeros((CH, 9, x.shape[-1]), _ft())
     for t in range(9):
         dy, dx = t // 3 - 1, t % 3 - 1
         dw[:, t, :] = np.einsum("nyxo,nyxc->oc", dpre, _shift(x, dy, dx), optimize=True)
-    return dw, dpre.sum(axis=(0, 1, 2)).astype(np.float32)
+    return dw, dpre.sum(axis=(0, 1, 2)).astype(_ft())
