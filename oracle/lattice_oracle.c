@@ -313,15 +313,23 @@ static uint64_t octile(const lo_lattice* lat, int dx, int dy, int dl) {
   return planar + al * lat->via;
 }
 
-uint32_t lo_astar(const lo_lattice* lat, const lo_net* net, uint64_t* expanded_out) {
+/* Shared body of lo_astar and lo_astar_path.  With `path` non-NULL every
+ * accepted relaxation records its predecessor state, as the reference's
+ * SearchRecord does (cpu_astar.cc:495-497), and the goal state's chain is
+ * written forward (start first) as global cell ids. */
+static uint32_t astar_run(const lo_lattice* lat, const lo_net* net, uint64_t* expanded_out,
+                          uint32_t* path, uint32_t path_cap, uint32_t* path_len) {
   win_ctx c;
   ctx_init(&c, lat, net);
   const size_t cells = (size_t)c.L * c.w * c.h;
   /* Record per (cell, heading): heading 0..7 planar, 8 start / none, 9 via up,
-   * 10 via down.  Only the cost is needed here. */
+   * 10 via down. */
   const size_t states = cells * 11;
   uint32_t* g = (uint32_t*)malloc(states * sizeof(uint32_t));
   for (size_t i = 0; i < states; ++i) g[i] = LO_INF;
+  uint64_t* pred = path ? (uint64_t*)malloc(states * sizeof(uint64_t)) : NULL;
+  size_t goal_state = (size_t)-1;
+  if (path_len) *path_len = 0;
   const int sl = (int)net->start_layer, sx = (int)(net->start_x - net->win_x0),
             sy = (int)(net->start_y - net->win_y0);
   const int gl = (int)net->goal_layer, gx = (int)(net->goal_x - net->win_x0),
@@ -341,6 +349,7 @@ uint32_t lo_astar(const lo_lattice* lat, const lo_net* net, uint64_t* expanded_o
       if (g[ci * 11 + (size_t)cur.heading] != cur.g) continue;
       if (cur.l == gl && cur.x == gx && cur.y == gy) {
         result = (uint32_t)cur.g;
+        goal_state = ci * 11 + (size_t)cur.heading;
         break;
       }
       ++expanded;
@@ -365,6 +374,7 @@ uint32_t lo_astar(const lo_lattice* lat, const lo_net* net, uint64_t* expanded_o
         const size_t ni = cell_index(&c, nl, nx, ny) * 11 + (size_t)heading;
         if (g[ni] != LO_INF && g[ni] <= ng) continue;
         g[ni] = (uint32_t)ng;
+        if (pred) pred[ni] = ci * 11 + (size_t)cur.heading;
         const uint64_t hh = octile(lat, gx - nx, gy - ny, gl - nl);
         astar_item it = {ng + hh, hh, ng, nl, ny, nx, heading, seq++};
         aheap_push(&hp, it);
@@ -372,9 +382,45 @@ uint32_t lo_astar(const lo_lattice* lat, const lo_net* net, uint64_t* expanded_o
     }
     free(hp.items);
   }
+  if (path && goal_state != (size_t)-1) {
+    /* walk back to the start state (heading 8 at the start cell) */
+    const size_t start_state = cell_index(&c, sl, sx, sy) * 11 + 8;
+    uint32_t n = 0;
+    size_t st = goal_state;
+    for (;;) {
+      ++n;
+      if (st == start_state) break;
+      st = (size_t)pred[st];
+    }
+    if (n > path_cap) {
+      if (path_len) *path_len = UINT32_MAX;
+    } else {
+      st = goal_state;
+      for (uint32_t k = n; k-- > 0;) {
+        const size_t cell = st / 11;
+        const int l = (int)(cell / ((size_t)c.w * c.h));
+        const size_t rem = cell % ((size_t)c.w * c.h);
+        const int y = (int)(rem / (size_t)c.w), x = (int)(rem % (size_t)c.w);
+        path[k] = (uint32_t)(((size_t)l * lat->height + (size_t)(c.y0 + y)) * lat->width +
+                             (size_t)(c.x0 + x));
+        if (k) st = (size_t)pred[st];
+      }
+      if (path_len) *path_len = n;
+    }
+  }
+  free(pred);
   free(g);
   if (expanded_out) *expanded_out = expanded;
   return result;
+}
+
+uint32_t lo_astar(const lo_lattice* lat, const lo_net* net, uint64_t* expanded_out) {
+  return astar_run(lat, net, expanded_out, NULL, 0, NULL);
+}
+
+uint32_t lo_astar_path(const lo_lattice* lat, const lo_net* net, uint64_t* expanded_out,
+                       uint32_t* path, uint32_t path_cap, uint32_t* path_len) {
+  return astar_run(lat, net, expanded_out, path, path_cap, path_len);
 }
 
 /* --------------------------- sweep schedule --------------------------- */

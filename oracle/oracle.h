@@ -70,8 +70,17 @@ typedef struct lo_net {
 uint32_t lo_dijkstra(const lo_lattice* lat, const lo_net* net, int full, uint32_t* dist,
                      uint32_t* path, uint32_t path_cap, uint32_t* path_len);
 
-/* A* restatement with the reference pop key.  Returns the goal cost. */
+/* A* restatement with the reference pop key.  Returns the goal cost;
+ * *expanded receives the count of expanded (popped, current, non-goal)
+ * states, the reference's CpuRouteTelemetry::expanded_states. */
 uint32_t lo_astar(const lo_lattice* lat, const lo_net* net, uint64_t* expanded);
+
+/* lo_astar that also returns the A* path forward (start first) as global cell
+ * ids, from the predecessor recorded by each accepted relaxation (the
+ * reference's reconstruction, cpu_astar.cc:518-545).  *path_len is 0 when
+ * disconnected and UINT32_MAX when path_cap is too small. */
+uint32_t lo_astar_path(const lo_lattice* lat, const lo_net* net, uint64_t* expanded,
+                       uint32_t* path, uint32_t path_cap, uint32_t* path_len);
 
 typedef struct lo_sweep_stats {
   uint32_t sweeps;         /* sweeps executed including the final quiet one */
