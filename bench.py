@@ -181,12 +181,23 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def frontier_bytes(results):
-    """Bytes the frontier expansions move: per expanded cell its queue entry
-    (4 B), its label word and the words of its 10 neighbours (11 x 8 B), plus
-    4 B per emitted path cell."""
-    exp = results["row_steps"].astype(np.float64).sum()
-    return exp * (4.0 + 11 * 8.0) + 4.0 * results["path_len"].astype(np.float64).sum()
+# Bytes one cell expansion of the frontier moves: its queue entry (4 B), its
+# label word and the words of its 10 neighbours (11 x 8 B).
+EXPANSION_BYTES = 4.0 + 11 * 8.0
+
+
+def frontier_bytes(lat, nets, results):
+    """Algorithmic bytes of one frontier batch, from the oracle, not from the
+    GPU's own work: the distinct cells the A* restatement of RouteWithCpuAStar
+    expands per net (the cell expansions an exact search needs) times the
+    bytes of an expansion, plus 4 B per emitted path cell.  Returns (those
+    bytes, the bytes of the GPU's own expansions, re-expansions included)."""
+    import oracle
+
+    _, _, cells = oracle.astar_batch(lat, nets, counts=True)
+    path = 4.0 * results["path_len"].astype(np.float64).sum()
+    gpu = results["row_steps"].astype(np.float64).sum() * EXPANSION_BYTES + path
+    return cells.astype(np.float64).sum() * EXPANSION_BYTES + path, gpu
 
 
 def certified(results):
@@ -200,11 +211,12 @@ def certified(results):
 def algorithmic_bytes(lat, nets, results):
     """Bytes the sweep schedule must move.
 
-    Per processed window row: the layer rows read and written (4 B per cell of
-    the window width) plus the obstacle and via bits (2 bits per cell per
-    layer); plus 4 B per emitted path cell.  The per-net row counters are the
-    CPU restatement's counts (the GPU tests check they are identical)."""
-    w = nets["win_w"].astype(np.float64)
+    Per processed frame row: the layer rows read and written (4 B per cell of
+    the row, which runs along the window's longer side) plus the obstacle and
+    via bits (2 bits per cell per layer); plus 4 B per emitted path cell.  The
+    per-net row counters are the CPU restatement's counts (the GPU tests check
+    they are identical)."""
+    w = np.maximum(nets["win_w"], nets["win_h"]).astype(np.float64)
     rows_moved = results["row_loads"].astype(np.float64) + results["row_stores"].astype(np.float64)
     label_bytes = (4.0 * w * rows_moved).sum()
     mask_bytes = (results["row_steps"].astype(np.float64) * lat.layers * w * 2.0 / 8.0).sum()
@@ -619,8 +631,9 @@ def main():
     if rank == 0:
         peak, peak_kind = load_peaks()
         avg_ms = total_ms / args.steps
-        fbytes = frontier_bytes(results)
+        fbytes, gpu_fbytes = frontier_bytes(lat, nets, results)
         achieved = fbytes / (avg_ms / 1000.0) / 1e9
+        one_pass_f = (nets["win_w"].astype(np.float64) * nets["win_h"] * lat.layers * 4.25).sum()
         traffic = load_traffic()
         sweep_ms = sweep["total_ms"] / args.steps
         sbytes, one_pass = algorithmic_bytes(lat, nets, sweep["results"])
@@ -646,6 +659,10 @@ def main():
                 "traffic": (traffic or {}).get("frontier_dram_bytes_per_step"),
                 "kernel": "lattice_frontier_kernel (all width classes of one execution)",
                 "bytes_alg_per_step": fbytes,
+                "bytes_alg_source": "oracle A* expanded cells x 92 B + 4 B per path cell",
+                "gpu_expansion_bytes_per_step": gpu_fbytes,
+                "one_pass_bytes_per_step": one_pass_f,
+                "one_pass_frac": one_pass_f / (avg_ms / 1000.0) / 1e9 / peak,
             },
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h), "ms_per_step": e2e_ms / args.steps,

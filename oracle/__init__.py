@@ -152,9 +152,13 @@ def dijkstra(lat, net_row, full=False, want_dist=False, path_cap=1 << 22, cell_c
     return cost, (path[:n].copy() if n != 0xFFFFFFFF else None), dist
 
 
-def dijkstra_batch(lat, nets, threads=None, path_cap_per_net=None, cell_cost=None):
+def dijkstra_batch(lat, nets, threads=None, path_cap_per_net=None, cell_cost=None,
+                   cell_cost_own=None, own=None):
     """Exact costs and canonical reverse paths of every net; ``cell_cost``
-    (optional, uint32 [layers][height][width]) adds a per-cell entry price."""
+    (optional, uint32 [layers][height][width]) adds a per-cell entry price.
+    Rip-up pricing: with ``own`` (one array of global cell ids per net, the
+    net's previous route, or None) those cells enter at ``cell_cost_own``
+    instead."""
     L = lib()
     ref = LatticeRef(lat, cell_cost)
     nets = np.ascontiguousarray(nets)
@@ -171,9 +175,23 @@ def dijkstra_batch(lat, nets, threads=None, path_cap_per_net=None, cell_cost=Non
     paths = np.empty(total, dtype=np.uint32)
     costs = np.empty(count, dtype=np.uint32)
     lens = np.empty(count, dtype=np.uint32)
-    L.lo_dijkstra_batch(ctypes.byref(ref.c), _net_ptr(nets), ctypes.c_uint32(count),
-                        ctypes.c_int(threads), _ptr(costs), _ptr(lens), _ptr(offsets, U64P),
-                        _ptr(paths), ctypes.c_uint64(total))
+    if own is None:
+        L.lo_dijkstra_batch(ctypes.byref(ref.c), _net_ptr(nets), ctypes.c_uint32(count),
+                            ctypes.c_int(threads), _ptr(costs), _ptr(lens), _ptr(offsets, U64P),
+                            _ptr(paths), ctypes.c_uint64(total))
+    else:
+        assert cell_cost is not None and cell_cost_own is not None and len(own) == count
+        cost_own = np.ascontiguousarray(cell_cost_own, dtype=np.uint32)
+        assert cost_own.size == lat.layers * lat.height * lat.width
+        sizes = np.array([0 if o is None else len(o) for o in own], dtype=np.uint64)
+        own_offsets = np.zeros(count + 1, dtype=np.uint64)
+        own_offsets[1:] = np.cumsum(sizes)
+        parts = [np.asarray(o, dtype=np.uint32) for o in own if o is not None and len(o)]
+        own_cells = np.ascontiguousarray(np.concatenate(parts) if parts else np.zeros(1, np.uint32))
+        L.lo_dijkstra_batch_own(ctypes.byref(ref.c), _net_ptr(nets), ctypes.c_uint32(count),
+                                ctypes.c_int(threads), _ptr(cost_own), _ptr(own_offsets, U64P),
+                                _ptr(own_cells), _ptr(costs), _ptr(lens), _ptr(offsets, U64P),
+                                _ptr(paths), ctypes.c_uint64(total))
     out = []
     for i in range(count):
         n = int(lens[i])
@@ -201,14 +219,23 @@ def astar_path(lat, net_row, path_cap=1 << 22):
     return cost, expanded.value, (path[:n].copy() if 0 < n != 0xFFFFFFFF else None)
 
 
-def astar_batch(lat, nets, threads=None):
+def astar_batch(lat, nets, threads=None, counts=False):
+    """A* restatement costs of every net; with ``counts`` also (expanded
+    states, distinct expanded cells) per net as uint64 arrays."""
     L = lib()
     ref = LatticeRef(lat)
     nets = np.ascontiguousarray(nets)
     costs = np.empty(len(nets), dtype=np.uint32)
-    L.lo_astar_batch(ctypes.byref(ref.c), _net_ptr(nets), ctypes.c_uint32(len(nets)),
-                     ctypes.c_int(threads or os.cpu_count() or 1), _ptr(costs))
-    return costs
+    if not counts:
+        L.lo_astar_batch(ctypes.byref(ref.c), _net_ptr(nets), ctypes.c_uint32(len(nets)),
+                         ctypes.c_int(threads or os.cpu_count() or 1), _ptr(costs))
+        return costs
+    states = np.empty(len(nets), dtype=np.uint64)
+    cells = np.empty(len(nets), dtype=np.uint64)
+    L.lo_astar_batch_ex(ctypes.byref(ref.c), _net_ptr(nets), ctypes.c_uint32(len(nets)),
+                        ctypes.c_int(threads or os.cpu_count() or 1), _ptr(costs),
+                        _ptr(states, U64P), _ptr(cells, U64P))
+    return costs, states, cells
 
 
 def sweep_batch(lat, nets, threads=None, max_sweeps=100000):

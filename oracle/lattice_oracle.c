@@ -30,6 +30,10 @@ typedef struct win_ctx {
   const lo_lattice* lat;
   const lo_net* net;
   int L, w, h, x0, y0, words;
+  /* Optional rip-up pricing: cells whose bit is set in `own` (window-local
+   * cell index) enter at cost_own[c] instead of cell_cost[c]. */
+  const uint8_t* own;
+  const uint32_t* cost_own;
 } win_ctx;
 
 static inline int lat_blocked(const lo_lattice* lat, int l, int gx, int gy) {
@@ -71,6 +75,8 @@ static void ctx_init(win_ctx* c, const lo_lattice* lat, const lo_net* net) {
   c->x0 = (int)net->win_x0;
   c->y0 = (int)net->win_y0;
   c->words = lat->width / 32;
+  c->own = NULL;
+  c->cost_own = NULL;
 }
 
 static inline size_t cell_index(const win_ctx* c, int l, int x, int y) {
@@ -133,7 +139,12 @@ static inline uint32_t move_cost(const lo_lattice* lat, int h) {
 static inline uint64_t entry_cost(const win_ctx* c, int l, int x, int y) {
   const lo_lattice* lat = c->lat;
   if (lat->cell_cost == NULL) return 0;
-  return lat->cell_cost[((size_t)l * lat->height + (c->y0 + y)) * lat->width + (c->x0 + x)];
+  const size_t g = ((size_t)l * lat->height + (c->y0 + y)) * lat->width + (c->x0 + x);
+  if (c->own != NULL) {
+    const size_t wi = cell_index(c, l, x, y);
+    if ((c->own[wi >> 3] >> (wi & 7)) & 1u) return c->cost_own[g];
+  }
+  return lat->cell_cost[g];
 }
 
 /* Reverse canonical path from exact labels.  Returns path length, or
@@ -179,10 +190,22 @@ static uint32_t canonical_walk(const win_ctx* c, const uint32_t* dist, int gl, i
 
 /* ------------------------------ Dijkstra ------------------------------ */
 
+static uint32_t dijkstra_run(const lo_lattice* lat, const lo_net* net, int full,
+                             uint32_t* dist_out, uint32_t* path, uint32_t path_cap,
+                             uint32_t* path_len, const uint8_t* own, const uint32_t* cost_own);
+
 uint32_t lo_dijkstra(const lo_lattice* lat, const lo_net* net, int full, uint32_t* dist_out,
                      uint32_t* path, uint32_t path_cap, uint32_t* path_len) {
+  return dijkstra_run(lat, net, full, dist_out, path, path_cap, path_len, NULL, NULL);
+}
+
+static uint32_t dijkstra_run(const lo_lattice* lat, const lo_net* net, int full,
+                             uint32_t* dist_out, uint32_t* path, uint32_t path_cap,
+                             uint32_t* path_len, const uint8_t* own, const uint32_t* cost_own) {
   win_ctx c;
   ctx_init(&c, lat, net);
+  c.own = own;
+  c.cost_own = cost_own;
   const size_t cells = (size_t)c.L * c.w * c.h;
   uint32_t* dist = dist_out ? dist_out : (uint32_t*)malloc(cells * sizeof(uint32_t));
   for (size_t i = 0; i < cells; ++i) dist[i] = LO_INF;
@@ -318,7 +341,8 @@ static uint64_t octile(const lo_lattice* lat, int dx, int dy, int dl) {
  * SearchRecord does (cpu_astar.cc:495-497), and the goal state's chain is
  * written forward (start first) as global cell ids. */
 static uint32_t astar_run(const lo_lattice* lat, const lo_net* net, uint64_t* expanded_out,
-                          uint32_t* path, uint32_t path_cap, uint32_t* path_len) {
+                          uint32_t* path, uint32_t path_cap, uint32_t* path_len,
+                          uint64_t* cells_out) {
   win_ctx c;
   ctx_init(&c, lat, net);
   const size_t cells = (size_t)c.L * c.w * c.h;
@@ -328,6 +352,9 @@ static uint32_t astar_run(const lo_lattice* lat, const lo_net* net, uint64_t* ex
   uint32_t* g = (uint32_t*)malloc(states * sizeof(uint32_t));
   for (size_t i = 0; i < states; ++i) g[i] = LO_INF;
   uint64_t* pred = path ? (uint64_t*)malloc(states * sizeof(uint64_t)) : NULL;
+  /* distinct cells with an expanded state (cells_out) */
+  uint8_t* seen = cells_out ? (uint8_t*)calloc((cells + 7) / 8, 1) : NULL;
+  uint64_t distinct = 0;
   size_t goal_state = (size_t)-1;
   if (path_len) *path_len = 0;
   const int sl = (int)net->start_layer, sx = (int)(net->start_x - net->win_x0),
@@ -353,6 +380,10 @@ static uint32_t astar_run(const lo_lattice* lat, const lo_net* net, uint64_t* ex
         break;
       }
       ++expanded;
+      if (seen && !((seen[ci >> 3] >> (ci & 7)) & 1u)) {
+        seen[ci >> 3] |= (uint8_t)(1u << (ci & 7));
+        ++distinct;
+      }
       for (int mv = 0; mv < 10; ++mv) {
         int nl = cur.l, nx = cur.x, ny = cur.y, legal, heading;
         if (mv < 8) {
@@ -409,18 +440,20 @@ static uint32_t astar_run(const lo_lattice* lat, const lo_net* net, uint64_t* ex
     }
   }
   free(pred);
+  free(seen);
   free(g);
   if (expanded_out) *expanded_out = expanded;
+  if (cells_out) *cells_out = distinct;
   return result;
 }
 
 uint32_t lo_astar(const lo_lattice* lat, const lo_net* net, uint64_t* expanded_out) {
-  return astar_run(lat, net, expanded_out, NULL, 0, NULL);
+  return astar_run(lat, net, expanded_out, NULL, 0, NULL, NULL);
 }
 
 uint32_t lo_astar_path(const lo_lattice* lat, const lo_net* net, uint64_t* expanded_out,
                        uint32_t* path, uint32_t path_cap, uint32_t* path_len) {
-  return astar_run(lat, net, expanded_out, path, path_cap, path_len);
+  return astar_run(lat, net, expanded_out, path, path_cap, path_len, NULL);
 }
 
 /* --------------------------- sweep schedule --------------------------- */
@@ -636,6 +669,11 @@ typedef struct batch_job {
   const lo_lattice* lat;
   const lo_net* nets;
   uint32_t count;
+  /* rip-up pricing (kind 0 only): net i's own cells are
+   * own_cells[own_offsets[i] .. own_offsets[i + 1]) (global ids) */
+  const uint32_t* cost_own;
+  const uint64_t* own_offsets;
+  const uint32_t* own_cells;
   int kind; /* 0 dijkstra, 1 astar, 2 sweep */
   uint32_t max_sweeps;
   uint32_t* costs;
@@ -644,6 +682,8 @@ typedef struct batch_job {
   uint32_t* paths;
   uint64_t path_capacity;
   lo_sweep_stats* stats;
+  uint64_t* expanded_states; /* kind 1, optional */
+  uint64_t* expanded_cells;  /* kind 1, optional */
   uint32_t next;
   pthread_mutex_t lock;
 } batch_job;
@@ -665,10 +705,33 @@ static void* batch_worker(void* arg) {
         const uint64_t end = (i + 1 < job->count) ? job->path_offsets[i + 1] : job->path_capacity;
         cap = (uint32_t)(end - job->path_offsets[i]);
       }
-      job->costs[i] = lo_dijkstra(job->lat, net, 0, NULL, path, cap, path ? &len : NULL);
+      uint8_t* own = NULL;
+      if (job->own_offsets != NULL && job->own_offsets[i + 1] > job->own_offsets[i]) {
+        const lo_lattice* lat = job->lat;
+        const size_t wcells = (size_t)lat->layers * net->win_w * net->win_h;
+        own = (uint8_t*)calloc((wcells + 7) / 8, 1);
+        for (uint64_t k = job->own_offsets[i]; k < job->own_offsets[i + 1]; ++k) {
+          const size_t gcell = job->own_cells[k];
+          const size_t plane = (size_t)lat->height * lat->width;
+          const int l = (int)(gcell / plane);
+          const int gy = (int)((gcell % plane) / (size_t)lat->width);
+          const int gx = (int)(gcell % (size_t)lat->width);
+          const int x = gx - (int)net->win_x0, y = gy - (int)net->win_y0;
+          if (x < 0 || y < 0 || x >= (int)net->win_w || y >= (int)net->win_h) continue;
+          const size_t wi = ((size_t)l * net->win_h + (size_t)y) * net->win_w + (size_t)x;
+          own[wi >> 3] |= (uint8_t)(1u << (wi & 7));
+        }
+      }
+      job->costs[i] = dijkstra_run(job->lat, net, 0, NULL, path, cap, path ? &len : NULL, own,
+                                   job->cost_own);
+      free(own);
       if (job->path_lens) job->path_lens[i] = len;
     } else if (job->kind == 1) {
-      job->costs[i] = lo_astar(job->lat, net, NULL);
+      uint64_t states = 0, cells = 0;
+      job->costs[i] = astar_run(job->lat, net, &states, NULL, 0, NULL,
+                                job->expanded_cells ? &cells : NULL);
+      if (job->expanded_states) job->expanded_states[i] = states;
+      if (job->expanded_cells) job->expanded_cells[i] = cells;
     } else {
       const size_t cells = (size_t)job->lat->layers * net->win_w * net->win_h;
       uint32_t* dist = (uint32_t*)malloc(cells * sizeof(uint32_t));
@@ -707,14 +770,42 @@ void lo_dijkstra_batch(const lo_lattice* lat, const lo_net* nets, uint32_t count
   run_batch(&job, threads);
 }
 
+void lo_dijkstra_batch_own(const lo_lattice* lat, const lo_net* nets, uint32_t count,
+                           int threads, const uint32_t* cell_cost_own,
+                           const uint64_t* own_offsets, const uint32_t* own_cells,
+                           uint32_t* costs, uint32_t* path_lens, uint64_t* path_offsets,
+                           uint32_t* paths, uint64_t path_capacity) {
+  batch_job job = {0};
+  job.lat = lat;
+  job.nets = nets;
+  job.count = count;
+  job.kind = 0;
+  job.cost_own = cell_cost_own;
+  job.own_offsets = own_offsets;
+  job.own_cells = own_cells;
+  job.costs = costs;
+  job.path_lens = path_lens;
+  job.path_offsets = path_offsets;
+  job.paths = paths;
+  job.path_capacity = path_capacity;
+  run_batch(&job, threads);
+}
+
 void lo_astar_batch(const lo_lattice* lat, const lo_net* nets, uint32_t count, int threads,
                     uint32_t* costs) {
+  lo_astar_batch_ex(lat, nets, count, threads, costs, NULL, NULL);
+}
+
+void lo_astar_batch_ex(const lo_lattice* lat, const lo_net* nets, uint32_t count, int threads,
+                       uint32_t* costs, uint64_t* expanded_states, uint64_t* expanded_cells) {
   batch_job job = {0};
   job.lat = lat;
   job.nets = nets;
   job.count = count;
   job.kind = 1;
   job.costs = costs;
+  job.expanded_states = expanded_states;
+  job.expanded_cells = expanded_cells;
   run_batch(&job, threads);
 }
 

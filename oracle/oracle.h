@@ -105,8 +105,25 @@ uint32_t lo_sweep_schedule_oriented(const lo_lattice* lat, const lo_net* net, ui
 void lo_dijkstra_batch(const lo_lattice* lat, const lo_net* nets, uint32_t count, int threads,
                        uint32_t* costs, uint32_t* path_lens, uint64_t* path_offsets,
                        uint32_t* paths, uint64_t path_capacity);
+
+/* lo_dijkstra_batch with rip-up pricing (lat->cell_cost required): cells of
+ * net i's previous route, own_cells[own_offsets[i] .. own_offsets[i + 1])
+ * (global cell ids; own_offsets has count + 1 entries), enter at
+ * cell_cost_own[c] instead of cell_cost[c]. */
+void lo_dijkstra_batch_own(const lo_lattice* lat, const lo_net* nets, uint32_t count,
+                           int threads, const uint32_t* cell_cost_own,
+                           const uint64_t* own_offsets, const uint32_t* own_cells,
+                           uint32_t* costs, uint32_t* path_lens, uint64_t* path_offsets,
+                           uint32_t* paths, uint64_t path_capacity);
 void lo_astar_batch(const lo_lattice* lat, const lo_net* nets, uint32_t count, int threads,
                     uint32_t* costs);
+
+/* lo_astar_batch that also reports, per net, the expanded states (the
+ * reference's expanded_states) and the distinct cells with an expanded state
+ * (the cell expansions an exact cell-level A* needs: the frontier's unit of
+ * algorithmic work).  Either output may be NULL. */
+void lo_astar_batch_ex(const lo_lattice* lat, const lo_net* nets, uint32_t count, int threads,
+                       uint32_t* costs, uint64_t* expanded_states, uint64_t* expanded_cells);
 void lo_sweep_batch(const lo_lattice* lat, const lo_net* nets, uint32_t count, int threads,
                     uint32_t max_sweeps, uint32_t* costs, lo_sweep_stats* stats);
 

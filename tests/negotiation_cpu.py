@@ -48,21 +48,19 @@ class CpuRank:
                        if c == oracle.lo_inf() or (self.usage[p.astype(np.int64)] > self.pol.capacity).any()]
             else:
                 idx = range(len(nets))
+            idx = list(idx)
             self.costs = self.costs.copy()
             self.paths = list(self.paths)
-            for i in idx:
-                mine = self.cost.copy()
-                if self.costs[i] != oracle.lo_inf():
-                    own = self.paths[i].astype(np.int64)
-                    mine[own] = self.cost_own[own]
-                c, p = oracle.dijkstra_batch(self.lat, nets[i:i + 1], cell_cost=mine)
-                self.costs[i] = c[0]
-                self.paths[i] = p[0]
-        usage = np.zeros(self.cells, np.uint64)
-        for c, p in zip(self.costs, self.paths):
-            if c != oracle.lo_inf():
-                np.add.at(usage, p.astype(np.int64), 1)
-        return usage
+            if idx:
+                own = [self.paths[i] if self.costs[i] != oracle.lo_inf() else None for i in idx]
+                c, p = oracle.dijkstra_batch(self.lat, nets[idx], cell_cost=self.cost,
+                                             cell_cost_own=self.cost_own, own=own)
+                for k, i in enumerate(idx):
+                    self.costs[i] = c[k]
+                    self.paths[i] = p[k]
+        reached = [p for c, p in zip(self.costs, self.paths) if c != oracle.lo_inf()]
+        cells = np.concatenate(reached).astype(np.int64) if reached else np.zeros(0, np.int64)
+        return np.bincount(cells, minlength=self.cells).astype(np.uint64)
 
     def price(self, r, usage):
         pol = self.pol

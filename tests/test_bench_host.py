@@ -43,11 +43,37 @@ def test_clock_summary_skips_rows_before_timing(tmp_path, bench):
     assert out["reasons"] == ["sw_power_cap"]
 
 
-def test_frontier_bytes_follow_the_expansion_count(bench):
-    res = np.zeros(3, dtype=[("row_steps", "<u4"), ("path_len", "<u4")])
-    res["row_steps"] = [10, 0, 5]
-    res["path_len"] = [4, 0, 2]
-    assert bench.frontier_bytes(res) == 15 * (4 + 11 * 8) + 4 * 6
+def test_frontier_bytes_come_from_the_oracle_expansions(bench):
+    """The frontier's algorithmic bytes count the oracle A*'s distinct expanded
+    cells, not the GPU's own expansions (which are reported beside them)."""
+    import oracle
+    from apgar_b200 import synth
+
+    lat, nets = synth.config_small(1)
+    nets = nets[:6].copy()
+    _, _, cells = oracle.astar_batch(lat, nets, counts=True)
+    res = np.zeros(len(nets), dtype=[("row_steps", "<u4"), ("path_len", "<u4")])
+    res["row_steps"] = 1000
+    res["path_len"] = 3
+    alg, gpu = bench.frontier_bytes(lat, nets, res)
+    assert cells.sum() > 0
+    assert alg == cells.sum() * (4 + 11 * 8) + 4 * 3 * len(nets)
+    assert gpu == 1000 * len(nets) * (4 + 11 * 8) + 4 * 3 * len(nets)
+
+
+def test_oracle_expanded_cells_are_distinct_cells_of_expanded_states():
+    """Expanded states count every (cell, heading) the A* pops and expands;
+    distinct cells are at most that and at least one per expanded cell."""
+    import oracle
+    from apgar_b200 import synth
+
+    lat, nets = synth.config_small(1)
+    costs, states, cells = oracle.astar_batch(lat, nets[:8].copy(), counts=True)
+    assert np.array_equal(costs, oracle.astar_batch(lat, nets[:8].copy()))
+    assert (cells <= states).all() and (cells[states > 0] > 0).all()
+    for i in range(3):
+        _, expanded, _ = oracle.astar_path(lat, nets[i:i + 1].copy())
+        assert expanded == states[i]
 
 
 def test_reference_arm_prints_one_json_line():
