@@ -166,8 +166,13 @@ class B200PendingRoute final : public PendingRouteExecution {
   std::uint64_t states_;
 };
 
+// Readback form by generator value: the stock frontier and the added
+// persistent-workspace generator return the full workspace, the others
+// compact paths.  Values, not enumerator names, so that the shim builds
+// against the stock header as well as the patched one.
 bool full_workspace(PlanarGenerator generator) {
-  return generator == PlanarGenerator::kBucketedFrontier;
+  return generator == PlanarGenerator::kBucketedFrontier ||
+         static_cast<std::uint8_t>(generator) == APGAR_B200_GENERATOR_B200_PERSISTENT_WORKSPACE;
 }
 
 // ---- the backend ----
@@ -303,6 +308,10 @@ class B200PlanarRouteBackend final : public IPlanarRouteBackend {
       rc = apgar_b200_readback_batch_workspace(p->handle_, labels.data(), preds.data(), owners.data(),
                                                pred_owners.data());
       if (rc != APGAR_B200_OK) return last_error(rc);
+      // the workspace arrays just read are part of this readback
+      t.device_to_host_readback_bytes +=
+          query_count * per_query *
+          (sizeof(std::uint64_t) + sizeof(std::uint32_t) + 2 * sizeof(std::uint64_t));
       // place each query's rows at the workspace slice its request named
       std::uint64_t extent = 0;
       for (const auto& [offset, count] : p->offsets_) extent = std::max(extent, offset + count);

@@ -130,6 +130,7 @@ struct PendingBatch {
   ViewObject* view = nullptr;
   bool leased = false;
   bool workspace_mode = false;
+  uint8_t generator = 0;
   uint32_t query_count = 0;
   uint64_t states = 0;
   uint64_t batch_bytes = 0;
@@ -263,19 +264,27 @@ int validate_view(const apgar_b200_compiled_header_v1& h, const apgar_b200_layer
 // Candidate-batch admission (gpu/cuda/planar_router.cu:1731-1909): ordering,
 // ownership, associations, workspace bounds, policy encoding and the
 // cost-sentinel bound.
+// Generators whose readback is the full workspace (labels, predecessors and
+// owners of every state) rather than compact paths.
+bool full_workspace_generator(uint8_t generator) {
+  return generator == APGAR_B200_GENERATOR_BUCKETED_FRONTIER ||
+         generator == APGAR_B200_GENERATOR_B200_PERSISTENT_WORKSPACE;
+}
+
 int validate_batch(const ViewObject& v, const apgar_b200_batch_request& req,
                    const apgar_b200_batch_query_v1* queries, uint32_t count,
                    const apgar_b200_policy_edge_v1* edges, uint64_t edge_count) {
   const uint64_t n = v.legal.size();
   const uint64_t S = 9ull * n;
   if (req.schema_version != 1u || req.batch_id == 0 || count == 0 ||
-      edge_count > kMaximumPolicyEntries || req.maximum_rounds == 0 || req.generator > 2) {
+      edge_count > kMaximumPolicyEntries || req.maximum_rounds == 0 ||
+      req.generator > APGAR_B200_GENERATOR_B200_PERSISTENT_WORKSPACE) {
     return invariant("candidate batch has invalid schema, identity, policy size, generator or rounds");
   }
   if (req.maximum_workspace_states_per_query < S) {
     return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "batch exceeds the per-query workspace-state capacity");
   }
-  const bool frontier = req.generator == APGAR_B200_GENERATOR_BUCKETED_FRONTIER;
+  const bool frontier = full_workspace_generator(req.generator);
   if (frontier && req.maximum_frontier_states_per_query < S) {
     return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "batch exceeds the per-query frontier-state capacity");
   }
@@ -327,7 +336,7 @@ int run_batch(ViewObject* v, const apgar_b200_batch_request& req,
               const volatile uint8_t* cancel, PendingBatch* pending) {
   const uint64_t n = v->legal.size();
   const uint64_t S = 9ull * n;
-  const bool workspace_mode = req.generator == APGAR_B200_GENERATOR_BUCKETED_FRONTIER;
+  const bool workspace_mode = full_workspace_generator(req.generator);
   Workspace& w = v->ws;
   const uint64_t Q = count;
   // deterministic workspace bytes for this batch (checked against the budget
@@ -341,7 +350,9 @@ int run_batch(ViewObject* v, const apgar_b200_batch_request& req,
     return set_error(APGAR_B200_RESOURCE_EXHAUSTED, "batch exceeds the device-memory budget");
   }
   APGAR_B200_CUDA("cudaMalloc(queries)", w.queries.ensure(Q));
-  APGAR_B200_CUDA("cudaMalloc(policy)", w.policy.ensure(std::max<uint64_t>(edge_count, 1)));
+  // no policy buffer without policy edges (the kernel reads none), so a
+  // fresh workspace holds exactly the bytes `need` accounts for
+  APGAR_B200_CUDA("cudaMalloc(policy)", w.policy.ensure(edge_count));
   APGAR_B200_CUDA("cudaMalloc(results)", w.results.ensure(Q));
   APGAR_B200_CUDA("cudaMalloc(compact)", w.compact.ensure(Q));
   APGAR_B200_CUDA("cudaMalloc(labels)", w.labels.ensure(Q * S));
@@ -418,6 +429,7 @@ int run_batch(ViewObject* v, const apgar_b200_batch_request& req,
   APGAR_B200_CUDA("cudaEventElapsedTime", cudaEventElapsedTime(&ms, t0, t1));
   pending->view = v;
   pending->workspace_mode = workspace_mode;
+  pending->generator = req.generator;
   pending->query_count = count;
   pending->states = S;
   pending->batch_bytes = static_cast<uint64_t>(need);
@@ -438,7 +450,10 @@ void fill_telemetry(const PendingBatch& p, uint64_t readback_bytes, uint32_t max
   t->kernel_launch_count = p.launches;
   t->blocking_status_readback_count = 0;  // no host round trip during the search
   t->dispatched_rounds = max_rounds;
-  t->finalization_launch_count = 0;
+  // The persistent generators' descriptor counts the batch's last launch
+  // (path packing, or the single search launch of the full workspace, which
+  // writes every final result header) as its finalization launch.
+  t->finalization_launch_count = p.generator >= APGAR_B200_GENERATOR_B200_PERSISTENT ? 1u : 0u;
   t->kernel_milliseconds = p.kernel_ms;
 }
 
@@ -605,7 +620,7 @@ extern "C" int apgar_b200_execute_route(void* view, uint8_t generator, uint32_t 
   auto* v = static_cast<ViewObject*>(view);
   const uint64_t n = v->legal.size();
   if (start_node >= n || goal_node >= n || maximum_rounds == 0 || start_node == goal_node ||
-      generator > 2) {
+      generator > APGAR_B200_GENERATOR_B200_PERSISTENT_WORKSPACE) {
     return invariant("route received invalid endpoint, generator or budget bounds");
   }
   if (int rc = check_device(v->device); rc != APGAR_B200_OK) return rc;

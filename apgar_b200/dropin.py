@@ -20,6 +20,7 @@ from . import BackendError, _check, lib  # noqa: F401
 GENERATOR_FRONTIER = 0
 GENERATOR_SWEEP = 1
 GENERATOR_PERSISTENT = 2
+GENERATOR_PERSISTENT_WORKSPACE = 3
 
 HEADER_DTYPE = np.dtype([
     ("schema_version", "<u4"), ("compiler_version", "<u4"),
@@ -116,7 +117,7 @@ def make_queries(view_nodes: int, entries, batch_id: int = 7, generator: int = G
         count = 0 if pol is None else len(pol)
         q[i] = (1, i, batch_id, i + 1, i + 1, e.get("policy_identity", 0), e.get("routing_profile_fingerprint", 0),
                 e["start_node"], e["goal_node"], offset, count, i * S, S,
-                S if generator == GENERATOR_FRONTIER else 0,
+                S if generator in (GENERATOR_FRONTIER, GENERATOR_PERSISTENT_WORKSPACE) else 0,
                 e.get("orthogonal_step_surcharge", 0), e.get("diagonal_step_surcharge", 0),
                 e.get("bend_surcharge", 0), maximum_rounds, generator, (0, 0, 0))
         if count:

@@ -15,7 +15,7 @@ def _enum(prefix):
     with open(HEADER) as f:
         text = f.read()
     return {name[len(prefix):].lower(): int(value)
-            for name, value in re.findall(r"\b(" + prefix + r"[A-Z_]+)\s*=\s*(\d+)", text)}
+            for name, value in re.findall(r"\b(" + prefix + r"[A-Z0-9_]+)\s*=\s*(\d+)", text)}
 
 
 def test_path_codes():
@@ -40,3 +40,11 @@ def test_completion_and_corridor_codes():
     cor = _enum("APGAR_B200_CORRIDOR_")
     assert (cor["none"], cor["certified"], cor["fallback_exit"], cor["fallback_unreached"]) == (
         corridor.NONE, corridor.CERTIFIED, corridor.FALLBACK_EXIT, corridor.FALLBACK_UNREACHED)
+
+
+def test_generator_codes():
+    gen = _enum("APGAR_B200_GENERATOR_")
+    assert gen == {"bucketed_frontier": dropin.GENERATOR_FRONTIER,
+                   "heading_sweep": dropin.GENERATOR_SWEEP,
+                   "b200_persistent": dropin.GENERATOR_PERSISTENT,
+                   "b200_persistent_workspace": dropin.GENERATOR_PERSISTENT_WORKSPACE}
