@@ -85,26 +85,33 @@ APGAR_B200_API int apgar_b200_query_metadata(apgar_b200_metadata* out);
 
 /* =================== A. drop-in seam (reference V1 records) =================== */
 
-/* Generator values of PlanarGenerator (planar_router.h:42-45) plus the value
- * this backend adds for its own persistent engine.
+/* Generator values of PlanarGenerator (planar_router.h:42-45) plus the two
+ * values this backend adds for its own persistent engine (the reference's
+ * extension mechanism: a new enumerator with its own descriptor,
+ * schemas/device_candidate_batch/v1.md:21-25).
  *
- * APGAR_B200_GENERATOR_B200_PERSISTENT searches a whole batch in one launch
- * with no host round trips and returns compact paths.  Its generator
- * descriptor (the reference's DescribePlanarGenerator, planar_router.h:56-100)
- * is: workspace kSweep (compact-path readback), chunk_rounds = the request's
- * maximum_rounds, fixed_launches = 3 (search, offset scan, pack),
- * kernels_per_round = 0, launches_once_per_chunk = false, and host_chunked =
- * false, a flag the descriptor gains with this value.  For host_chunked ==
- * false the telemetry check expects 0 blocking status readbacks,
- * fixed_launches + finalization launches, and device bytes
- * Q*(120 + 120 + 32) + E*16 + Q*S*8 + Q*N*12 + Q*S*4 + 16 for Q queries,
- * E policy edges, N nodes and S = 9N states.  The two stock generators keep
- * their descriptors; this engine serves them with the same single launch and
- * reports its own counts. */
+ * The persistent generators search a whole batch on the device with no
+ * host-chunked rounds.  B200_PERSISTENT returns compact paths (3 launches:
+ * search, path-offset scan, packing); B200_PERSISTENT_WORKSPACE returns the
+ * full workspace (1 launch).  Their descriptor (the reference's
+ * DescribePlanarGenerator, planar_router.h:56-100): workspace kSweep or
+ * kFrontier by readback form, chunk_rounds = 1, 8 examined work per round and
+ * per node, 8 turn relaxations per examined work, no per-round kernels,
+ * fixed_launches = 2 or 0, and host_chunked = false, a flag the descriptor
+ * gains with these values.  The batch reports 0 blocking status readbacks,
+ * its last launch as the finalization launch, dispatched_rounds = the most
+ * rounds any query ran, and device bytes
+ * Q*(120 + 120 + 32) + E*16 + Q*S*8 + Q*N*12 + Q*S*4 (+ Q*S*16 for the full
+ * workspace) + 16, for Q queries, E policy edges, N nodes and S = 9N states.
+ * apgar_b200/adapter/reference_generator.patch is that change to the
+ * reference's host code.  The two stock generators keep their descriptors;
+ * this engine serves them with the same launches and reports its own
+ * counts, which their host-chunked descriptors do not describe. */
 enum {
-  APGAR_B200_GENERATOR_BUCKETED_FRONTIER = 0, /* PlanarGenerator::kBucketedFrontier */
-  APGAR_B200_GENERATOR_HEADING_SWEEP = 1,     /* PlanarGenerator::kHeadingAwareSweep */
-  APGAR_B200_GENERATOR_B200_PERSISTENT = 2    /* added: one fused launch per batch */
+  APGAR_B200_GENERATOR_BUCKETED_FRONTIER = 0,          /* PlanarGenerator::kBucketedFrontier */
+  APGAR_B200_GENERATOR_HEADING_SWEEP = 1,              /* PlanarGenerator::kHeadingAwareSweep */
+  APGAR_B200_GENERATOR_B200_PERSISTENT = 2,            /* added: compact paths */
+  APGAR_B200_GENERATOR_B200_PERSISTENT_WORKSPACE = 3   /* added: full workspace */
 };
 
 /* DeviceCompiledHeaderV1 (planar_router.h:170-188), 112 bytes. */
@@ -534,6 +541,11 @@ typedef struct apgar_b200_lattice_options {
                               1..31; larger windows take 16 warps.  0 = the default
                               0x13110F0C (2^12, 2^15, 2^17, 2^19).  Results do not
                               depend on it. */
+  uint32_t wide_bucket_width; /* FRONTIER: key width of the 16-warp class's levels (its
+                                 nets are the batch's longest searches, so its schedule
+                                 is tuned apart); 0 = bucket_width; raised like it */
+  uint32_t wide_chain;        /* FRONTIER: chain of the 16-warp class, meaning as chain;
+                                 0 = chain.  Results depend on neither. */
 } apgar_b200_lattice_options;
 
 /* Per-cell entry prices for a FRONTIER plan (no reference counterpart at this
