@@ -70,6 +70,8 @@ class LatticeOptions(ctypes.Structure):
         ("bucket_width", ctypes.c_uint32),
         ("chain", ctypes.c_uint32),
         ("class_bounds", ctypes.c_uint32),
+        ("wide_bucket_width", ctypes.c_uint32),
+        ("wide_chain", ctypes.c_uint32),
     ]
 
 
@@ -85,10 +87,18 @@ def class_bounds(*log2_limits: int) -> int:
 
 
 def _options(generator: str, max_iterations: int, bucket_width: int, chain: int = 0,
-             bounds: int = 0) -> LatticeOptions:
+             bounds: int = 0, wide_bucket_width: int = 0, wide_chain: int = 0) -> LatticeOptions:
     if generator not in GENERATORS:
         raise BackendError(1, f"unknown lattice generator {generator!r}")
-    return LatticeOptions(GENERATORS[generator], max_iterations, bucket_width, chain, bounds)
+    return LatticeOptions(GENERATORS[generator], max_iterations, bucket_width, chain, bounds,
+                          wide_bucket_width, wide_chain)
+
+
+def _schedule_fields(schedule):
+    """(bucket_width, chain, class_bounds, wide_bucket_width, wide_chain) of a
+    tuned schedule (``apgar_b200.autotune.Schedule``)."""
+    return (schedule.bucket_width, schedule.chain, schedule.class_bounds,
+            getattr(schedule, "wide_bucket_width", 0), getattr(schedule, "wide_chain", 0))
 
 
 class PlanInfo(ctypes.Structure):
@@ -198,15 +208,18 @@ class DeviceLattice:
     def route(self, nets: np.ndarray, max_sweeps: int = 4096, cancel: np.ndarray | None = None,
               want_paths: bool = True, path_capacity: int | None = None, out=None,
               generator: str = "sweep", max_rounds: int = 1 << 30, bucket_width: int = 0,
-              chain: int = 0, class_bounds: int = 0, schedule=None):
+              chain: int = 0, class_bounds: int = 0, schedule=None, wide_bucket_width: int = 0,
+              wide_chain: int = 0):
         """Searches every net; returns (results record array, packed paths).
 
         ``generator`` is "sweep" (budget ``max_sweeps``) or "frontier"
         (budget ``max_rounds``, key level width ``bucket_width``, 0 = twice
         the largest move; ``chain``, 0 = the default per width class, n = up
         to n - 1 chained expansions per queued cell; ``class_bounds``, the
-        packed width-class limits of ``class_bounds()``, 0 = the default; or a
-        tuned ``schedule`` holding all three).  ``out`` may supply
+        packed width-class limits of ``class_bounds()``, 0 = the default;
+        ``wide_bucket_width`` and ``wide_chain``, the 16-warp class's own level
+        width and chain, 0 = as the others; or a tuned ``schedule`` holding
+        all five).  ``out`` may supply
         preallocated (results, paths) host arrays (pinned memory makes the
         transfers faster)."""
         nets = np.ascontiguousarray(nets)
@@ -234,9 +247,10 @@ class DeviceLattice:
                 ctypes.c_uint64(paths.size if want_paths else 0), ctypes.byref(total)))
         else:
             if schedule is not None:
-                bucket_width, chain, class_bounds = (schedule.bucket_width, schedule.chain,
-                                                     schedule.class_bounds)
-            opts = _options(generator, max_rounds, bucket_width, chain, class_bounds)
+                bucket_width, chain, class_bounds, wide_bucket_width, wide_chain = \
+                    _schedule_fields(schedule)
+            opts = _options(generator, max_rounds, bucket_width, chain, class_bounds,
+                            wide_bucket_width, wide_chain)
             _check(lib().apgar_b200_lattice_route_ex(
                 self.handle, _vp(nets), ctypes.c_uint32(count), ctypes.byref(opts),
                 _vp(cancel), _vp(results), _vp(paths) if want_paths else None,
@@ -297,8 +311,11 @@ class DeviceLattice:
         ``apgar_b200.autotune.tune``) whose bucket width, chain and class bounds
         replace the three arguments."""
         if schedule is not None:
-            bucket_width, chain, class_bounds = schedule.bucket_width, schedule.chain, schedule.class_bounds
-        return Plan(self, nets, max_sweeps, generator, max_rounds, bucket_width, chain, class_bounds)
+            bucket_width, chain, class_bounds, wide_bucket_width, wide_chain = _schedule_fields(schedule)
+        else:
+            wide_bucket_width = wide_chain = 0
+        return Plan(self, nets, max_sweeps, generator, max_rounds, bucket_width, chain, class_bounds,
+                    wide_bucket_width, wide_chain)
 
 
 class Plan:
@@ -306,7 +323,8 @@ class Plan:
 
     def __init__(self, lattice: DeviceLattice, nets: np.ndarray, max_sweeps: int,
                  generator: str = "sweep", max_rounds: int = 1 << 30, bucket_width: int = 0,
-                 chain: int = 0, class_bounds: int = 0):
+                 chain: int = 0, class_bounds: int = 0, wide_bucket_width: int = 0,
+                 wide_chain: int = 0):
         self.lattice = lattice
         self.nets = np.ascontiguousarray(nets)
         self.generator = generator
@@ -316,7 +334,8 @@ class Plan:
                                                  ctypes.c_uint32(len(self.nets)),
                                                  ctypes.c_uint32(max_sweeps), ctypes.byref(handle)))
         else:
-            opts = _options(generator, max_rounds, bucket_width, chain, class_bounds)
+            opts = _options(generator, max_rounds, bucket_width, chain, class_bounds,
+                            wide_bucket_width, wide_chain)
             _check(lib().apgar_b200_lattice_plan_ex(lattice.handle, _vp(self.nets),
                                                     ctypes.c_uint32(len(self.nets)),
                                                     ctypes.byref(opts), ctypes.byref(handle)))

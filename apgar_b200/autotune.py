@@ -33,10 +33,15 @@ class Schedule:
     bucket_width: int = 0  # 0 = twice the largest move cost
     chain: int = 0         # 0 = the per-class default (no chaining)
     class_bounds: int = 0  # 0 = the library default limits
+    # the 16-warp class (the batch's longest searches, its critical path):
+    # its own level width and chain, 0 = as the other classes
+    wide_bucket_width: int = 0
+    wide_chain: int = 0
 
     def describe(self) -> dict:
         bounds = [(self.class_bounds >> (8 * k)) & 0xFF for k in range(4)] if self.class_bounds else None
-        return {"bucket_width": self.bucket_width, "chain": self.chain, "class_log2_limits": bounds}
+        return {"bucket_width": self.bucket_width, "chain": self.chain, "class_log2_limits": bounds,
+                "wide_bucket_width": self.wide_bucket_width, "wide_chain": self.wide_chain}
 
 
 DEFAULT = Schedule()
@@ -157,6 +162,17 @@ def tune(lattice, nets, max_nets: int | None = None, warmup: int = 1, reps: int 
     ms = measure(s)
     if ms < best_ms * (1.0 - MIN_GAIN):
         best, best_ms = s, ms
+    # the widest class alone: wider levels mean fewer level openings on its
+    # nets' round chains (the batch's critical path) at the price of extra
+    # expansions, which the other classes' throughput cannot afford
+    # (a chain for the widest class alone measured 2-4x slower on the medium
+    # batch, depths 4-16, so it is not searched; the option stays available)
+    base = best
+    for factor in (2, 4):
+        s = dataclasses.replace(base, wide_bucket_width=min_width * factor)
+        ms = measure(s)
+        if ms < best_ms * (1.0 - MIN_GAIN):
+            best, best_ms = s, ms
     out = (best, table)
     _CACHE[key] = out
     return out

@@ -122,7 +122,9 @@ struct PlanObject {
   uint32_t max_sweeps = 0;  // sweeps (SWEEP) or rounds (FRONTIER)
   uint32_t generator = APGAR_B200_LATTICE_SWEEP;
   uint32_t bucket_width = 0;
+  uint32_t wide_bucket_width = 0;  // FRONTIER: level width of the 16-warp class
   uint32_t chain = 0;    // FRONTIER: apgar_b200_lattice_options::chain
+  uint32_t wide_chain = 0;  // FRONTIER: apgar_b200_lattice_options::wide_chain
   uint32_t class_bounds = kDefaultClassBounds;  // FRONTIER: log2 class limits, byte per class
   bool per_net = false;  // FRONTIER: one slab per net (else persistent slots)
   const uint32_t* cell_cost = nullptr;  // caller-owned device prices (frontier only)
@@ -287,7 +289,8 @@ std::vector<uint32_t> sweep_planes(const uint32_t* in, int planes, int height, i
 int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint32_t count,
                uint32_t max_sweeps, PlanObject* plan,
                uint32_t generator = APGAR_B200_LATTICE_SWEEP, uint32_t bucket_width = 0,
-               uint32_t chain = 0, uint32_t class_bounds = 0) {
+               uint32_t chain = 0, uint32_t class_bounds = 0, uint32_t wide_bucket_width = 0,
+               uint32_t wide_chain = 0) {
   const LatticeDeviceView& v = lat->view;
   const bool frontier = generator == APGAR_B200_LATTICE_FRONTIER;
   plan->lattice = lat;
@@ -299,7 +302,12 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
   // falls in the next level (the frontier kernel relies on it: a cell that
   // left the far list never returns to it, so its far bit needs no clearing).
   plan->bucket_width = std::max(bucket_width, 2u * std::max(v.orth, std::max(v.diag, v.via)));
+  plan->wide_bucket_width =
+      wide_bucket_width != 0
+          ? std::max(wide_bucket_width, 2u * std::max(v.orth, std::max(v.diag, v.via)))
+          : plan->bucket_width;
   plan->chain = chain;
+  plan->wide_chain = wide_chain != 0 ? wide_chain : chain;
   plan->class_bounds = class_bounds != 0 ? class_bounds : kDefaultClassBounds;
   APGAR_B200_CUDA("cudaDeviceGetAttribute",
                   cudaDeviceGetAttribute(&plan->sm_count, cudaDevAttrMultiProcessorCount,
@@ -523,9 +531,6 @@ int execute_plan(PlanObject* plan, cudaStream_t stream) {
   fbase.prev_paths = plan->prev_paths;
   fbase.cell_cost_own = plan->cell_cost_own;
   if (plan->corridor != nullptr) {
-    if (plan->cell_cost != nullptr) {
-      return set_error(APGAR_B200_UNSUPPORTED, "corridor mode is not combined with per-cell prices");
-    }
     fbase.corridor = plan->corridor;
     fbase.corridor_status = plan->corridor_status.get();
   }
@@ -564,7 +569,12 @@ int execute_plan(PlanObject* plan, cudaStream_t stream) {
         fl.own_bits = plan->own_bits;
       }
       fl.next_plan = reinterpret_cast<unsigned int*>(plan->counters.get() + 2 + k);
-      fl.chain = plan->chain != 0 ? plan->chain - 1 : default_chain(c.warps_per_net);
+      // the 16-warp class (the longest searches) may take its own schedule
+      const bool wide = c.warps_per_net == 16;
+      const uint32_t chain = wide ? plan->wide_chain : plan->chain;
+      fl.chain = chain != 0 ? chain - 1 : default_chain(c.warps_per_net);
+      if (wide) fl.bucket_width = plan->wide_bucket_width;
+
     }
     APGAR_B200_CUDA("lattice frontier launch", launch_lattice_frontier(fc, plan->sm_count, stream));
     APGAR_B200_CUDA("lattice pack launch",
@@ -917,7 +927,9 @@ int check_options(const apgar_b200_lattice_options& o) {
     if (o.max_iterations == 0 || o.max_iterations > (1u << 30)) {
       return set_error(APGAR_B200_INTERNAL_INVARIANT, "frontier budget must be 1..2^30 rounds");
     }
-    if (o.chain > 16) return set_error(APGAR_B200_INTERNAL_INVARIANT, "frontier chain must be 0..16");
+    if (o.chain > 16 || o.wide_chain > 16) {
+      return set_error(APGAR_B200_INTERNAL_INVARIANT, "frontier chain must be 0..16");
+    }
     if (o.class_bounds != 0 && !class_bounds_valid(o.class_bounds)) {
       return set_error(APGAR_B200_INTERNAL_INVARIANT,
                        "frontier class bounds must be strictly increasing log2 sizes in 1..31");
@@ -942,7 +954,7 @@ int route_impl(void* lattice, const apgar_b200_lattice_net* nets, uint32_t count
     if (lat->route_plan == nullptr) lat->route_plan = std::make_unique<PlanObject>();
     PlanObject* plan = lat->route_plan.get();
     if (int rc = build_plan(lat, nets, count, o.max_iterations, plan, o.generator, o.bucket_width,
-                            o.chain, o.class_bounds);
+                            o.chain, o.class_bounds, o.wide_bucket_width, o.wide_chain);
         rc != APGAR_B200_OK) {
       return rc;
     }
@@ -976,7 +988,7 @@ extern "C" int apgar_b200_lattice_route(void* lattice, const apgar_b200_lattice_
                                         const volatile uint32_t* cancel,
                                         apgar_b200_lattice_result* results, uint32_t* paths,
                                         uint64_t path_capacity, uint64_t* path_total) {
-  const apgar_b200_lattice_options o{APGAR_B200_LATTICE_SWEEP, max_sweeps, 0, 0, 0};
+  const apgar_b200_lattice_options o{APGAR_B200_LATTICE_SWEEP, max_sweeps, 0, 0, 0, 0, 0};
   return route_impl(lattice, nets, count, o, cancel, results, paths, path_capacity, path_total);
 }
 
@@ -1004,7 +1016,8 @@ extern "C" int apgar_b200_lattice_plan_ex(void* lattice, const apgar_b200_lattic
     auto plan = std::make_unique<PlanObject>();
     if (int rc = build_plan(lat, nets, count, options->max_iterations, plan.get(),
                             options->generator, options->bucket_width, options->chain,
-                            options->class_bounds);
+                            options->class_bounds, options->wide_bucket_width,
+                            options->wide_chain);
         rc != APGAR_B200_OK) {
       return rc;
     }

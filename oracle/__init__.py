@@ -582,10 +582,13 @@ def _window_free(lat, net):
     return bits[:, y0:y0 + h, x0:x0 + w] == 0
 
 
-def corridor_certificate(lat, net, mask):
+def corridor_certificate(lat, net, mask, cell_cost=None):
     """(status, corridor cost or None, least exit key or None) of one net
     for a bool [64][64] coarse corridor (coarse scale as in
-    apgar_b200.corridor.coarse_shift)."""
+    apgar_b200.corridor.coarse_shift).  ``cell_cost`` (optional, uint32
+    [layers][height][width]): per-cell entry prices, paid inside the
+    corridor; an exit's key leaves out its outside cell's price, a lower bound
+    because prices are non-negative."""
     net = np.ascontiguousarray(np.asarray(net).reshape(1))
     n0 = net[0]
     w, h = int(n0["win_w"]), int(n0["win_h"])
@@ -606,7 +609,10 @@ def corridor_certificate(lat, net, mask):
     if not (free[sl, sy, sx] and free[gl, gy, gx]):
         return CORRIDOR_CERTIFIED, None, None  # disconnected either way
     big = 1 << 30
-    price = np.zeros((lat.layers, lat.height, lat.width), dtype=np.uint32)
+    if cell_cost is None:
+        price = np.zeros((lat.layers, lat.height, lat.width), dtype=np.uint32)
+    else:
+        price = np.array(cell_cost, dtype=np.uint32).reshape(lat.layers, lat.height, lat.width)
     price[:, y0:y0 + h, x0:x0 + w][:, ~inside] = big
     cost, _, dist = dijkstra(lat, net, full=True, want_dist=True, cell_cost=price.reshape(-1))
     if cost >= big:

@@ -13,7 +13,8 @@ def test_class_bounds_packing():
     word = apgar_b200.class_bounds(12, 15, 17, 20)
     assert word == 0x14110F0C
     assert autotune.Schedule(class_bounds=word).describe()["class_log2_limits"] == [12, 15, 17, 20]
-    assert autotune.DEFAULT.describe() == {"bucket_width": 0, "chain": 0, "class_log2_limits": None}
+    assert autotune.DEFAULT.describe() == {"bucket_width": 0, "chain": 0, "class_log2_limits": None,
+                                           "wide_bucket_width": 0, "wide_chain": 0}
     with pytest.raises(ValueError):
         apgar_b200.class_bounds(12, 15)
     for bounds in autotune.BOUND_SETS:

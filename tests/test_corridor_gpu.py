@@ -16,12 +16,15 @@ from apgar_b200 import corridor, synth
 pytestmark = pytest.mark.gpu
 
 
-def _run(lat, nets, masks):
+def _run(lat, nets, masks, cell_cost=None):
     dev = apgar_b200.DeviceLattice(lat)
     try:
         plan = dev.plan(nets, generator="frontier")
         bits = torch.from_numpy(corridor.pack(masks).view(np.int32)).cuda().view(torch.uint32)
         plan.set_corridors(bits)
+        if cell_cost is not None:
+            prices = torch.from_numpy(cell_cost.view(np.int32)).cuda().view(torch.uint32)
+            plan.set_cell_costs(prices)
         plan.execute()
         res, paths = plan.readback()
         status = plan.corridor_status()
@@ -31,15 +34,16 @@ def _run(lat, nets, masks):
     return res, apgar_b200.split_paths(res, paths), status
 
 
-def _check(lat, nets, masks):
-    res, paths, status = _run(lat, nets, masks)
-    cost_o, paths_o = oracle.dijkstra_batch(lat, nets)
+def _check(lat, nets, masks, cell_cost=None):
+    res, paths, status = _run(lat, nets, masks, cell_cost)
+    cost_o, paths_o = oracle.dijkstra_batch(lat, nets, cell_cost=cell_cost)
     assert (res["completion"] != apgar_b200.COMPLETION_REJECTED).all()
     assert np.array_equal(res["cost"], cost_o), np.flatnonzero(res["cost"] != cost_o)[:10]
     for i in range(len(nets)):
         if cost_o[i] != oracle.lo_inf():
             assert np.array_equal(paths[i], paths_o[i]), i
-    want = np.array([oracle.corridor_certificate(lat, nets[i], masks[i])[0] for i in range(len(nets))])
+    want = np.array([oracle.corridor_certificate(lat, nets[i], masks[i], cell_cost)[0]
+                     for i in range(len(nets))])
     assert np.array_equal(status, want), (np.flatnonzero(status != want)[:10], status[:10], want[:10])
     return status
 
@@ -112,3 +116,18 @@ def test_repeated_executions_do_not_read_stale_labels():
         plan.close()
     finally:
         dev.close()
+
+
+@pytest.mark.parametrize("radius", [1, 2])
+def test_priced_corridors_match_the_priced_oracle(radius):
+    """Corridor mode under per-cell entry prices (the negotiated rounds'
+    snapshot): costs and canonical paths equal the priced full-window oracle,
+    and each outcome equals the priced certificate restatement."""
+    lat, nets = _case(31 + radius, 64, layers=3)
+    rng = np.random.default_rng(40 + radius)
+    cells = lat.layers * lat.height * lat.width
+    # sparse congestion prices, as a negotiation's snapshot has them
+    cell_cost = np.where(rng.random(cells) < 0.15, rng.integers(1, 120, cells), 0).astype(np.uint32)
+    masks = corridor.segment_corridor(nets, radius) & (rng.random((len(nets), 64, 64)) < 0.95)
+    status = _check(lat, nets, masks, cell_cost)
+    assert (status == corridor.CERTIFIED).any()

@@ -86,3 +86,27 @@ def _priced_out(lat, net, mask):
     price = np.zeros((lat.layers, lat.height, lat.width), np.uint32)
     price[:, y0:y0 + h, x0:x0 + w][:, ~inside] = 1 << 30
     return price.reshape(-1)
+
+
+@pytest.mark.parametrize("seed", [15, 16])
+def test_priced_certificate_is_sound(seed):
+    """Under non-negative entry prices (a negotiated round's snapshot) a
+    certified corridor cost is the priced full-window optimum and its path the
+    priced canonical path."""
+    lat, nets = _case(seed)
+    rng = np.random.default_rng(seed + 7)
+    cells = lat.layers * lat.height * lat.width
+    cell_cost = np.where(rng.random(cells) < 0.2, rng.integers(1, 80, cells), 0).astype(np.uint32)
+    cost_full, paths_full = oracle.dijkstra_batch(lat, nets, cell_cost=cell_cost)
+    seen = set()
+    for radius in (0, 1, 3):
+        masks = corridor.segment_corridor(nets, radius)
+        for i in range(len(nets)):
+            status, cost, bound = oracle.corridor_certificate(lat, nets[i], masks[i], cell_cost)
+            seen.add(status)
+            if status == oracle.CORRIDOR_CERTIFIED and cost is not None:
+                assert cost == cost_full[i]
+                priced = _priced_out(lat, nets[i], masks[i]) + cell_cost
+                _, path, _ = oracle.dijkstra(lat, nets[i], cell_cost=priced)
+                assert np.array_equal(path, paths_full[i]), i
+    assert oracle.CORRIDOR_CERTIFIED in seen
