@@ -13,6 +13,9 @@
 #                                                     host path, built from a
 #                                                     patched copy of the
 #                                                     reference (below)
+#   apgar_b200/adapter/_build/dropin_bench            the drop-in benchmark on the
+#                                                     reference corpus (bench.py
+#                                                     --workload dropin)
 # The patched copy: reference_generator.patch (the B200 persistent generators
 # and their descriptor, the change a maintainer applies to the reference) is
 # applied to copies of the files it touches under _build/ref_patched/, and
@@ -97,3 +100,8 @@ PY
   "$PATCHED/libapgar_ref_patched.a" -L"$ROOT/apgar_b200" -lapgar_b200 -lpthread \
   -Wl,-rpath,'$ORIGIN/../..' -o "$OUT/prepared_batch_check"
 echo "$OUT/prepared_batch_check"
+# the drop-in benchmark on the reference's corpus (bench.py --workload dropin)
+"$CXX" "${PFLAGS[@]}" -Wall -Wextra "$HERE/dropin_bench.cc" "$PATCHED/kicad_fixture.cc" \
+  "$PATCHED/b200_planar_backend.o" "$PATCHED/libapgar_ref_patched.a" -L"$ROOT/apgar_b200" \
+  -lapgar_b200 -lpthread -Wl,-rpath,'$ORIGIN/../..' -o "$OUT/dropin_bench"
+echo "$OUT/dropin_bench"

@@ -1704,6 +1704,15 @@ extern "C" int apgar_b200_negotiation_readback(void* negotiation, uint32_t* usag
   return APGAR_B200_OK;
 }
 
+extern "C" int apgar_b200_negotiation_device_prices(void* negotiation, const uint32_t** cell_costs) {
+  if (negotiation == nullptr || cell_costs == nullptr) {
+    return set_error(APGAR_B200_INTERNAL_INVARIANT, "negotiation prices received a null argument");
+  }
+  *cell_costs = static_cast<NegotiationObject*>(negotiation)->cell_cost.get();
+  clear_error();
+  return APGAR_B200_OK;
+}
+
 extern "C" int apgar_b200_negotiation_release(void* negotiation) {
   delete static_cast<NegotiationObject*>(negotiation);
   return APGAR_B200_OK;

@@ -220,13 +220,35 @@ class LearnedRouter:
         self.bits = torch.empty((n, 128), dtype=torch.uint32, device="cuda")
         plan.set_corridors(self.bits)
 
-    def propose(self, stream: int = 0) -> None:
-        rasters(self.plan, stream=stream, out=(self.rasters, self.dims))
+    def propose(self, stream: int = 0, cell_costs=None) -> None:
+        """Rasters -> CNN -> corridors.  ``cell_costs``: device address (int)
+        or CUDA uint32 tensor of per-cell prices for the congestion channel
+        (a negotiation's snapshot), or None."""
+        if cell_costs is not None and not isinstance(cell_costs, int):
+            cell_costs = cell_costs.data_ptr()
+        _check(lib().apgar_b200_corridor_rasters(
+            self.plan.handle, ctypes.c_void_p(cell_costs) if cell_costs else None,
+            _ptr(self.rasters), _ptr(self.dims), ctypes.c_void_p(stream)))
         self.net.forward(self.rasters, self.dims, acts=self.acts, logits=self.logits, stream=stream)
         corridors(self.plan, self.logits, self.dims, threshold=float(self.policy["threshold"]),
                   dilate=int(self.policy["dilate"]), out=self.bits, stream=stream,
                   max_window_cells=int(self.policy.get("max_window_cells", 0)))
 
+    def clear(self, stream: int = 0) -> None:
+        """No corridor for any net (every window searched at once)."""
+        import torch
+
+        with torch.cuda.stream(torch.cuda.ExternalStream(stream)) if stream else _null():
+            self.bits.zero_()
+
     def execute(self, stream: int = 0) -> None:
         self.propose(stream)
         self.plan.execute(stream)
+
+
+class _null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False

@@ -88,6 +88,30 @@ class Negotiation:
             sum_usage(usage)
             self.step(r, self.PRICE, stream, partial)
 
+    def device_prices(self) -> int:
+        """Device address of the current snapshot prices (uint32 per cell)."""
+        ptr = ctypes.c_void_p()
+        _check(lib().apgar_b200_negotiation_device_prices(self.handle, ctypes.byref(ptr)))
+        return ptr.value
+
+    def run_learned(self, rounds: int, router, stream: int = 0, partial: bool = False,
+                    from_round: int = 1) -> None:
+        """A whole negotiation in split-round steps with a learned corridor
+        proposal before each priced round: ``router`` (a
+        ``learned.LearnedRouter`` on this negotiation's plan) reads the
+        current snapshot as its congestion raster and sets every net's
+        corridor; rounds before ``from_round`` search without corridors.
+        Corridor results are certified or searched again over the window, so
+        the routes, usage and prices equal those of ``run``."""
+        prices = self.device_prices()
+        for r in range(rounds):
+            if r >= from_round:
+                router.propose(stream, cell_costs=prices)
+            else:
+                router.clear(stream)
+            self.step(r, self.ROUTE, stream, partial)
+            self.step(r, self.PRICE, stream, partial)
+
     def readback(self):
         """(usage, history, next snapshot prices, per-round stats list)."""
         usage = np.empty(self.cells, np.uint32)

@@ -68,10 +68,14 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-corridor form (reported beside the headline)")
-    ap.add_argument("--workload", choices=["medium", "negotiated", "full"], default="medium",
+    ap.add_argument("--workload", choices=["medium", "negotiated", "full", "dropin"],
+                    default="medium",
                     help="medium: the headline batch; negotiated: 10 rip-up/reroute rounds "
                          "on the 6 x 4096^2 lattice with multi-terminal nets (one CUDA graph); "
-                         "full: 20 rounds on the 8 x 8192^2 full-scale configuration")
+                         "full: 20 rounds on the 8 x 8192^2 full-scale configuration; dropin: "
+                         "the reference's corpus at 4..512 candidate queries per case through "
+                         "the reference's own prepared batch path over this backend, beside the "
+                         "reference's CPU A*")
     ap.add_argument("--no-tune", action="store_true",
                     help="medium workload: skip the (untimed) frontier schedule autotuner and use "
                          "the library's default schedule")
@@ -455,11 +459,80 @@ def run_negotiated_ranked(args, rank, world, local):
     dist.destroy_process_group()
 
 
+DROPIN_METRIC = ("prepared end-to-end candidate queries/s on the reference's corpus "
+                 "(drop-in through the reference's prepared batch path)")
+
+
+def run_dropin(args, rank):
+    """The drop-in on the reference's own workload: every case of its parity
+    corpus (BuildPhase3CandidateCorpus) at k = 4..512 candidate policies, the
+    prepared end-to-end scope of the reference's report (the view upload once,
+    then per batch: H2D, search, D2H and the reference's host validation and
+    sealing), timed by apgar_b200/adapter/_build/dropin_bench (built with the
+    reference sources), beside the reference's own CPU A* on all host threads
+    and on one.  Pooled throughput = queries over summed medians."""
+    if rank != 0:
+        return
+    exe = os.path.join(ROOT, "apgar_b200", "adapter", "_build", "dropin_bench")
+    if not os.path.exists(exe):
+        raise SystemExit("dropin_bench is not built (apgar_b200/adapter/build_adapter.sh needs the "
+                         "reference sources)")
+    out = subprocess.run([exe], capture_output=True, text=True, timeout=1800)
+    if out.returncode != 0:
+        raise SystemExit("dropin_bench failed: " + out.stderr[-2000:])
+    data = json.loads(out.stdout)
+    ks = [row["k"] for row in data["cases"][0]["k"]]
+    per_k = []
+    tot = {"q": 0, "gpu": 0.0, "par": 0.0, "ser": 0.0, "best": 0.0}
+    for k in ks:
+        rows = [next(r for r in c["k"] if r["k"] == k) for c in data["cases"]]
+        q = k * len(rows)
+        g = sum(r["gpu_ms"] for r in rows)
+        p = sum(r["cpu_par_ms"] for r in rows)
+        s = sum(r["cpu_ser_ms"] for r in rows)
+        best = sum(min(r["cpu_par_ms"], r["cpu_ser_ms"]) for r in rows)
+        tot["q"] += q
+        tot["gpu"] += g
+        tot["par"] += p
+        tot["ser"] += s
+        tot["best"] += best
+        per_k.append({"k": k, "gpu_qps": q / (g / 1e3), "cpu_parallel_qps": q / (p / 1e3),
+                      "cpu_serial_qps": q / (s / 1e3), "gpu_over_faster_cpu": best / g,
+                      "cases_gpu_slower": [c["name"] for c, r in zip(data["cases"], rows)
+                                           if r["gpu_ms"] > min(r["cpu_par_ms"], r["cpu_ser_ms"])]})
+    value = tot["q"] / (tot["gpu"] / 1e3)
+    line = {
+        "metric": DROPIN_METRIC, "value": value, "unit": "queries/s", "n_gpus": 1,
+        "steps": data["repetitions"], "warmup": 1, "ms_per_step": tot["gpu"] / len(ks),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+        "data": "the reference's own parity corpus (generated boards and its KiCad fixture)",
+        "config": {"workload": "BuildPhase3CandidateCorpus, 11 cases, k = " +
+                               ",".join(map(str, ks)) + " candidate policies per batch "
+                               "(BuildDeterministicAlternativePolicies over the base route)",
+                   "generator": "kB200Persistent (compact paths)",
+                   "scope": "prepared end to end: H2D, search, D2H, host validation and sealing; "
+                            "the view upload excluded"},
+        "per_k": per_k,
+        "gpu_over_faster_cpu_pooled": tot["best"] / tot["gpu"],
+        "cpu_baseline": {"value": tot["q"] / (tot["par"] / 1e3), "unit": "queries/s",
+                         "cores": data["threads"], "kind": "reference",
+                         "sample": "the same batches, the reference's RouteWithCpuAStar "
+                                   "compiled from its sources, one query per task",
+                         "serial_value": tot["q"] / (tot["ser"] / 1e3)},
+        "costs_match_cpu": data["costs_match"],
+        "cases": data["cases"],
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     rank, world, local = dist_env()
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "dropin":
+        run_dropin(args, rank)
         return
     if args.workload in ("negotiated", "full"):
         if world > 1 or args.ranked:

@@ -836,6 +836,12 @@ APGAR_B200_API int apgar_b200_negotiation_set_usage_buffer(void* negotiation, ui
 APGAR_B200_API int apgar_b200_negotiation_readback(void* negotiation, uint32_t* usage, uint64_t* history,
                                     uint32_t* cell_costs, apgar_b200_negotiation_round* rounds,
                                     uint32_t round_count);
+/* Device pointer of the negotiation's current snapshot prices (one uint32 per
+ * lattice cell, on the plan's device), written by each round's PRICE step
+ * and read by the next ROUTE: for instance the congestion raster of a
+ * learned corridor proposal between the two (stream-ordered after the
+ * PRICE step's `stream`).  Valid while the negotiation lives. */
+APGAR_B200_API int apgar_b200_negotiation_device_prices(void* negotiation, const uint32_t** cell_costs);
 APGAR_B200_API int apgar_b200_negotiation_release(void* negotiation);
 
 #ifdef __cplusplus
