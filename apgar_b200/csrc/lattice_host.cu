@@ -64,10 +64,15 @@ cudaError_t launch_corridors(const float* logits, const uint32_t* dims,
 
 namespace {
 
-// Width classes: warps per net (each lane holds lattice_cells_per_lane(L)
-// cells of every layer, so a class covers 32 * C * G cells of a frame row).
-constexpr int kGroupSizes[] = {1, 2, 4, 8, 16};
-constexpr int kClassCount = 5;
+// Width classes: warps per net.  A sweep net takes the fewest warps whose
+// lanes cover its frame row (each lane holds lattice_cells_per_lane(L) cells
+// of every layer, so G warps cover 32 * C * G cells): the widest class is
+// issue-bound, and warps past the row's end would run every instruction on
+// padding.  The frontier uses the power-of-two sizes (kFrontierClasses).
+constexpr int kGroupSizes[] = {1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15, 16};
+constexpr int kClassCount = 16;
+// Frontier width classes 0..4 (1, 2, 4, 8 and 16 warps) as kGroupSizes indices.
+constexpr int kFrontierClasses[] = {0, 1, 3, 7, 15};
 constexpr size_t kMaxSmemPerBlock = 227 * 1024;
 
 struct LatticeObject;
@@ -336,7 +341,7 @@ int build_plan(LatticeObject* lat, const apgar_b200_lattice_net* host_nets, uint
     if (frontier) {
       // packed queue entries hold x and y in 14 bits each
       if (n.win_w > 16384u || n.win_h > 16384u) continue;
-      members[frontier_class(cells, plan->class_bounds)].push_back(i);
+      members[kFrontierClasses[frontier_class(cells, plan->class_bounds)]].push_back(i);
       continue;
     }
     const uint32_t frame_width = std::max(n.win_w, n.win_h);

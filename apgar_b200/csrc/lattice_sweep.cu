@@ -827,11 +827,24 @@ cudaError_t launch_one(const SweepLaunch& launch, int max_rows, cudaStream_t str
 
 template <int L, int C>
 cudaError_t launch_layers(int G, const SweepLaunch& launch, int max_rows, cudaStream_t stream) {
+  // every group size 1..16: the host gives a net the fewest warps that
+  // cover its frame row
   switch (G) {
     case 1: return launch_one<L, C, 1>(launch, max_rows, stream);
     case 2: return launch_one<L, C, 2>(launch, max_rows, stream);
+    case 3: return launch_one<L, C, 3>(launch, max_rows, stream);
     case 4: return launch_one<L, C, 4>(launch, max_rows, stream);
+    case 5: return launch_one<L, C, 5>(launch, max_rows, stream);
+    case 6: return launch_one<L, C, 6>(launch, max_rows, stream);
+    case 7: return launch_one<L, C, 7>(launch, max_rows, stream);
     case 8: return launch_one<L, C, 8>(launch, max_rows, stream);
+    case 9: return launch_one<L, C, 9>(launch, max_rows, stream);
+    case 10: return launch_one<L, C, 10>(launch, max_rows, stream);
+    case 11: return launch_one<L, C, 11>(launch, max_rows, stream);
+    case 12: return launch_one<L, C, 12>(launch, max_rows, stream);
+    case 13: return launch_one<L, C, 13>(launch, max_rows, stream);
+    case 14: return launch_one<L, C, 14>(launch, max_rows, stream);
+    case 15: return launch_one<L, C, 15>(launch, max_rows, stream);
     case 16: return launch_one<L, C, 16>(launch, max_rows, stream);
     default: return cudaErrorInvalidValue;
   }
