@@ -4,18 +4,21 @@
 //
 // Layout.  Every net owns a 64 x 64 coarse grid (coarse cell = 2^s x 2^s
 // window cells on all layers, the corridor bitmap's scale); only the top-left
-// cw x ch cells lie inside the window.  Tensors are NHWC bf16 [net][64][64][C];
-// cells outside the window are never read (treated as zero, "same" padding at
-// the window border) and never written.
+// cw x ch cells lie inside the window.  Tensors are NHWC bf16 [net][66][64][C]
+// (grid row y stored at y + 1); the producers write the pad row above and
+// grid rows 0 .. ch with the cells outside the window as zeros ("same"
+// padding at the window border), which is all an in-window output reads.
 //
 // Layers 1-5 (3x3, 16 -> 32 then 32 -> 32, bias, ReLU) run as implicit GEMMs
-// on the 5th-generation tensor cores: a CTA takes 128 output cells (two rows
-// of one net), gathers their 3x3 neighbourhoods (im2col) into shared memory
-// as the A operand (M = 128 cells, K = 9 * Cin, K-major, no swizzle), keeps
-// the weights resident as the B operand (N = 32 channels), and one elected
-// thread issues tcgen05.mma (kind::f16, bf16 x bf16 -> f32) into a 128 x 32
-// tensor-memory accumulator.  The epilogue reads it back with tcgen05.ld (one
-// warp per 32 TMEM lanes), adds the bias, applies the ReLU and stores bf16.
+// on the 5th-generation tensor cores: a tile is 128 output cells (two rows of
+// one net); TMA stages its four input rows once as channel planes in shared
+// memory, each of the 9 taps' A operands is a shifted descriptor into that
+// stage (M = 128 cells, K = Cin, K-major, no swizzle, no im2col copy), the
+// weights stay resident as the B operand (N = 32 channels), and one thread
+// issues tcgen05.mma (kind::f16, bf16 x bf16 -> f32) into a 128 x 32
+// tensor-memory accumulator.  Loads, MMAs and the epilogue (tcgen05.ld, one
+// warp per 32 TMEM lanes: bias, ReLU, bf16 stores) are separate warp roles
+// handed over by mbarriers, several tiles in flight.
 // The input gradient of layers 2-5 is the same kernel run on the output
 // gradient with the spatially flipped, transposed weights; its epilogue gates
 // by the previous layer's ReLU.  The weight gradient is a second tcgen05 GEMM:
@@ -27,11 +30,14 @@
 // The head (3x3, 32 -> 1, FP32 weights), the loss, the bias gradients, Adam
 // and the corridor extraction are small and run on the CUDA cores.
 //
-// Every wait on a tensor-core completion is bounded: on expiry the kernel
-// records APGAR_B200_CNN_TIMEOUT in its error word, waits once more (bounded)
-// for its own MMAs, frees its tensor memory and returns.
+// Every mbarrier wait (TMA loads, tensor-core completions, the hand-offs
+// between warp roles) is bounded: on expiry the kernel records
+// APGAR_B200_CNN_TIMEOUT in its error word, waits once more (bounded) for its
+// own copies and MMAs in flight, frees its tensor memory and returns.
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <cstdint>
 
@@ -184,54 +190,87 @@ __device__ __forceinline__ void unpack8(uint4 q, float* v) {
 
 // ------------------------------- rasters ----------------------------------
 
-// One block per net: the 16 input channels of every coarse cell, plus the
-// net's coarse dims (cw | ch << 8 | s << 16).
-__global__ void raster_kernel(LatticeDeviceView lat, const apgar_b200_lattice_net* __restrict__ nets,
-                              uint32_t count, const uint32_t* __restrict__ cell_cost,
-                              __nv_bfloat16* __restrict__ out, uint32_t* __restrict__ dims) {
+// One block per net: the 16 input channels of every coarse cell of rows
+// -1 .. ch (the rows any in-window output reads; row ch and the columns
+// cw .. 63 are zero), plus the net's coarse dims (cw | ch << 8 | s << 16).
+// The blocked counts are gathered over (fine row, mask word) pairs of the
+// window, every layer's word of a pair loaded together, and summed per
+// coarse cell exactly (integer shared-memory atomics); a thread per coarse
+// cell then forms its channels.
+__global__ void __launch_bounds__(256) raster_kernel(LatticeDeviceView lat,
+                                                     const apgar_b200_lattice_net* __restrict__ nets,
+                                                     uint32_t count, const uint32_t* __restrict__ cell_cost,
+                                                     __nv_bfloat16* __restrict__ out,
+                                                     uint32_t* __restrict__ dims) {
+  __shared__ uint32_t blocked_sum[kCells], all_sum[kCells];
   const uint32_t n = blockIdx.x;
   if (n >= count) return;
+  const int tid = threadIdx.x;
   const apgar_b200_lattice_net net = nets[n];
   const int w = static_cast<int>(net.win_w), h = static_cast<int>(net.win_h);
   int s = 2;
   while ((((w > h ? w : h) - 1) >> s) >= kGrid - 1) ++s;  // at most 63 coarse cells a side
   const int cw = (w + (1 << s) - 1) >> s, ch = (h + (1 << s) - 1) >> s;
-  if (threadIdx.x == 0) dims[n] = static_cast<uint32_t>(cw) | (static_cast<uint32_t>(ch) << 8) |
-                                  (static_cast<uint32_t>(s) << 16);
-  const float scx = static_cast<float>((static_cast<int>(net.start_x) - static_cast<int>(net.win_x0)) >> s);
-  const float scy = static_cast<float>((static_cast<int>(net.start_y) - static_cast<int>(net.win_y0)) >> s);
-  const float gcx = static_cast<float>((static_cast<int>(net.goal_x) - static_cast<int>(net.win_x0)) >> s);
-  const float gcy = static_cast<float>((static_cast<int>(net.goal_y) - static_cast<int>(net.win_y0)) >> s);
+  if (tid == 0) dims[n] = static_cast<uint32_t>(cw) | (static_cast<uint32_t>(ch) << 8) |
+                          (static_cast<uint32_t>(s) << 16);
+  const int rows = min(ch, kGrid - 1) + 1;  // grid rows written: 0 .. ch
+  for (int c = tid; c < rows * kGrid; c += blockDim.x) {
+    blocked_sum[c] = 0u;
+    all_sum[c] = 0u;
+  }
+  __syncthreads();
+  const int x0w = static_cast<int>(net.win_x0), y0w = static_cast<int>(net.win_y0);
+  const int wlo = x0w >> 5, nw = ((x0w + w - 1) >> 5) - wlo + 1;
+  for (int u = tid; u < h * nw; u += blockDim.x) {
+    const int y = u / nw, wi = wlo + u % nw;
+    // window columns of this word, and the coarse cells they fall in
+    const int fx0 = max(0, (wi << 5) - x0w), fx1 = min(w, (wi << 5) + 32 - x0w);
+    const int cx0 = fx0 >> s, cx1 = (fx1 - 1) >> s;  // at most 9 coarse cells (s >= 2)
+    uint32_t m[9], b[9];
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+      const int cx = cx0 + j;
+      const int lo = max(fx0, cx << s) + x0w - (wi << 5), hi = min(fx1, (cx + 1) << s) + x0w - (wi << 5);
+      m[j] = cx <= cx1 ? (hi >= 32 ? 0xFFFFFFFFu : ((1u << hi) - 1u)) & ~((1u << lo) - 1u) : 0u;
+      b[j] = 0u;
+    }
+    const uint32_t* word = lat.blocked + static_cast<size_t>(y0w + y) * lat.words + wi;
+    const size_t layer_stride = static_cast<size_t>(lat.height) * lat.words;
+    uint32_t all = 0xFFFFFFFFu;
+#pragma unroll 4
+    for (int l = 0; l < lat.layers; ++l) {
+      const uint32_t v = __ldg(word + l * layer_stride);
+      all &= v;
+#pragma unroll
+      for (int j = 0; j < 9; ++j) b[j] += __popc(v & m[j]);
+    }
+    const int cy = y >> s;
+#pragma unroll
+    for (int j = 0; j < 9; ++j) {
+      // m[j] is zero past cx1: nothing is added there
+      if (b[j] != 0u) atomicAdd(&blocked_sum[cy * kGrid + cx0 + j], b[j]);
+      const uint32_t a = __popc(all & m[j]);
+      if (a != 0u) atomicAdd(&all_sum[cy * kGrid + cx0 + j], a);
+    }
+  }
+  __syncthreads();
+  const float scx = static_cast<float>((static_cast<int>(net.start_x) - x0w) >> s);
+  const float scy = static_cast<float>((static_cast<int>(net.start_y) - y0w) >> s);
+  const float gcx = static_cast<float>((static_cast<int>(net.goal_x) - x0w) >> s);
+  const float gcy = static_cast<float>((static_cast<int>(net.goal_y) - y0w) >> s);
   const float sgx = gcx - scx, sgy = gcy - scy;
   const float seg2 = sgx * sgx + sgy * sgy;
-  for (int c = threadIdx.x; c < kCells; c += blockDim.x) {
-    const int cy = c / kGrid, cx = c % kGrid;
+  for (int c = tid; c < (rows + 1) * kGrid; c += blockDim.x) {
+    const int cy = c / kGrid - 1, cx = c % kGrid;  // row -1: the zero pad row above the grid
     float v[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = 0.f;
-    if (cx < cw && cy < ch) {
+    if (cx < cw && cy >= 0 && cy < ch) {
       const int x0 = cx << s, x1 = min(w, (cx + 1) << s);
       const int y0 = cy << s, y1 = min(h, (cy + 1) << s);
-      const int gx0 = static_cast<int>(net.win_x0) + x0, gx1 = static_cast<int>(net.win_x0) + x1;
-      uint32_t blocked = 0, all_blocked = 0;
-      for (int y = y0; y < y1; ++y) {
-        const int gy = static_cast<int>(net.win_y0) + y;
-        for (int wi = gx0 >> 5; wi <= (gx1 - 1) >> 5; ++wi) {
-          const int lo = max(gx0, wi << 5) - (wi << 5), hi = min(gx1, (wi + 1) << 5) - (wi << 5);
-          const uint32_t m = (hi >= 32 ? 0xFFFFFFFFu : ((1u << hi) - 1u)) & ~((1u << lo) - 1u);
-          uint32_t all = 0xFFFFFFFFu;
-          for (int l = 0; l < lat.layers; ++l) {
-            const uint32_t word =
-                __ldg(lat.blocked + (static_cast<size_t>(l) * lat.height + gy) * lat.words + wi);
-            blocked += __popc(word & m);
-            all &= word;
-          }
-          all_blocked += __popc(all & m);
-        }
-      }
       const float cells = static_cast<float>((x1 - x0) * (y1 - y0));
-      v[0] = static_cast<float>(blocked) / (cells * static_cast<float>(lat.layers));
-      v[1] = static_cast<float>(all_blocked) / cells;
+      v[0] = static_cast<float>(blocked_sum[cy * kGrid + cx]) / (cells * static_cast<float>(lat.layers));
+      v[1] = static_cast<float>(all_sum[cy * kGrid + cx]) / cells;
       if (cell_cost != nullptr) {
         // congestion: mean entry price over a sample of at most 4 x 4 cells per layer
         const int step = max(1, (1 << s) / 4);
@@ -265,12 +304,6 @@ __global__ void raster_kernel(LatticeDeviceView lat, const apgar_b200_lattice_ne
     uint4* dst = reinterpret_cast<uint4*>(out + act_cell(n, cy, cx) * kCin0);
     dst[0] = pack8(v);
     dst[1] = pack8(v + 8);
-  }
-  // the zero pad rows above and below the grid
-  for (int c = threadIdx.x; c < 2 * kGrid; c += blockDim.x) {
-    uint4* dst = reinterpret_cast<uint4*>(out + act_cell(n, c < kGrid ? -1 : kGrid, c % kGrid) * kCin0);
-    dst[0] = make_uint4(0u, 0u, 0u, 0u);
-    dst[1] = make_uint4(0u, 0u, 0u, 0u);
   }
 }
 
@@ -359,151 +392,259 @@ __device__ __forceinline__ uint4 halo_chunk(const uint8_t* halo, int m, int t, i
 }
 
 // The forward conv's operands.  A: the tile's four input rows (y0 - 1 ..
-// y0 + 2, 64 cells each) staged once as CIN / 8 planes of 16-byte chunks
-// (8 channels of one cell), one zero guard cell at each end of a plane.  The
-// A operand of tap (dy, dx) for the 128 output cells is the staged run that
-// starts at cell 1 + (1 + dy) * 64 + dx: K-major, 8-cell groups 128 bytes
-// apart (SBO), the two chunks of a K = 16 step one plane apart (LBO).  No
-// im2col copy.  B: the weights, [32 rows][9 * CIN], K-major.
+// y0 + 2, 64 cells each) staged as CIN / 8 planes of 16-byte chunks (8
+// channels of one cell).  Each plane is [128-byte lead][256 cells][128-byte
+// tail]; the last chunk of the lead and the first of the tail are zero guard
+// cells.  The A operand of tap (dy, dx) for the 128 output cells is the
+// staged run that starts at cell (1 + dy) * 64 + dx: K-major, 8-cell groups
+// 128 bytes apart (SBO), the two chunks of a K = 16 step one plane apart
+// (LBO).  No im2col copy.  B: the weights, [32 rows][9 * CIN], K-major.
+//
+// Roles (warp-specialised, 192 threads): warp 4 lane 0 loads stages with TMA
+// (a 3-D tensor map over the NHWC tensor, {8 channels, chunk, cell}, whose
+// box {8, 1, 256} lands one plane: the NHWC -> planar transposition is done
+// by the copy engine); warp 5 lane 0 issues the MMAs; warps 0-3 (TMEM lanes
+// 0-127) drain the accumulators.  Stages and accumulators form rings handed
+// over by mbarriers, so loads, MMAs and epilogues of different tiles overlap.
+// Pipeline depth: stages (A tiles in flight) and accumulators per CTA, CTAs
+// per SM.
+constexpr int kConvStages = 3, kConvAccs = 2, kConvPerSm = 3;
+static_assert((kConvAccs & (kConvAccs - 1)) == 0, "TMEM allocations are powers of two columns");
+
 template <int CIN>
 struct ConvSmem {
   static constexpr int K = 9 * CIN;
   static constexpr int kChunks = K / 8;                 // 16-byte chunks per B row
   static constexpr int kSboB = kChunks * 128;           // bytes between 8-row groups of B
   static constexpr int kBytesB = 4 * kSboB;             // 32 rows
-  static constexpr int kStageCells = 4 * kGrid + 2;     // 4 rows and two guards
-  static constexpr int kPlane = kStageCells * 16;       // bytes per channel-chunk plane
+  static constexpr int kLead = 128;                     // plane bytes before cell 0
+  static constexpr int kPlane = kLead + 4 * kGrid * 16 + 128;
   static constexpr int kBytesA = (CIN / 8) * kPlane;
-  static constexpr int kBytes = kBytesA + kBytesB + 16;
+  static constexpr int kTx = (CIN / 8) * 4 * kGrid * 16;  // TMA bytes per stage
+  static constexpr int kStages = kConvStages;
+  static constexpr int kAccs = kConvAccs;               // 32-column accumulators
+  static constexpr int kOffB = kStages * kBytesA;
+  static constexpr int kOffBias = kOffB + kBytesB;      // 32 f32
+  static constexpr int kOffBar = kOffBias + 128;        // full, empty, accfull, accempty
+  static constexpr int kBytes = kOffBar + 8 * (2 * kStages + 2 * kAccs);
+  static_assert(kPlane % 128 == 0 && kBytesA % 128 == 0, "TMA destinations are 128-byte aligned");
 };
 
+constexpr int kConvThreads = 192;
+constexpr int kEpiWarps = 4;
+
+__device__ __forceinline__ void bar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+// One plane of a stage: box {8, 1, 256} at {0, chunk, cell} of the tensor map.
+__device__ __forceinline__ void tma_load_plane(uint32_t dst, const CUtensorMap* map, int chunk, int cell,
+                                               uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(chunk), "r"(cell), "r"(bar)
+      : "memory");
+}
+
+// The next tile of this CTA's strided item sequence after `item` that has
+// rows to write (y0 <= ch), or `items` when there is none.
+__device__ __forceinline__ uint32_t next_conv_item(const uint32_t* dims, uint32_t item, uint32_t items) {
+  for (; item < items; item += gridDim.x) {
+    const uint32_t d = __ldg(dims + item / (kGrid / 2));
+    if (static_cast<int>(item % (kGrid / 2)) * 2 <= static_cast<int>(dims_h(d))) return item;
+  }
+  return items;
+}
+
 // out[cell][co] = epilogue(sum_{tap, ci} x[cell + tap][ci] * w[co][tap][ci]).
+// `xmap`: the input as {8 channels, CIN / 8 chunks, count * 66 * 64 cells}.
 template <int CIN, int EPI>
-__global__ void __launch_bounds__(128) conv3x3_tc_kernel(ConvArgs a) {
+__global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const __grid_constant__ CUtensorMap xmap,
+                                                                  ConvArgs a) {
   using S = ConvSmem<CIN>;
-  constexpr int kPer = 4 * kGrid * (CIN / 8) / 128;  // staged chunks per thread
+  constexpr int kSt = S::kStages, kAc = S::kAccs;
   extern __shared__ __align__(1024) uint8_t smem[];
-  uint8_t* sa = smem;
-  uint8_t* sb = smem + S::kBytesA;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(smem + S::kBytesA + S::kBytesB);
+  uint8_t* sb = smem + S::kOffB;
+  float* sbias = reinterpret_cast<float*>(smem + S::kOffBias);
+  const uint32_t bar0 = smem_addr(smem + S::kOffBar);
+  // barrier addresses: full[s], empty[s], accfull[q], accempty[q]
+  const auto full = [&](int st) { return bar0 + 8u * static_cast<uint32_t>(st); };
+  const auto empty = [&](int st) { return bar0 + 8u * static_cast<uint32_t>(kSt + st); };
+  const auto accfull = [&](int q) { return bar0 + 8u * static_cast<uint32_t>(2 * kSt + q); };
+  const auto accempty = [&](int q) { return bar0 + 8u * static_cast<uint32_t>(2 * kSt + kAc + q); };
   __shared__ uint32_t tmem_slot;
+  __shared__ int abort_flag;
+  __shared__ uint32_t loaded, waited;  // stages loaded / whose loads the MMA role waited for
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   // weights: the resident B operand (N = 32 rows, K-major)
-  for (int u = tid; u < 32 * S::kChunks; u += 128) {
+  for (int u = tid; u < 32 * S::kChunks; u += kConvThreads) {
     const int n = u / S::kChunks, c = u % S::kChunks;
     const uint4 v = __ldg(reinterpret_cast<const uint4*>(a.w + static_cast<size_t>(n) * S::K) + c);
     *reinterpret_cast<uint4*>(sb + (n % 8) * 16 + (n / 8) * S::kSboB + c * 128) = v;
   }
-  // the guard cells of every plane stay zero
-  if (tid < 2 * (CIN / 8)) {
-    const int j = tid >> 1;
-    *reinterpret_cast<uint4*>(sa + j * S::kPlane + ((tid & 1) ? (S::kStageCells - 1) * 16 : 0)) =
+  if constexpr (EPI == kEpiRelu) {
+    if (tid < 32) sbias[tid] = __ldg(a.bias + tid);
+  }
+  // the guard cells of every plane of every stage stay zero (TMA writes cells only)
+  for (int u = tid; u < 2 * kSt * (CIN / 8); u += kConvThreads) {
+    const int plane = u >> 1;  // stage * (CIN / 8) + chunk
+    *reinterpret_cast<uint4*>(smem + plane * S::kPlane +
+                              ((u & 1) ? S::kLead + 4 * kGrid * 16 : S::kLead - 16)) =
         make_uint4(0u, 0u, 0u, 0u);
   }
-  if (warp == 0) tmem_alloc(&tmem_slot, 32);
-  if (tid == 0) bar_init(smem_addr(bar), 1);
+  if (warp == 5) tmem_alloc(&tmem_slot, 32 * kAc);
+  if (tid == 0) {
+    for (int st = 0; st < kSt; ++st) {
+      bar_init(full(st), 1);
+      bar_init(empty(st), 1);
+    }
+    for (int q = 0; q < kAc; ++q) {
+      bar_init(accfull(q), 1);
+      bar_init(accempty(q), 32 * kEpiWarps);
+    }
+    abort_flag = 0;
+    loaded = waited = 0;
+  }
   fence_async_smem();
   fence_before_sync();
   __syncthreads();
   fence_after_sync();
   const uint32_t tmem = tmem_slot;
-  const uint32_t idesc = idesc_bf16(128, 32, 0, 0);
-  uint32_t phase = 0;
-  bool failed = false;
-
   const uint32_t items = a.count * (kGrid / 2);
-  for (uint32_t item = blockIdx.x; item < items; item += gridDim.x) {
-    const uint32_t net = item / (kGrid / 2);
-    const int y0 = static_cast<int>(item % (kGrid / 2)) * 2;
-    const uint32_t d = a.dims[net];
-    const int cw = static_cast<int>(dims_w(d)), ch = static_cast<int>(dims_h(d));
-    // rows up to ch are written (row ch as zeros: the next layer's taps read it)
-    if (y0 > ch) continue;  // uniform
-    // stage rows y0 - 1 .. y0 + 2: 256 contiguous cells of the padded tensor,
-    // every load of a thread in flight before its first store
-    {
-      const uint4* src = reinterpret_cast<const uint4*>(a.x + act_cell(net, y0 - 1, 0) * CIN);
-      uint4 v[kPer];
+  const volatile int* abort_v = &abort_flag;
+  // a bounded wait; on expiry every role stops at its next check
+  const auto wait = [&](uint32_t bar, uint32_t parity) {
+    if (bar_wait(bar, parity)) return true;
+    atomicExch(&abort_flag, 1);
+    return false;
+  };
+
+  if (warp == 4) {
+    // ---- producer: one thread, four (two) plane loads per stage ----
+    if (lane == 0) {
+      uint32_t k = 0;
+      for (uint32_t item = next_conv_item(a.dims, blockIdx.x, items); item < items;
+           item = next_conv_item(a.dims, item + gridDim.x, items), ++k) {
+        const int st = static_cast<int>(k % kSt);
+        if (*abort_v || !wait(empty(st), ((k / kSt) & 1u) ^ 1u)) break;
+        const uint32_t net = item / (kGrid / 2);
+        const int y0 = static_cast<int>(item % (kGrid / 2)) * 2;
+        const int cell = static_cast<int>((static_cast<size_t>(net) * kPadRows + y0) * kGrid);  // row y0 - 1
+        const uint32_t dst = smem_addr(smem + st * S::kBytesA) + S::kLead;
+        bar_expect_tx(full(st), S::kTx);
 #pragma unroll
-      for (int k = 0; k < kPer; ++k) v[k] = __ldg(src + tid + k * 128);
-#pragma unroll
-      for (int k = 0; k < kPer; ++k) {
-        const int u = tid + k * 128;
-        const int j = u % (CIN / 8), c = u / (CIN / 8);
-        *reinterpret_cast<uint4*>(sa + j * S::kPlane + (1 + c) * 16) = v[k];
+        for (int j = 0; j < CIN / 8; ++j) tma_load_plane(dst + j * S::kPlane, &xmap, j, cell, full(st));
       }
+      loaded = k;
     }
-    fence_async_smem();
-    __syncthreads();
-    if (tid == 0) {
+  } else if (warp == 5) {
+    // ---- MMA issuer: one thread, 9 taps x CIN / 16 K-steps per tile ----
+    if (lane == 0) {
+      const uint32_t idesc = idesc_bf16(128, 32, 0, 0);
+      const uint32_t b0 = smem_addr(sb);
+      uint32_t k = 0, consumed = 0;
+      for (uint32_t item = next_conv_item(a.dims, blockIdx.x, items); item < items;
+           item = next_conv_item(a.dims, item + gridDim.x, items), ++k) {
+        const int st = static_cast<int>(k % kSt), q = static_cast<int>(k % kAc);
+        if (*abort_v || !wait(full(st), (k / kSt) & 1u)) break;
+        ++consumed;
+        if (!wait(accempty(q), ((k / kAc) & 1u) ^ 1u)) break;
+        fence_after_sync();
+        const uint32_t a0 = smem_addr(smem + st * S::kBytesA) + S::kLead;
+        const uint32_t acc = tmem + static_cast<uint32_t>(q * 32);
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+          const int off = (t / 3) * kGrid + (t % 3 - 1);  // staged cell of output 0
+#pragma unroll
+          for (int jj = 0; jj < CIN / 16; ++jj) {
+            const int kk = t * (CIN / 16) + jj;
+            mma_bf16(acc, umma_desc(a0 + 2 * jj * S::kPlane + off * 16, S::kPlane, 128),
+                     umma_desc(b0 + kk * 256, 128, S::kSboB), idesc, kk > 0 ? 1u : 0u);
+          }
+        }
+        mma_commit(empty(st));  // the stage is free once these MMAs have read it
+        mma_commit(accfull(q));
+      }
+      waited = consumed;
+      // the last tile's MMAs (all earlier ones complete before it) are done
+      // before the CTA can free its tensor memory
+      if (k > 0) wait(accfull(static_cast<int>((k - 1) % kAc)), ((k - 1) / kAc) & 1u);
+    }
+  } else {
+    // ---- epilogue: warps 0-3, thread = accumulator row = cell m ----
+    uint32_t k = 0;
+    for (uint32_t item = next_conv_item(a.dims, blockIdx.x, items); item < items;
+         item = next_conv_item(a.dims, item + gridDim.x, items), ++k) {
+      const int q = static_cast<int>(k % kAc);
+      const bool ok = !*abort_v && wait(accfull(q), (k / kAc) & 1u);
+      if (__any_sync(0xFFFFFFFFu, !ok)) break;  // warp-uniform: tcgen05.ld is .sync.aligned
       fence_after_sync();
-      const uint32_t a0 = smem_addr(sa), b0 = smem_addr(sb);
-#pragma unroll 1
-      for (int t = 0; t < 9; ++t) {
-        const int first = 1 + (1 + t / 3 - 1) * kGrid + (t % 3 - 1);  // staged cell of output 0
+      float o[32];
+      tmem_load32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(q * 32), o);
+      fence_before_sync();
+      bar_arrive(accempty(q));
+      const uint32_t net = item / (kGrid / 2);
+      const int y0 = static_cast<int>(item % (kGrid / 2)) * 2;
+      const uint32_t d = __ldg(a.dims + net);
+      const int cw = static_cast<int>(dims_w(d)), ch = static_cast<int>(dims_h(d));
+      const int m = warp * 32 + lane;
+      const int py = y0 + m / kGrid, px = m % kGrid;
+      const size_t cell = act_cell(net, py, px);
+      // cells outside the window are written as zeros (the layout's invariant)
+      if (px < cw && py < ch) {
+        if constexpr (EPI == kEpiRelu) {
 #pragma unroll
-        for (int jj = 0; jj < CIN / 16; ++jj) {
-          const int kk = t * (CIN / 16) + jj;
-          mma_bf16(tmem, umma_desc(a0 + 2 * jj * S::kPlane + first * 16, S::kPlane, 128),
-                   umma_desc(b0 + kk * 256, 128, S::kSboB), idesc, kk > 0 ? 1u : 0u);
+          for (int c4 = 0; c4 < 8; ++c4) {
+            const float4 b4 = reinterpret_cast<const float4*>(sbias)[c4];
+            o[4 * c4 + 0] = fmaxf(o[4 * c4 + 0] + b4.x, 0.f);
+            o[4 * c4 + 1] = fmaxf(o[4 * c4 + 1] + b4.y, 0.f);
+            o[4 * c4 + 2] = fmaxf(o[4 * c4 + 2] + b4.z, 0.f);
+            o[4 * c4 + 3] = fmaxf(o[4 * c4 + 3] + b4.w, 0.f);
+          }
+        } else {
+          const uint4* g = reinterpret_cast<const uint4*>(a.gate + cell * kCh);
+#pragma unroll
+          for (int qq = 0; qq < 4; ++qq) {
+            float gv[8];
+            unpack8(__ldg(g + qq), gv);
+#pragma unroll
+            for (int i = 0; i < 8; ++i) o[qq * 8 + i] = gv[i] > 0.f ? o[qq * 8 + i] : 0.f;
+          }
         }
-      }
-      mma_commit(smem_addr(bar));
-    }
-    const bool ok = bar_wait(smem_addr(bar), phase);
-    phase ^= 1u;
-    if (__syncthreads_or(!ok)) {
-      failed = true;
-      break;
-    }
-    fence_after_sync();
-    // epilogue: thread = accumulator row = cell m; cells outside the window
-    // are written as zeros (the layout's invariant)
-    float v[32];
-    tmem_load32(tmem + (static_cast<uint32_t>(warp * 32) << 16), v);
-    const int m = warp * 32 + lane;
-    const int py = y0 + m / kGrid, px = m % kGrid;
-    const size_t cell = act_cell(net, py, px);
-    if (px < cw && py < ch) {
-      if constexpr (EPI == kEpiRelu) {
-#pragma unroll
-        for (int c = 0; c < 32; ++c) v[c] = fmaxf(v[c] + __ldg(a.bias + c), 0.f);
       } else {
-        const uint4* g = reinterpret_cast<const uint4*>(a.gate + cell * kCh);
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          float gv[8];
-          unpack8(__ldg(g + q), gv);
-#pragma unroll
-          for (int i = 0; i < 8; ++i) v[q * 8 + i] = gv[i] > 0.f ? v[q * 8 + i] : 0.f;
-        }
+        for (int c = 0; c < 32; ++c) o[c] = 0.f;
       }
-    } else {
+      if (py < kGrid) {
+        uint4* dst = reinterpret_cast<uint4*>(a.y + cell * kCh);
 #pragma unroll
-      for (int c = 0; c < 32; ++c) v[c] = 0.f;
-    }
-    if (py < kGrid) {
-      uint4* dst = reinterpret_cast<uint4*>(a.y + cell * kCh);
+        for (int qq = 0; qq < 4; ++qq) dst[qq] = pack8(o + qq * 8);
+      }
+      if (y0 == 0 && m < kGrid) {
+        // the zero pad row above the grid
+        uint4* pad = reinterpret_cast<uint4*>(a.y + act_cell(net, -1, m) * kCh);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) dst[q] = pack8(v + q * 8);
+        for (int qq = 0; qq < 4; ++qq) pad[qq] = make_uint4(0u, 0u, 0u, 0u);
+      }
     }
-    if (y0 == 0 && m < kGrid) {
-      // the zero pad row above the grid
-      uint4* pad = reinterpret_cast<uint4*>(a.y + act_cell(net, -1, m) * kCh);
-#pragma unroll
-      for (int q = 0; q < 4; ++q) pad[q] = make_uint4(0u, 0u, 0u, 0u);
-    }
-    fence_before_sync();
-    __syncthreads();
   }
-  if (failed) {
-    if (tid == 0) atomicOr(a.error, APGAR_B200_CNN_TIMEOUT);
-    bar_wait(smem_addr(bar), phase);  // once more, bounded, for the MMAs in flight
+  __syncthreads();
+  if (warp == 4 && lane == 0) {
+    // loads nobody waited for (only after an expired wait): let them land
+    // before the CTA's shared memory goes away
+    for (uint32_t k = waited; k < loaded; ++k) {
+      bar_wait(full(static_cast<int>(k % kSt)), (k / kSt) & 1u);
+    }
   }
+  if (tid == 0 && abort_flag) atomicOr(a.error, APGAR_B200_CNN_TIMEOUT);
   fence_before_sync();
   __syncthreads();
-  if (warp == 0) tmem_free(tmem, 32);
+  fence_after_sync();
+  if (warp == 5) tmem_free(tmem, 32 * kAc);
 }
 
 // ------------------- weight gradient on tensor cores ----------------------
@@ -641,37 +782,73 @@ __global__ void __launch_bounds__(128) conv_wgrad_tc_kernel(WgradArgs a) {
 
 // ------------------------------ head + loss -------------------------------
 
-// logit[cell] = b6 + sum_{tap, ci} w6[tap][ci] * act[cell + tap][ci] (FP32).
-__global__ void head_forward_kernel(const __nv_bfloat16* __restrict__ act, const float* __restrict__ w6,
-                                    const float* __restrict__ b6, const uint32_t* __restrict__ dims,
-                                    uint32_t count, float* __restrict__ logits) {
-  __shared__ float ws[9 * kCh];
+// logit[cell] = b6 + sum_{tap, ci} w6[tap][ci] * act[cell + tap][ci] (FP32,
+// taps outside the window skipped, outside cells 0).  A block takes one band
+// of kHeadRows rows of one net: it stages the band's rows and their halo
+// (rows y0 - 1 .. y0 + kHeadRows, window rows only) in shared memory with
+// cp.async, the 16-byte chunks of a cell rotated by its column (chunk q of
+// cell x at slot q ^ (x & 3)) so that a warp's 32 neighbouring cells read
+// conflict-free; each thread then sums its cells' 288 products in the same
+// order as a plain per-cell loop.
+constexpr int kHeadRows = 8;
+constexpr int kHeadBands = kGrid / kHeadRows;
+constexpr int kHeadStageRows = kHeadRows + 2;
+constexpr int kHeadSmem = kHeadStageRows * kGrid * kCh * 2;
+
+__global__ void __launch_bounds__(256, 3) head_forward_kernel(const __nv_bfloat16* __restrict__ act,
+                                                           const float* __restrict__ w6,
+                                                           const float* __restrict__ b6,
+                                                           const uint32_t* __restrict__ dims, uint32_t count,
+                                                           float* __restrict__ logits) {
+  extern __shared__ __align__(16) uint8_t hs[];  // [kHeadStageRows][64 cells][4 chunks]
+  __shared__ __align__(16) float ws[9 * kCh];
+  const uint32_t net = blockIdx.x / kHeadBands;
+  const int y0 = static_cast<int>(blockIdx.x % kHeadBands) * kHeadRows;
+  if (net >= count) return;
+  const uint32_t d = dims[net];
+  const int cw = static_cast<int>(dims_w(d)), ch = static_cast<int>(dims_h(d));
+  float* out = logits + grid_cell(net, y0, 0);
+  if (y0 >= ch) {  // uniform: a band below the window
+    for (int i = threadIdx.x; i < kHeadRows * kGrid; i += blockDim.x) out[i] = 0.f;
+    return;
+  }
   for (int i = threadIdx.x; i < 9 * kCh; i += blockDim.x) ws[i] = w6[i];
+  // window rows of the halo: y0 - 1 .. y0 + kHeadRows, clipped to [0, ch)
+  const int r0 = max(y0 - 1, 0), r1 = min(y0 + kHeadRows, ch - 1);
+  const uint8_t* src = reinterpret_cast<const uint8_t*>(act + act_cell(net, r0, 0) * kCh);
+  const int chunks = (r1 - r0 + 1) * kGrid * 4;
+  const uint32_t base = static_cast<uint32_t>(__cvta_generic_to_shared(hs));
+  for (int u = threadIdx.x; u < chunks; u += blockDim.x) {
+    const int c = u >> 2, q = u & 3;                  // staged cell (rows from r0), chunk
+    const int slot = (r0 - (y0 - 1)) * kGrid + c;     // stage row 0 is y0 - 1
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(base + slot * 64 + ((q ^ (c & 3)) << 4)),
+                 "l"(src + static_cast<size_t>(u) * 16)
+                 : "memory");
+  }
+  asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
   __syncthreads();
-  const size_t total = static_cast<size_t>(count) * kCells;
-  for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
-       i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-    const uint32_t net = static_cast<uint32_t>(i / kCells);
-    const int y = static_cast<int>((i / kGrid) % kGrid), x = static_cast<int>(i % kGrid);
-    const uint32_t d = dims[net];
-    const int cw = static_cast<int>(dims_w(d)), ch = static_cast<int>(dims_h(d));
+  const float bias = b6[0];
+#pragma unroll 1
+  for (int i = threadIdx.x; i < kHeadRows * kGrid; i += blockDim.x) {
+    const int y = y0 + i / kGrid, x = i % kGrid;
     float z = 0.f;
     if (x < cw && y < ch) {
-      z = b6[0];
+      z = bias;
+#pragma unroll 1
       for (int t = 0; t < 9; ++t) {
         const int sy = y + t / 3 - 1, sx = x + t % 3 - 1;
         if (sx < 0 || sy < 0 || sx >= cw || sy >= ch) continue;
-        const uint4* src = reinterpret_cast<const uint4*>(act + act_cell(net, sy, sx) * kCh);
+        const uint4* cell = reinterpret_cast<const uint4*>(hs + ((sy - (y0 - 1)) * kGrid + sx) * 64);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
           float v[8];
-          unpack8(__ldg(src + q), v);
+          unpack8(cell[q ^ (sx & 3)], v);
 #pragma unroll
           for (int k = 0; k < 8; ++k) z = fmaf(ws[t * kCh + q * 8 + k], v[k], z);
         }
       }
     }
-    logits[i] = z;
+    out[i] = z;
   }
 }
 
@@ -833,72 +1010,117 @@ __global__ void adam_kernel(float* __restrict__ params, const float* __restrict_
 
 // -------------------------- corridors from logits -------------------------
 
-// One block per net: coarse cells with logit > threshold, dilated by
-// `dilate` coarse cells (Chebyshev), plus both terminals, as the 128-word
-// corridor bitmap (bit cx % 32 of word 2 * cy + cx / 32).  A net whose window
-// holds more than max_cells cells (all layers; 0 = no limit) gets an empty
-// bitmap: no corridor, its whole window is searched at once.
-__global__ void corridor_kernel(const float* __restrict__ logits, const uint32_t* __restrict__ dims,
-                                const apgar_b200_lattice_net* __restrict__ nets, uint32_t count,
-                                float threshold, int dilate, uint64_t max_cells, int layers,
-                                uint32_t* __restrict__ bits) {
-  __shared__ uint8_t hot[kCells];
+// The corridor bitmap of each net: a coarse cell is on when it lies in the
+// window and is the start, the goal or within `dilate` cells (Chebyshev) of a
+// cell whose logit exceeds the threshold; row cy of the bitmap is words
+// 2 * cy (columns 0-31) and 2 * cy + 1.  Rows are 64-bit masks: the hot rows
+// come from warp ballots, the dilation is shifts and ORs of whole rows.  A net
+// whose window holds more than max_cells cells (all layers; 0 = no limit)
+// gets an empty bitmap: no corridor, its whole window is searched at once.
+__global__ void __launch_bounds__(128) corridor_kernel(const float* __restrict__ logits,
+                                                       const uint32_t* __restrict__ dims,
+                                                       const apgar_b200_lattice_net* __restrict__ nets,
+                                                       uint32_t count, float threshold, int dilate,
+                                                       uint64_t max_cells, int layers,
+                                                       uint32_t* __restrict__ bits) {
+  __shared__ uint64_t hot[kGrid], wide[kGrid];
   const uint32_t n = blockIdx.x;
   if (n >= count) return;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  uint32_t* out = bits + static_cast<size_t>(n) * 128;
   if (max_cells != 0 &&
       static_cast<uint64_t>(layers) * nets[n].win_w * nets[n].win_h > max_cells) {
-    for (int wd = threadIdx.x; wd < 128; wd += blockDim.x) bits[static_cast<size_t>(n) * 128 + wd] = 0u;
-    return;  // uniform: the whole block
+    out[tid] = 0u;  // 128 threads, 128 words
+    return;         // uniform: the whole block
   }
   const uint32_t d = dims[n];
   const int cw = static_cast<int>(dims_w(d)), ch = static_cast<int>(dims_h(d));
   const int s = static_cast<int>(d >> 16);
   const float* z = logits + static_cast<size_t>(n) * kCells;
-  for (int c = threadIdx.x; c < kCells; c += blockDim.x) {
-    const int y = c / kGrid, x = c % kGrid;
-    hot[c] = (x < cw && y < ch && z[c] > threshold) ? 1 : 0;
+  for (int y = warp; y < kGrid; y += 4) {
+    const bool lo = y < ch && lane < cw && z[y * kGrid + lane] > threshold;
+    const bool hi = y < ch && lane + 32 < cw && z[y * kGrid + 32 + lane] > threshold;
+    const uint32_t blo = __ballot_sync(0xFFFFFFFFu, lo), bhi = __ballot_sync(0xFFFFFFFFu, hi);
+    if (lane == 0) hot[y] = static_cast<uint64_t>(blo) | (static_cast<uint64_t>(bhi) << 32);
   }
   __syncthreads();
-  const apgar_b200_lattice_net net = nets[n];
-  const int sx = (static_cast<int>(net.start_x) - static_cast<int>(net.win_x0)) >> s;
-  const int sy = (static_cast<int>(net.start_y) - static_cast<int>(net.win_y0)) >> s;
-  const int gx = (static_cast<int>(net.goal_x) - static_cast<int>(net.win_x0)) >> s;
-  const int gy = (static_cast<int>(net.goal_y) - static_cast<int>(net.win_y0)) >> s;
-  // one warp per output word: 32 coarse cells of one row
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  for (int wd = warp; wd < 128; wd += blockDim.x / 32) {
-    const int y = wd / 2, x = (wd % 2) * 32 + lane;
-    bool on = false;
-    if (x < cw && y < ch) {
-      on = (x == sx && y == sy) || (x == gx && y == gy);
-      for (int dy = -dilate; dy <= dilate && !on; ++dy) {
-        const int yy = y + dy;
-        if (yy < 0 || yy >= ch) continue;
-        for (int dx = -dilate; dx <= dilate; ++dx) {
-          const int xx = x + dx;
-          if (xx >= 0 && xx < cw && hot[yy * kGrid + xx]) {
-            on = true;
-            break;
-          }
-        }
-      }
-    }
-    const uint32_t word = __ballot_sync(0xFFFFFFFFu, on);
-    if (lane == 0) bits[static_cast<size_t>(n) * 128 + wd] = word;
+  const int dl = min(dilate, kGrid - 1);  // beyond 63 every column is covered already
+  if (tid < kGrid) {
+    const uint64_t v = hot[tid];
+    uint64_t h = 0;
+    for (int dx = -dl; dx <= dl; ++dx) h |= dx >= 0 ? v >> dx : v << -dx;  // none when dilate < 0
+    wide[tid] = h;
   }
+  __syncthreads();
+  if (tid < kGrid) {
+    const int y = tid;
+    uint64_t o = 0;
+    for (int dy = -dl; dy <= dl; ++dy) {
+      const int yy = y + dy;
+      if (yy >= 0 && yy < kGrid) o |= wide[yy];  // hot rows ch .. 63 are zero
+    }
+    const apgar_b200_lattice_net net = nets[n];
+    const int sx = (static_cast<int>(net.start_x) - static_cast<int>(net.win_x0)) >> s;
+    const int sy = (static_cast<int>(net.start_y) - static_cast<int>(net.win_y0)) >> s;
+    const int gx = (static_cast<int>(net.goal_x) - static_cast<int>(net.win_x0)) >> s;
+    const int gy = (static_cast<int>(net.goal_y) - static_cast<int>(net.win_y0)) >> s;
+    if (y == sy && sx >= 0 && sx < kGrid) o |= 1ull << sx;
+    if (y == gy && gx >= 0 && gx < kGrid) o |= 1ull << gx;
+    o &= y < ch ? (cw >= kGrid ? ~0ull : (1ull << cw) - 1ull) : 0ull;
+    out[2 * y] = static_cast<uint32_t>(o);
+    out[2 * y + 1] = static_cast<uint32_t>(o >> 32);
+  }
+}
+
+// The driver's tensor-map encoder, resolved once through the runtime (no
+// link against the driver library).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      f = nullptr;
+    }
+    return reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+  }();
+  return fn;
+}
+
+// The conv input [count][66][64][CIN] bf16 as {8 channels, CIN / 8 chunks,
+// cells}: a box {8, 1, 256} is one 16-byte chunk of 256 consecutive cells.
+template <int CIN>
+cudaError_t conv_input_map(const __nv_bfloat16* x, uint32_t count, CUtensorMap* map) {
+  const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+  if (encode == nullptr) return cudaErrorNotSupported;
+  if ((reinterpret_cast<uintptr_t>(x) & 15u) != 0) return cudaErrorInvalidValue;
+  const cuuint64_t dims[3] = {8, CIN / 8, static_cast<cuuint64_t>(count) * kPadRows * kGrid};
+  const cuuint64_t strides[2] = {16, CIN * 2};  // bytes, dims 1 and 2
+  const cuuint32_t box[3] = {8, 1, 4 * kGrid};
+  const cuuint32_t elem[3] = {1, 1, 1};
+  const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<__nv_bfloat16*>(x), dims,
+                            strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
 template <int CIN, int EPI>
 cudaError_t launch_conv(const ConvArgs& a, int sm_count, cudaStream_t stream) {
-  const int bytes = ConvSmem<CIN>::kBytes;
-  cudaError_t e = cudaFuncSetAttribute(conv3x3_tc_kernel<CIN, EPI>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if (e != cudaSuccess) return e;
+  using S = ConvSmem<CIN>;
   const uint32_t items = a.count * (kGrid / 2);
-  // ~35 KB of shared memory and 32 TMEM columns per CTA: four per SM
-  const uint32_t grid = min(items, static_cast<uint32_t>(max(sm_count, 1) * 4));
-  if (grid == 0) return cudaSuccess;
-  conv3x3_tc_kernel<CIN, EPI><<<grid, 128, bytes, stream>>>(a);
+  if (items == 0) return cudaSuccess;
+  // planes are addressed by 32-bit cell coordinates
+  if (static_cast<uint64_t>(a.count) * kPadRows * kGrid > 0x7FFFFFFFull) return cudaErrorInvalidValue;
+  CUtensorMap map;
+  cudaError_t e = conv_input_map<CIN>(a.x, a.count, &map);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(conv3x3_tc_kernel<CIN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           S::kBytes);
+  if (e != cudaSuccess) return e;
+  // ~71 KB of shared memory (32 channels) and 64 TMEM columns per CTA: three
+  // per SM (three CTAs' pipelines per SM measured faster than two deeper ones)
+  const uint32_t grid = min(items, static_cast<uint32_t>(max(sm_count, 1) * kConvPerSm));
+  conv3x3_tc_kernel<CIN, EPI><<<grid, kConvThreads, S::kBytes, stream>>>(map, a);
   return cudaGetLastError();
 }
 
@@ -948,6 +1170,7 @@ cudaError_t launch_forward(const float* params, const void* operands, const void
                            uint32_t* error, int sm_count, cudaStream_t stream) {
   constexpr ParamOffsets P = param_offsets();
   constexpr OperandOffsets O = operand_offsets();
+  if (count == 0) return cudaSuccess;
   const auto* ops = static_cast<const __nv_bfloat16*>(operands);
   for (int l = 0; l < 5; ++l) {
     ConvArgs a{};
@@ -962,11 +1185,8 @@ cudaError_t launch_forward(const float* params, const void* operands, const void
                                  : launch_conv<kCh, kEpiRelu>(a, sm_count, stream);
     if (e != cudaSuccess) return e;
   }
-  const uint32_t blocks = min(static_cast<uint32_t>(max(sm_count, 1) * 8),
-                              static_cast<uint32_t>((static_cast<size_t>(count) * kCells + 255) / 256));
-  if (blocks == 0) return cudaSuccess;
-  head_forward_kernel<<<blocks, 256, 0, stream>>>(static_cast<const __nv_bfloat16*>(acts[4]),
-                                                  params + P.w6, params + P.b6, dims, count, logits);
+  head_forward_kernel<<<count * kHeadBands, 256, kHeadSmem, stream>>>(
+      static_cast<const __nv_bfloat16*>(acts[4]), params + P.w6, params + P.b6, dims, count, logits);
   return cudaGetLastError();
 }
 
@@ -1037,7 +1257,7 @@ cudaError_t launch_corridors(const float* logits, const uint32_t* dims,
                              int dilate, uint64_t max_cells, int layers, uint32_t* bits,
                              cudaStream_t stream) {
   if (count == 0) return cudaSuccess;
-  corridor_kernel<<<count, 256, 0, stream>>>(logits, dims, nets, count, threshold, dilate, max_cells,
+  corridor_kernel<<<count, 128, 0, stream>>>(logits, dims, nets, count, threshold, dilate, max_cells,
                                              layers, bits);
   return cudaGetLastError();
 }

@@ -97,7 +97,7 @@ class CorridorNet:
     def activations(self, count: int, distinct: bool):
         t = self.torch
         n = 5 if distinct else 2
-        bufs = [t.empty((count, PADDED_ROWS, GRID, CHANNELS), dtype=t.bfloat16, device="cuda")
+        bufs = [t.zeros((count, PADDED_ROWS, GRID, CHANNELS), dtype=t.bfloat16, device="cuda")
                 for _ in range(n)]
         return bufs if distinct else [bufs[i % 2] for i in range(5)]
 
@@ -148,15 +148,16 @@ class CorridorNet:
 
 
 def rasters(plan, cell_costs=None, stream: int = 0, out=None):
-    """(rasters bf16 [n][64][64][16], dims uint32 [n]) of every net of a plan
-    (into `out` = (rasters, dims) when given)."""
+    """(rasters bf16 [n][66][64][16], dims uint32 [n]) of every net of a plan
+    (into `out` = (rasters, dims) when given).  Only the pad row and grid rows
+    0 .. ch of each net are written; a buffer allocated here starts zeroed."""
     import torch
 
     n = len(plan.nets)
     if out is not None:
         r, d = out
     else:
-        r = torch.empty((n, PADDED_ROWS, GRID, RASTER_CHANNELS), dtype=torch.bfloat16, device="cuda")
+        r = torch.zeros((n, PADDED_ROWS, GRID, RASTER_CHANNELS), dtype=torch.bfloat16, device="cuda")
         d = torch.empty(n, dtype=torch.uint32, device="cuda")
     costs = None if cell_costs is None else _ptr(cell_costs)
     _check(lib().apgar_b200_corridor_rasters(plan.handle, costs, _ptr(r), _ptr(d), ctypes.c_void_p(stream)))
@@ -212,7 +213,7 @@ class LearnedRouter:
         self.net = net if net is not None else CorridorNet.load()
         self.policy = policy if policy is not None else load_policy()
         n = len(plan.nets)
-        self.rasters = torch.empty((n, PADDED_ROWS, GRID, RASTER_CHANNELS), dtype=torch.bfloat16,
+        self.rasters = torch.zeros((n, PADDED_ROWS, GRID, RASTER_CHANNELS), dtype=torch.bfloat16,
                                    device="cuda")
         self.dims = torch.empty(n, dtype=torch.uint32, device="cuda")
         self.acts = self.net.activations(n, distinct=False)

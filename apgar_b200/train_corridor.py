@@ -120,7 +120,7 @@ def priced_dataset(samples: int, rounds: int = 6, size: int = 2048, first_seed: 
         for r in range(rounds):
             if got >= samples:
                 break
-            ras = torch.empty((n, learned.PADDED_ROWS, learned.GRID, learned.RASTER_CHANNELS),
+            ras = torch.zeros((n, learned.PADDED_ROWS, learned.GRID, learned.RASTER_CHANNELS),
                               dtype=torch.bfloat16, device="cuda")
             dim = torch.empty(n, dtype=torch.uint32, device="cuda")
             # the snapshot the round's search is priced by (round 0: none)

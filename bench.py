@@ -84,6 +84,12 @@ def parse_args():
                          "all-reduce of usage) even on one GPU; it is the form used for N > 1")
     ap.add_argument("--rounds", type=int, default=None,
                     help="negotiated rounds (default 10, or 20 for the full workload)")
+    ap.add_argument("--neg-sample", type=int, default=2048,
+                    help="negotiated workloads: segments of the round-0 comparison (frontier, "
+                         "sweep, oracle bytes and CPU baseline)")
+    ap.add_argument("--learned-rounds", action="store_true",
+                    help="negotiated workloads: also run the negotiation with learned corridor "
+                         "proposals in every priced round and report it beside the line")
     ap.add_argument("--full-ripup", action="store_true",
                     help="negotiated: reroute every net each round (default: only nets "
                          "crossing overused cells after round 0)")
@@ -244,6 +250,71 @@ def cpu_baseline(lat, nets, sample: int):
                       f"(cpu_astar.cc:323-638) extended with vias, {threads} threads, {dt:.2f} s"}, costs
 
 
+def round0_sample(args, lat, segs, dev):
+    """Round 0 of a negotiation (zero prices) on a bounded sample of its
+    segments, untimed by the negotiation itself: the frontier (the search every
+    round runs) against the plain sweep on the same segments, the frontier
+    launch's roofline from the oracle's expansions, and the CPU A* port on all
+    host threads over the same sample (one oracle run gives both)."""
+    import torch
+
+    import apgar_b200
+    import oracle
+
+    sample = np.ascontiguousarray(segs[: min(args.neg_sample, len(segs))])
+    stream = torch.cuda.current_stream()
+
+    def timed(plan, reps=3):
+        for _ in range(3):
+            plan.execute(stream.cuda_stream)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            plan.execute(stream.cuda_stream)
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    fp = dev.plan(sample, generator="frontier")
+    f_ms = timed(fp)
+    fres, _ = fp.readback(want_paths=False)
+    fp.close()
+    sp = dev.plan(sample, generator="sweep")
+    s_ms = timed(sp)
+    sres, _ = sp.readback(want_paths=False)
+    sp.close()
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    cpu_costs, _, cells = oracle.astar_batch(lat, sample, threads=threads, counts=True)
+    cpu_s = time.perf_counter() - t0
+    ok = fres["completion"] != apgar_b200.COMPLETION_REJECTED
+    peak, peak_kind = load_peaks()
+    fbytes = cells.astype(np.float64).sum() * EXPANSION_BYTES + 4.0 * fres["path_len"].astype(np.float64).sum()
+    achieved = fbytes / (f_ms / 1000.0) / 1e9
+    n = len(sample)
+    return {
+        "round0_sample": {
+            "segments": n, "frontier_ms": f_ms, "sweep_ms": s_ms, "frontier_over_sweep": s_ms / f_ms,
+            "frontier_routes_per_s": n / (f_ms / 1000.0), "sweep_routes_per_s": n / (s_ms / 1000.0),
+            "same_costs": bool(np.array_equal(fres["cost"], sres["cost"])),
+        },
+        "roofline": {
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+            "kernel": f"lattice_frontier_kernel, round 0 (zero prices) of the first {n} segments",
+            "bytes_alg_per_launch": fbytes,
+            "bytes_alg_source": "oracle A* expanded cells x 92 B + 4 B per path cell",
+        },
+        "cpu_baseline": {
+            "value": n / cpu_s, "unit": "routes/s", "cores": threads, "kind": "port",
+            "sample": f"round 0 of the first {n} segments, A* port of RouteWithCpuAStar "
+                      f"(cpu_astar.cc:323-638) extended with vias, {threads} threads, {cpu_s:.2f} s",
+            "costs_match_gpu": bool(np.array_equal(cpu_costs[ok], fres["cost"][ok])),
+        },
+    }
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -357,9 +428,54 @@ def run_negotiated(args, rank, world, local):
     }
     neg.close()
     plan.close()
+    if args.learned_rounds:
+        line["learned_rounds"] = learned_negotiation(args, segs, dev, res, ms)
+    line.update(round0_sample(args, lat, segs, dev))
     dev.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+# activations of the corridor CNN take ~0.6 MB per segment (two ping-pong
+# buffers and the rasters): larger negotiations would not fit beside the plan
+LEARNED_ROUNDS_MAX_SEGMENTS = 65536
+
+
+def learned_negotiation(args, segs, dev, plain_results, plain_ms):
+    """The same negotiation with a learned corridor proposal before every
+    priced round (round 0 searches without corridors), one warm-up and one
+    timed run; its routes must equal the plain negotiation's."""
+    import torch
+
+    from apgar_b200 import learned, negotiate, prices
+
+    if len(segs) > LEARNED_ROUNDS_MAX_SEGMENTS:
+        return {"skipped": f"{len(segs)} segments: the CNN's activations would not fit beside the "
+                           f"plan (limit {LEARNED_ROUNDS_MAX_SEGMENTS})"}
+    partial = not args.full_ripup
+    plan = dev.plan(segs, generator="frontier")
+    neg = negotiate.Negotiation(plan, prices.policy(capacity=1))
+    router = learned.LearnedRouter(plan)
+    stream = torch.cuda.current_stream()
+    neg.run_learned(args.rounds, router, stream.cuda_stream, partial)
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    neg.run_learned(args.rounds, router, stream.cuda_stream, partial)
+    b.record(stream)
+    torch.cuda.synchronize()
+    l_ms = a.elapsed_time(b)
+    router.net.check_error()
+    res, _ = plan.readback(want_paths=False)
+    status = plan.corridor_status()
+    neg.close()
+    plan.close()
+    return {"value": len(segs) * args.rounds / (l_ms / 1000.0), "unit": "routes/s",
+            "ms_per_negotiation": l_ms, "plain_over_learned": l_ms / plain_ms,
+            "same_results": bool(np.array_equal(res["cost"], plain_results["cost"]) and
+                                 np.array_equal(res["completion"], plain_results["completion"])),
+            "last_round_certified": float((status == 1).mean()),
+            "last_round_fallback": float((status >= 2).mean())}
 
 
 def run_negotiated_ranked(args, rank, world, local):

@@ -676,8 +676,12 @@ APGAR_B200_API int apgar_b200_compile_legal_edges(const apgar_b200_edge_rules* r
  * 5 inside the window, 6-9 coarse offsets to start and goal / 32, 10 distance
  * to the start-goal segment / 8 (capped at 4), 11-15 zero.
  * Tensors are device memory: rasters bf16 [count][66][64][16]; activations
- * bf16 [count][66][64][32] (grid row y stored at row y + 1, rows 0 and 65 and
- * the cells outside each net's window zero, written by the producers);
+ * bf16 [count][66][64][32] (grid row y stored at row y + 1).  The producers
+ * write the rows that in-window outputs read, with the cells outside each
+ * net's window as zeros: the pad row above the grid and grid rows 0 .. ch
+ * (coarse height ch; row ch is all zeros).  Rows below are left as they are:
+ * they reach only cells outside the window, whose outputs are written as
+ * zeros, and the gradients read inputs inside the window only;
  * logits and dlogit f32 [count][64][64]; labels u8
  * [count][64][64]; dims u32 [count] (coarse width | height << 8 | scale << 16).
  * params f32 [apgar_b200_cnn_param_count()]: per layer l w[32][9][cin_l] then
