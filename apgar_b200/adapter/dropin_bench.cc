@@ -14,6 +14,7 @@
 //             queries and policies, the search, D2H of compact paths and the
 //             reference's host validation, reconstruction and sealing (the
 //             view upload is prepared once and excluded, as there);
+//             gpu_kernel: the batch telemetry's kernel time, the part of gpu spent on the device;
 //  * cpu_par: the reference's RouteWithCpuAStar over the k queries on all
 //             host threads (one query per task);
 //  * cpu_ser: the same on one thread.
@@ -160,7 +161,7 @@ int main() {
         queries.push_back(gpu::PlanarCandidateBatchQuery{.query_id = i + 1, .input_ordinal = i, .request = req});
       }
       const std::vector<std::uint64_t> want = cpu_batch(c, pols, k, threads);
-      std::vector<double> g, cp, cs;
+      std::vector<double> g, gk, cp, cs;
       std::uint64_t sealed = 0;
       for (int rep = 0; rep < kRepetitions + 1; ++rep) {
         gpu::PlanarCandidateBatchPolicy policy;
@@ -191,6 +192,9 @@ int main() {
           continue;
         }
         g.push_back(t1 - t0);
+        if (const auto* batch = std::get_if<gpu::PlanarCandidateBatch>(&result)) {
+          gk.push_back(batch->telemetry.kernel_milliseconds);
+        }
         cp.push_back(t3 - t2);
         if (rep <= 3) {  // the serial CPU form is slow: three repetitions
           const double t4 = now_ms();
@@ -198,9 +202,9 @@ int main() {
           cs.push_back(now_ms() - t4);
         }
       }
-      std::printf("%s{\"k\": %u, \"gpu_ms\": %.4f, \"cpu_par_ms\": %.4f, \"cpu_ser_ms\": %.4f, "
-                  "\"sealed\": %llu}",
-                  first_k ? "" : ", ", k, median(g), median(cp), median(cs),
+      std::printf("%s{\"k\": %u, \"gpu_ms\": %.4f, \"gpu_kernel_ms\": %.4f, \"cpu_par_ms\": %.4f, "
+                  "\"cpu_ser_ms\": %.4f, \"sealed\": %llu}",
+                  first_k ? "" : ", ", k, median(g), gk.empty() ? 0.0 : median(gk), median(cp), median(cs),
                   static_cast<unsigned long long>(sealed));
       first_k = false;
     }

@@ -225,12 +225,24 @@ class LearnedRouter:
         """Rasters -> CNN -> corridors.  ``cell_costs``: device address (int)
         or CUDA uint32 tensor of per-cell prices for the congestion channel
         (a negotiation's snapshot), or None."""
+        self.rasterize(stream, cell_costs)
+        self.infer(stream)
+        self.extract(stream)
+
+    def rasterize(self, stream: int = 0, cell_costs=None) -> None:
+        """The proposal's first stage: every net's coarse raster and dims."""
         if cell_costs is not None and not isinstance(cell_costs, int):
             cell_costs = cell_costs.data_ptr()
         _check(lib().apgar_b200_corridor_rasters(
             self.plan.handle, ctypes.c_void_p(cell_costs) if cell_costs else None,
             _ptr(self.rasters), _ptr(self.dims), ctypes.c_void_p(stream)))
+
+    def infer(self, stream: int = 0) -> None:
+        """The second stage: the CNN's logits from the rasters."""
         self.net.forward(self.rasters, self.dims, acts=self.acts, logits=self.logits, stream=stream)
+
+    def extract(self, stream: int = 0) -> None:
+        """The third stage: the corridor bitmaps from the logits."""
         corridors(self.plan, self.logits, self.dims, threshold=float(self.policy["threshold"]),
                   dilate=int(self.policy["dilate"]), out=self.bits, stream=stream,
                   max_window_cells=int(self.policy.get("max_window_cells", 0)))

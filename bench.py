@@ -612,8 +612,10 @@ def run_dropin(args, rank):
         tot["par"] += p
         tot["ser"] += s
         tot["best"] += best
+        kern = sum(r.get("gpu_kernel_ms", 0.0) for r in rows)
         per_k.append({"k": k, "gpu_qps": q / (g / 1e3), "cpu_parallel_qps": q / (p / 1e3),
                       "cpu_serial_qps": q / (s / 1e3), "gpu_over_faster_cpu": best / g,
+                      "gpu_ms_per_batch": g / len(rows), "gpu_kernel_ms_per_batch": kern / len(rows),
                       "cases_gpu_slower": [c["name"] for c, r in zip(data["cases"], rows)
                                            if r["gpu_ms"] > min(r["cpu_par_ms"], r["cpu_ser_ms"])]})
     value = tot["q"] / (tot["gpu"] / 1e3)
@@ -759,6 +761,20 @@ def main():
         l_mid.record(stream)
         barrier()
         p_ms = max_over_ranks(l_start.elapsed_time(l_mid))
+        # and stage by stage
+        stage_ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+        stage_ms = [0.0, 0.0, 0.0]
+        for _ in range(args.steps):
+            stage_ev[0].record(stream)
+            router.rasterize(stream.cuda_stream)
+            stage_ev[1].record(stream)
+            router.infer(stream.cuda_stream)
+            stage_ev[2].record(stream)
+            router.extract(stream.cuda_stream)
+            stage_ev[3].record(stream)
+            stream.synchronize()
+            for i in range(3):
+                stage_ms[i] += stage_ev[i].elapsed_time(stage_ev[i + 1]) / args.steps
         router.net.check_error()
         l_res, _ = lplan.readback(want_paths=False)
         status = lplan.corridor_status()
@@ -766,6 +782,7 @@ def main():
         learned_form = {
             "value": l_cert * args.steps / (l_ms / 1000.0), "unit": UNIT,
             "ms_per_step": l_ms / args.steps, "proposal_ms_per_step": p_ms / args.steps,
+            "proposal_stage_ms": {"rasters": stage_ms[0], "cnn": stage_ms[1], "corridors": stage_ms[2]},
             "corridor_certified": float((status == 1).mean()),
             "fallback_exit": float((status == 2).mean()),
             "fallback_unreached": float((status == 3).mean()),
