@@ -93,6 +93,31 @@ struct Workspace {
   }
 };
 
+// Page-locked host staging, grown on demand and kept with its view: a batch's
+// inputs go up and its results come back through it in one asynchronous copy
+// per buffer, with a single synchronisation per direction.
+struct PinnedStage {
+  uint8_t* p = nullptr;
+  size_t cap = 0;
+  ~PinnedStage() {
+    if (p != nullptr) cudaFreeHost(p);
+  }
+  cudaError_t ensure(size_t n) {
+    if (n <= cap) return cudaSuccess;
+    if (p != nullptr) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+    void* q = nullptr;
+    const cudaError_t e = cudaHostAlloc(&q, n, cudaHostAllocDefault);
+    if (e != cudaSuccess) return e;
+    p = static_cast<uint8_t*>(q);
+    cap = n;
+    return cudaSuccess;
+  }
+};
+
+inline size_t round16(size_t n) { return (n + 15) & ~static_cast<size_t>(15); }
+
 struct ViewObject {
   int device = -1;
   int sm_count = 0;
@@ -104,6 +129,7 @@ struct ViewObject {
   DeviceBuffer<apgar_b200_node_v1> nodes_dev;  // full records, for path validation
   Lease lease;
   Workspace ws;
+  PinnedStage host_stage;
   uint32_t* cancel_host = nullptr;
   uint32_t* cancel_dev = nullptr;
   ~ViewObject() {
@@ -364,11 +390,18 @@ int run_batch(ViewObject* v, const apgar_b200_batch_request& req,
     APGAR_B200_CUDA("cudaMalloc(pred owners)", w.pred_owners.ensure(Q * S));
   }
   APGAR_B200_CUDA("cudaMalloc(counters)", w.counters.ensure(2));
-  APGAR_B200_CUDA("cudaMemcpy(queries)",
-                  cudaMemcpy(w.queries.get(), queries, Q * sizeof(*queries), cudaMemcpyHostToDevice));
-  if (edge_count > 0) {
-    APGAR_B200_CUDA("cudaMemcpy(policy)", cudaMemcpy(w.policy.get(), edges, edge_count * sizeof(*edges),
-                                                     cudaMemcpyHostToDevice));
+  // queries and policy edges through the pinned stage, copied in stream order
+  // before the search (the view's lease keeps the stage to this batch)
+  const size_t qbytes = Q * sizeof(*queries), ebytes = edge_count * sizeof(*edges);
+  APGAR_B200_CUDA("cudaHostAlloc(staging)", v->host_stage.ensure(round16(qbytes) + ebytes));
+  std::memcpy(v->host_stage.p, queries, qbytes);
+  if (ebytes > 0) std::memcpy(v->host_stage.p + round16(qbytes), edges, ebytes);
+  APGAR_B200_CUDA("cudaMemcpyAsync(queries)",
+                  cudaMemcpyAsync(w.queries.get(), v->host_stage.p, qbytes, cudaMemcpyHostToDevice, nullptr));
+  if (ebytes > 0) {
+    APGAR_B200_CUDA("cudaMemcpyAsync(policy)",
+                    cudaMemcpyAsync(w.policy.get(), v->host_stage.p + round16(qbytes), ebytes,
+                                    cudaMemcpyHostToDevice, nullptr));
   }
   if (v->cancel_host == nullptr) {
     void* h = nullptr;
@@ -556,22 +589,38 @@ extern "C" int apgar_b200_readback_batch(void* pending, apgar_b200_batch_result_
   auto* p = static_cast<PendingBatch*>(pending);
   if (int rc = check_device(p->view->device); rc != APGAR_B200_OK) return rc;
   Workspace& w = p->view->ws;
+  PinnedStage& stage = p->view->host_stage;
   const uint64_t Q = p->query_count;
-  APGAR_B200_CUDA("cudaMemcpy(results)", cudaMemcpy(results, w.results.get(), Q * sizeof(*results),
-                                                    cudaMemcpyDeviceToHost));
-  uint64_t bytes = Q * sizeof(*results);
+  // results, the path-state total and the compact records in one round trip
+  const size_t rbytes = Q * sizeof(*results), cbytes = Q * sizeof(*compact_paths);
+  const size_t off_total = round16(rbytes), off_compact = off_total + 16;
+  APGAR_B200_CUDA("cudaHostAlloc(staging)", stage.ensure(off_compact + cbytes));
+  APGAR_B200_CUDA("cudaMemcpyAsync(results)",
+                  cudaMemcpyAsync(stage.p, w.results.get(), rbytes, cudaMemcpyDeviceToHost, nullptr));
+  const bool compact = !p->workspace_mode;
+  if (compact) {
+    APGAR_B200_CUDA("cudaMemcpyAsync(path total)",
+                    cudaMemcpyAsync(stage.p + off_total, w.counters.get(), sizeof(unsigned long long),
+                                    cudaMemcpyDeviceToHost, nullptr));
+    if (compact_paths != nullptr) {
+      APGAR_B200_CUDA("cudaMemcpyAsync(compact paths)",
+                      cudaMemcpyAsync(stage.p + off_compact, w.compact.get(), cbytes, cudaMemcpyDeviceToHost,
+                                      nullptr));
+    }
+  }
+  APGAR_B200_CUDA("cudaStreamSynchronize(readback)", cudaStreamSynchronize(nullptr));
+  std::memcpy(results, stage.p, rbytes);
+  uint64_t bytes = rbytes;
   uint32_t max_rounds = 0;
   for (uint64_t i = 0; i < Q; ++i) max_rounds = std::max(max_rounds, results[i].rounds);
   uint64_t total = 0;
-  if (!p->workspace_mode) {
+  if (compact) {
     unsigned long long t = 0;
-    APGAR_B200_CUDA("cudaMemcpy(path total)", cudaMemcpy(&t, w.counters.get(), sizeof(t), cudaMemcpyDeviceToHost));
+    std::memcpy(&t, stage.p + off_total, sizeof(t));
     total = t;
     if (compact_paths != nullptr) {
-      APGAR_B200_CUDA("cudaMemcpy(compact paths)",
-                      cudaMemcpy(compact_paths, w.compact.get(), Q * sizeof(*compact_paths),
-                                 cudaMemcpyDeviceToHost));
-      bytes += Q * sizeof(*compact_paths);
+      std::memcpy(compact_paths, stage.p + off_compact, cbytes);
+      bytes += cbytes;
     }
     if (path_states != nullptr && total > 0) {
       if (total > path_capacity) {
