@@ -420,7 +420,8 @@ struct ConvSmem {
   static constexpr int kLead = 128;                     // plane bytes before cell 0
   static constexpr int kPlane = kLead + 4 * kGrid * 16 + 128;
   static constexpr int kBytesA = (CIN / 8) * kPlane;
-  static constexpr int kTx = (CIN / 8) * 4 * kGrid * 16;  // TMA bytes per stage
+  static constexpr int kTx = (CIN / 8) * 4 * kGrid * 16;  // TMA bytes per stage, 64-cell rows
+  static constexpr int kTxNarrow = (CIN / 8) * 6 * (kGrid / 2) * 16;  // 32-cell rows
   static constexpr int kStages = kConvStages;
   static constexpr int kAccs = kConvAccs;               // 32-column accumulators
   static constexpr int kOffB = kStages * kBytesA;
@@ -449,20 +450,54 @@ __device__ __forceinline__ void tma_load_plane(uint32_t dst, const CUtensorMap* 
       : "memory");
 }
 
-// The next tile of this CTA's strided item sequence after `item` that has
-// rows to write (y0 <= ch), or `items` when there is none.
+// Rows y0 - 1 .. y0 + 4, columns 0 .. 31 of one chunk: box {8, 1, 32, 6} at
+// {0, chunk, 0, padded row} of the narrow tensor map.
+__device__ __forceinline__ void tma_load_plane_narrow(uint32_t dst, const CUtensorMap* map, int chunk, int row,
+                                                      uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5}], [%6];" ::"r"(dst),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(chunk), "r"(0), "r"(row), "r"(bar)
+      : "memory");
+}
+
+// Tile `item` of the conv (net = item / 32, j = item % 32).  A net whose
+// window is at most 31 coarse columns wide takes tiles of four 32-cell rows
+// (y0 = 4j, j < 16): its column 31 is outside the window and zero, so the
+// shifted-run operands work with a 32-cell pitch, and the MMA work on columns
+// 32 .. 63 is skipped.  A wider net takes tiles of two 64-cell rows
+// (y0 = 2j).  A tile exists when y0 <= ch.
+struct ConvTile {
+  uint32_t net;
+  int y0;
+  int pitch;  // cells per tile row: 32 or 64
+};
+__device__ __forceinline__ bool conv_tile(const uint32_t* dims, uint32_t item, ConvTile& t) {
+  t.net = item / (kGrid / 2);
+  const int j = static_cast<int>(item % (kGrid / 2));
+  const uint32_t d = __ldg(dims + t.net);
+  const bool narrow = static_cast<int>(dims_w(d)) < kGrid / 2;
+  t.pitch = narrow ? kGrid / 2 : kGrid;
+  t.y0 = narrow ? 4 * j : 2 * j;
+  return (!narrow || j < kGrid / 4) && t.y0 <= static_cast<int>(dims_h(d));
+}
+
+// The next tile of this CTA's strided item sequence from `item` on, or
+// `items` when there is none.
 __device__ __forceinline__ uint32_t next_conv_item(const uint32_t* dims, uint32_t item, uint32_t items) {
+  ConvTile t;
   for (; item < items; item += gridDim.x) {
-    const uint32_t d = __ldg(dims + item / (kGrid / 2));
-    if (static_cast<int>(item % (kGrid / 2)) * 2 <= static_cast<int>(dims_h(d))) return item;
+    if (conv_tile(dims, item, t)) return item;
   }
   return items;
 }
 
 // out[cell][co] = epilogue(sum_{tap, ci} x[cell + tap][ci] * w[co][tap][ci]).
-// `xmap`: the input as {8 channels, CIN / 8 chunks, count * 66 * 64 cells}.
+// `xmap`: the input as {8 channels, CIN / 8 chunks, count * 66 * 64 cells};
+// `nmap`: the same as {8 channels, CIN / 8 chunks, 64 columns, count * 66 rows}.
 template <int CIN, int EPI>
 __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const __grid_constant__ CUtensorMap xmap,
+                                                                  const __grid_constant__ CUtensorMap nmap,
                                                                   ConvArgs a) {
   using S = ConvSmem<CIN>;
   constexpr int kSt = S::kStages, kAc = S::kAccs;
@@ -531,13 +566,19 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const __grid_c
            item = next_conv_item(a.dims, item + gridDim.x, items), ++k) {
         const int st = static_cast<int>(k % kSt);
         if (*abort_v || !wait(empty(st), ((k / kSt) & 1u) ^ 1u)) break;
-        const uint32_t net = item / (kGrid / 2);
-        const int y0 = static_cast<int>(item % (kGrid / 2)) * 2;
-        const int cell = static_cast<int>((static_cast<size_t>(net) * kPadRows + y0) * kGrid);  // row y0 - 1
+        ConvTile tile;
+        conv_tile(a.dims, item, tile);
+        const int row = static_cast<int>(tile.net * kPadRows + tile.y0);  // padded index of row y0 - 1
         const uint32_t dst = smem_addr(smem + st * S::kBytesA) + S::kLead;
-        bar_expect_tx(full(st), S::kTx);
+        if (tile.pitch == kGrid) {
+          bar_expect_tx(full(st), S::kTx);
 #pragma unroll
-        for (int j = 0; j < CIN / 8; ++j) tma_load_plane(dst + j * S::kPlane, &xmap, j, cell, full(st));
+          for (int j = 0; j < CIN / 8; ++j) tma_load_plane(dst + j * S::kPlane, &xmap, j, row * kGrid, full(st));
+        } else {
+          bar_expect_tx(full(st), S::kTxNarrow);
+#pragma unroll
+          for (int j = 0; j < CIN / 8; ++j) tma_load_plane_narrow(dst + j * S::kPlane, &nmap, j, row, full(st));
+        }
       }
       loaded = k;
     }
@@ -554,11 +595,13 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const __grid_c
         ++consumed;
         if (!wait(accempty(q), ((k / kAc) & 1u) ^ 1u)) break;
         fence_after_sync();
+        ConvTile tile;
+        conv_tile(a.dims, item, tile);
         const uint32_t a0 = smem_addr(smem + st * S::kBytesA) + S::kLead;
         const uint32_t acc = tmem + static_cast<uint32_t>(q * 32);
 #pragma unroll
         for (int t = 0; t < 9; ++t) {
-          const int off = (t / 3) * kGrid + (t % 3 - 1);  // staged cell of output 0
+          const int off = (t / 3) * tile.pitch + (t % 3 - 1);  // staged cell of output 0
 #pragma unroll
           for (int jj = 0; jj < CIN / 16; ++jj) {
             const int kk = t * (CIN / 16) + jj;
@@ -587,12 +630,14 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const __grid_c
       tmem_load32(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(q * 32), o);
       fence_before_sync();
       bar_arrive(accempty(q));
-      const uint32_t net = item / (kGrid / 2);
-      const int y0 = static_cast<int>(item % (kGrid / 2)) * 2;
+      ConvTile tile;
+      conv_tile(a.dims, item, tile);
+      const uint32_t net = tile.net;
+      const int y0 = tile.y0;
       const uint32_t d = __ldg(a.dims + net);
       const int cw = static_cast<int>(dims_w(d)), ch = static_cast<int>(dims_h(d));
       const int m = warp * 32 + lane;
-      const int py = y0 + m / kGrid, px = m % kGrid;
+      const int py = y0 + m / tile.pitch, px = m % tile.pitch;
       const size_t cell = act_cell(net, py, px);
       // cells outside the window are written as zeros (the layout's invariant)
       if (px < cw && py < ch) {
@@ -623,12 +668,23 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const __grid_c
         uint4* dst = reinterpret_cast<uint4*>(a.y + cell * kCh);
 #pragma unroll
         for (int qq = 0; qq < 4; ++qq) dst[qq] = pack8(o + qq * 8);
+        if (tile.pitch < kGrid) {
+          // a narrow tile's columns 32 .. 63 lie outside the window: zeros
+          uint4* far = reinterpret_cast<uint4*>(a.y + act_cell(net, py, px + kGrid / 2) * kCh);
+#pragma unroll
+          for (int qq = 0; qq < 4; ++qq) far[qq] = make_uint4(0u, 0u, 0u, 0u);
+        }
       }
-      if (y0 == 0 && m < kGrid) {
+      if (y0 == 0 && m < tile.pitch) {
         // the zero pad row above the grid
         uint4* pad = reinterpret_cast<uint4*>(a.y + act_cell(net, -1, m) * kCh);
 #pragma unroll
         for (int qq = 0; qq < 4; ++qq) pad[qq] = make_uint4(0u, 0u, 0u, 0u);
+        if (tile.pitch < kGrid) {
+          uint4* far = reinterpret_cast<uint4*>(a.y + act_cell(net, -1, m + kGrid / 2) * kCh);
+#pragma unroll
+          for (int qq = 0; qq < 4; ++qq) far[qq] = make_uint4(0u, 0u, 0u, 0u);
+        }
       }
     }
   }
@@ -1090,17 +1146,26 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 // The conv input [count][66][64][CIN] bf16 as {8 channels, CIN / 8 chunks,
 // cells}: a box {8, 1, 256} is one 16-byte chunk of 256 consecutive cells.
 template <int CIN>
-cudaError_t conv_input_map(const __nv_bfloat16* x, uint32_t count, CUtensorMap* map) {
+cudaError_t conv_input_map(const __nv_bfloat16* x, uint32_t count, CUtensorMap* map, CUtensorMap* narrow) {
   const PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
   if (encode == nullptr) return cudaErrorNotSupported;
   if ((reinterpret_cast<uintptr_t>(x) & 15u) != 0) return cudaErrorInvalidValue;
+  const cuuint32_t elem[4] = {1, 1, 1, 1};
+  // wide tiles: four 64-cell rows as 256 consecutive cells
   const cuuint64_t dims[3] = {8, CIN / 8, static_cast<cuuint64_t>(count) * kPadRows * kGrid};
   const cuuint64_t strides[2] = {16, CIN * 2};  // bytes, dims 1 and 2
   const cuuint32_t box[3] = {8, 1, 4 * kGrid};
-  const cuuint32_t elem[3] = {1, 1, 1};
-  const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<__nv_bfloat16*>(x), dims,
-                            strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 3, const_cast<__nv_bfloat16*>(x), dims, strides,
+                      box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                      CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return cudaErrorInvalidValue;
+  // narrow tiles: six rows of the first 32 cells
+  const cuuint64_t ndims[4] = {8, CIN / 8, kGrid, static_cast<cuuint64_t>(count) * kPadRows};
+  const cuuint64_t nstrides[3] = {16, CIN * 2, static_cast<cuuint64_t>(kGrid) * CIN * 2};
+  const cuuint32_t nbox[4] = {8, 1, kGrid / 2, 6};
+  r = encode(narrow, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(x), ndims, nstrides, nbox,
+             elem, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
 
@@ -1111,8 +1176,8 @@ cudaError_t launch_conv(const ConvArgs& a, int sm_count, cudaStream_t stream) {
   if (items == 0) return cudaSuccess;
   // planes are addressed by 32-bit cell coordinates
   if (static_cast<uint64_t>(a.count) * kPadRows * kGrid > 0x7FFFFFFFull) return cudaErrorInvalidValue;
-  CUtensorMap map;
-  cudaError_t e = conv_input_map<CIN>(a.x, a.count, &map);
+  CUtensorMap map, narrow;
+  cudaError_t e = conv_input_map<CIN>(a.x, a.count, &map, &narrow);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(conv3x3_tc_kernel<CIN, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            S::kBytes);
@@ -1120,7 +1185,7 @@ cudaError_t launch_conv(const ConvArgs& a, int sm_count, cudaStream_t stream) {
   // ~71 KB of shared memory (32 channels) and 64 TMEM columns per CTA: three
   // per SM (three CTAs' pipelines per SM measured faster than two deeper ones)
   const uint32_t grid = min(items, static_cast<uint32_t>(max(sm_count, 1) * kConvPerSm));
-  conv3x3_tc_kernel<CIN, EPI><<<grid, kConvThreads, S::kBytes, stream>>>(map, a);
+  conv3x3_tc_kernel<CIN, EPI><<<grid, kConvThreads, S::kBytes, stream>>>(map, narrow, a);
   return cudaGetLastError();
 }
 

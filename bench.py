@@ -289,6 +289,8 @@ def round0_sample(args, lat, segs, dev):
     cpu_costs, _, cells = oracle.astar_batch(lat, sample, threads=threads, counts=True)
     cpu_s = time.perf_counter() - t0
     ok = fres["completion"] != apgar_b200.COMPLETION_REJECTED
+    both = (fres["completion"] == apgar_b200.COMPLETION_REACHED) & \
+        (sres["completion"] == apgar_b200.COMPLETION_REACHED)
     peak, peak_kind = load_peaks()
     fbytes = cells.astype(np.float64).sum() * EXPANSION_BYTES + 4.0 * fres["path_len"].astype(np.float64).sum()
     achieved = fbytes / (f_ms / 1000.0) / 1e9
@@ -297,7 +299,12 @@ def round0_sample(args, lat, segs, dev):
         "round0_sample": {
             "segments": n, "frontier_ms": f_ms, "sweep_ms": s_ms, "frontier_over_sweep": s_ms / f_ms,
             "frontier_routes_per_s": n / (f_ms / 1000.0), "sweep_routes_per_s": n / (s_ms / 1000.0),
-            "same_costs": bool(np.array_equal(fres["cost"], sres["cost"])),
+            # over the segments both forms reached (a form rejects a segment
+            # when its window or queue bound is exceeded)
+            "same_costs": bool(np.array_equal(fres["cost"][both], sres["cost"][both])),
+            "both_reached": int(both.sum()),
+            "frontier_completion": np.bincount(fres["completion"], minlength=5).tolist(),
+            "sweep_completion": np.bincount(sres["completion"], minlength=5).tolist(),
         },
         "roofline": {
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
