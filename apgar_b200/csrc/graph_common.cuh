@@ -43,6 +43,9 @@ struct GraphLaunch {
   uint8_t generator;
   uint8_t workspace_mode;   // 1: converge fully and emit predecessors; 0: compact path
   const volatile uint32_t* cancel;  // host-mapped flag or nullptr
+  uint32_t max_policy_edges;  // the largest policy_count of the batch
+  uint32_t policy_smem_offset;  // where a query's edges are staged in shared memory, or ~0u
+  uint32_t nbr_smem_offset;     // where the neighbour table is staged in shared memory, or ~0u
 };
 
 struct PathCheckLaunch {

@@ -431,6 +431,7 @@ int run_batch(ViewObject* v, const apgar_b200_batch_request& req,
   L.generator = req.generator;
   L.workspace_mode = workspace_mode ? 1 : 0;
   L.cancel = v->cancel_dev;
+  for (uint64_t i = 0; i < Q; ++i) L.max_policy_edges = std::max(L.max_policy_edges, queries[i].policy_count);
 
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   APGAR_B200_CUDA("cudaEventCreate", cudaEventCreate(&t0));

@@ -43,10 +43,19 @@ __device__ __forceinline__ bool checked_add(uint64_t a, uint64_t b, uint64_t* ou
   return true;
 }
 
-__device__ __forceinline__ uint64_t load_label(const uint64_t* p) { return __ldcg(p); }
+// A label read while other threads of the CTA may lower it: at L2 for the
+// global slab, volatile for the shared-memory copy of a small graph.
+template <bool kShared>
+__device__ __forceinline__ uint64_t load_label(const uint64_t* p) {
+  if constexpr (kShared) {
+    return *reinterpret_cast<const volatile uint64_t*>(p);
+  } else {
+    return __ldcg(p);
+  }
+}
 
 __device__ __forceinline__ uint32_t nbr(const GraphDeviceView& g, uint32_t node, uint32_t d) {
-  return __ldg(g.neighbors + static_cast<size_t>(d) * g.node_count + node);
+  return g.neighbors[static_cast<size_t>(d) * g.node_count + node];  // global or staged
 }
 
 __device__ __forceinline__ uint64_t policy_adjustment(const apgar_b200_policy_edge_v1* pol,
@@ -54,13 +63,13 @@ __device__ __forceinline__ uint64_t policy_adjustment(const apgar_b200_policy_ed
   uint32_t lo = 0, hi = count;
   while (lo < hi) {
     const uint32_t mid = lo + (hi - lo) / 2u;
-    if (__ldg(&pol[mid].physical_edge_index) < edge) {
+    if (pol[mid].physical_edge_index < edge) {
       lo = mid + 1u;
     } else {
       hi = mid;
     }
   }
-  if (lo < count && __ldg(&pol[lo].physical_edge_index) == edge) return __ldg(&pol[lo].adjustment);
+  if (lo < count && pol[lo].physical_edge_index == edge) return pol[lo].adjustment;
   return 0;
 }
 
@@ -91,12 +100,13 @@ __device__ __forceinline__ bool transition_cost(const GraphDeviceView& g,
 
 // Canonical predecessor of state `s` (reference rule): the smallest
 // predecessor state index whose label plus the move cost equals label[s].
+template <bool kShared>
 __device__ uint32_t canonical_predecessor(const GraphDeviceView& g,
                                           const apgar_b200_batch_query_v1& q,
                                           const apgar_b200_policy_edge_v1* pol,
                                           const uint64_t* lab, uint32_t s) {
   const uint32_t node = s / 9u, h = s % 9u;
-  const uint64_t here = load_label(lab + s);
+  const uint64_t here = load_label<kShared>(lab + s);
   if (h == 8u || here == kGraphInf) return kInvalid32;
   const uint32_t pred = nbr(g, node, (h + 4u) & 7u);
   if (pred == kInvalid32) return kInvalid32;
@@ -104,7 +114,7 @@ __device__ uint32_t canonical_predecessor(const GraphDeviceView& g,
     if (ph == 8u && pred != q.start_node) continue;
     uint64_t t, c;
     if (!transition_cost(g, q, pol, pred, h, ph, &t)) continue;
-    if (checked_add(load_label(lab + pred * 9u + ph), t, &c) && c == here) return pred * 9u + ph;
+    if (checked_add(load_label<kShared>(lab + pred * 9u + ph), t, &c) && c == here) return pred * 9u + ph;
   }
   return kInvalid32;
 }
@@ -113,10 +123,17 @@ __device__ __forceinline__ void set_completion(apgar_b200_batch_result_v1& r, ui
   r.completion = static_cast<uint8_t>(c);
 }
 
+// kShared: the query's labels, queues and stamps, and the neighbour table,
+// live in shared memory (a graph small enough for them to fit: the drop-in
+// corpus has 10-697 nodes), so each round's label reads, atomics and
+// neighbour lookups stay on the SM; the labels are copied to the query's
+// global slab at the end where the host reads them.  Either form stages the
+// query's policy edges in shared memory when they fit.
+template <bool kShared>
 __global__ void __launch_bounds__(kThreads) graph_search_kernel(GraphLaunch p) {
   const uint32_t qi = blockIdx.x;
   if (qi >= p.query_count) return;
-  const GraphDeviceView& g = p.g;
+  GraphDeviceView g = p.g;
   const apgar_b200_batch_query_v1 q = p.queries[qi];
   const uint32_t N = g.node_count;
   const uint64_t S = 9ull * N;
@@ -124,8 +141,27 @@ __global__ void __launch_bounds__(kThreads) graph_search_kernel(GraphLaunch p) {
   uint32_t* queue0 = p.queues + static_cast<uint64_t>(qi) * 2u * N;
   uint32_t* queue1 = queue0 + N;
   uint32_t* stamp = p.stamps + static_cast<uint64_t>(qi) * N;
+  extern __shared__ __align__(16) uint8_t graph_smem[];
+  if constexpr (kShared) {
+    lab = reinterpret_cast<uint64_t*>(graph_smem);
+    queue0 = reinterpret_cast<uint32_t*>(graph_smem + S * 8u);
+    queue1 = queue0 + N;
+    stamp = queue1 + N;
+  }
   const apgar_b200_policy_edge_v1* pol = p.policy + q.policy_offset;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (p.policy_smem_offset != kInvalid32) {
+    // the query's policy edges, searched on every move, staged on the SM
+    auto* staged = reinterpret_cast<apgar_b200_policy_edge_v1*>(graph_smem + p.policy_smem_offset);
+    for (uint32_t i = tid; i < q.policy_count; i += kThreads) staged[i] = pol[i];
+    pol = staged;
+  }
+  if (p.nbr_smem_offset != kInvalid32) {
+    // the neighbour table [8][N], read on every move and path step
+    auto* staged = reinterpret_cast<uint32_t*>(graph_smem + p.nbr_smem_offset);
+    for (uint32_t i = tid; i < 8u * N; i += kThreads) staged[i] = __ldg(p.g.neighbors + i);
+    g.neighbors = staged;
+  }
 
   __shared__ uint32_t sh_count[2];
   __shared__ uint64_t sh_wmin[kThreads / 32];
@@ -180,7 +216,7 @@ __global__ void __launch_bounds__(kThreads) graph_search_kernel(GraphLaunch p) {
     for (uint32_t i = tid; i < count; i += kThreads) {
       const uint32_t n = qcur[i];
       for (uint32_t h = 0; h < 9u; ++h) {
-        const uint64_t v = load_label(lab + n * 9u + h);
+        const uint64_t v = load_label<kShared>(lab + n * 9u + h);
         local_min = v < local_min ? v : local_min;
       }
     }
@@ -222,7 +258,7 @@ __global__ void __launch_bounds__(kThreads) graph_search_kernel(GraphLaunch p) {
         uint64_t node_min = kGraphInf;
 #pragma unroll
         for (uint32_t h = 0; h < 9u; ++h) {
-          labs[h] = load_label(lab + n * 9u + h);
+          labs[h] = load_label<kShared>(lab + n * 9u + h);
           node_min = labs[h] < node_min ? labs[h] : node_min;
         }
         if (node_min >= threshold) {
@@ -280,7 +316,7 @@ __global__ void __launch_bounds__(kThreads) graph_search_kernel(GraphLaunch p) {
     __syncthreads();
     // best goal label after this round
     if (warp == 0) {
-      uint64_t gv = lane < 8 ? load_label(lab + static_cast<uint64_t>(q.goal_node) * 9u + lane) : kGraphInf;
+      uint64_t gv = lane < 8 ? load_label<kShared>(lab + static_cast<uint64_t>(q.goal_node) * 9u + lane) : kGraphInf;
       for (int o = 4; o > 0; o >>= 1) {
         const uint64_t other = __shfl_xor_sync(0xFFFFFFFFu, gv, o);
         gv = other < gv ? other : gv;
@@ -298,7 +334,7 @@ __global__ void __launch_bounds__(kThreads) graph_search_kernel(GraphLaunch p) {
   __shared__ uint32_t sh_goal_state;
   if (warp == 0) {
     const uint32_t s = q.goal_node * 9u + static_cast<uint32_t>(lane);
-    uint64_t v = lane < 8 ? load_label(lab + s) : kGraphInf;
+    uint64_t v = lane < 8 ? load_label<kShared>(lab + s) : kGraphInf;
     uint32_t st = lane < 8 ? s : kInvalid32;
     for (int o = 4; o > 0; o >>= 1) {
       const uint64_t ov = __shfl_xor_sync(0xFFFFFFFFu, v, o);
@@ -317,13 +353,17 @@ __global__ void __launch_bounds__(kThreads) graph_search_kernel(GraphLaunch p) {
   }
 
   if (p.workspace_mode) {
+    if constexpr (kShared) {
+      uint64_t* out = p.labels + static_cast<uint64_t>(qi) * S;
+      for (uint64_t s = tid; s < S; s += kThreads) out[s] = lab[s];
+    }
     uint32_t* pred = p.predecessors + static_cast<uint64_t>(qi) * S;
     uint64_t* own = p.state_owners + static_cast<uint64_t>(qi) * S;
     uint64_t* pown = p.predecessor_owners + static_cast<uint64_t>(qi) * S;
     for (uint64_t s = tid; s < S; s += kThreads) {
       pred[s] = (static_cast<uint32_t>(s) == q.start_node * 9u + 8u)
                     ? kInvalid32
-                    : canonical_predecessor(g, q, pol, lab, static_cast<uint32_t>(s));
+                    : canonical_predecessor<kShared>(g, q, pol, lab, static_cast<uint32_t>(s));
       own[s] = q.workspace_owner;
       pown[s] = q.workspace_owner;
     }
@@ -350,12 +390,12 @@ __global__ void __launch_bounds__(kThreads) graph_search_kernel(GraphLaunch p) {
         if (h == 8u) break;
         const uint32_t pred = nbr(g, node, (h + 4u) & 7u);
         if (pred == kInvalid32) break;
-        const uint64_t here = load_label(lab + cursor);
+        const uint64_t here = load_label<kShared>(lab + cursor);
         bool ok = false;
         if (lane < 9 && !(lane == 8 && pred != q.start_node)) {
           uint64_t t, c;
           ok = transition_cost(g, q, pol, pred, h, static_cast<uint32_t>(lane), &t) &&
-               checked_add(load_label(lab + pred * 9u + lane), t, &c) && c == here;
+               checked_add(load_label<kShared>(lab + pred * 9u + lane), t, &c) && c == here;
         }
         const unsigned ballot = __ballot_sync(0xFFFFFFFFu, ok);
         if (ballot == 0u) break;
@@ -444,9 +484,35 @@ __global__ void graph_pack_copy(const apgar_b200_compact_path_v1* compact, uint3
 
 }  // namespace
 
+// Shared-memory search for graphs whose labels, queues and stamps fit in
+// this many bytes (two CTAs per SM).
+constexpr size_t kSharedSearchBytes = 100 * 1024;
+// Policy edges staged in shared memory up to this many bytes (2048 edges).
+constexpr size_t kStagedPolicyBytes = 32 * 1024;
+
 cudaError_t launch_graph_search(const GraphLaunch& launch, cudaStream_t stream) {
   if (launch.query_count == 0) return cudaSuccess;
-  graph_search_kernel<<<launch.query_count, kThreads, 0, stream>>>(launch);
+  const size_t n = launch.g.node_count;
+  // shared layout: labels, queues and stamps; the neighbour table; the policy edges
+  const size_t state_bytes = (n * 9u * 8u + n * 12u + 15u) & ~static_cast<size_t>(15);
+  const size_t nbr_bytes = n * 8u * 4u;
+  const size_t policy_bytes = static_cast<size_t>(launch.max_policy_edges) * sizeof(apgar_b200_policy_edge_v1);
+  const size_t staged_policy = policy_bytes <= kStagedPolicyBytes ? policy_bytes : 0;
+  GraphLaunch l = launch;
+  l.policy_smem_offset = kInvalid32;
+  l.nbr_smem_offset = kInvalid32;
+  if (state_bytes + nbr_bytes + staged_policy <= kSharedSearchBytes) {
+    l.nbr_smem_offset = static_cast<uint32_t>(state_bytes);
+    if (staged_policy > 0) l.policy_smem_offset = static_cast<uint32_t>(state_bytes + nbr_bytes);
+    const cudaError_t e = cudaFuncSetAttribute(graph_search_kernel<true>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               static_cast<int>(kSharedSearchBytes));
+    if (e != cudaSuccess) return e;
+    graph_search_kernel<true><<<l.query_count, kThreads, state_bytes + nbr_bytes + staged_policy, stream>>>(l);
+  } else {
+    if (staged_policy > 0) l.policy_smem_offset = 0u;
+    graph_search_kernel<false><<<l.query_count, kThreads, staged_policy, stream>>>(l);
+  }
   return cudaGetLastError();
 }
 
