@@ -426,7 +426,8 @@ struct ConvSmem {
   static constexpr int kAccs = kConvAccs;               // 32-column accumulators
   static constexpr int kOffB = kStages * kBytesA;
   static constexpr int kOffBias = kOffB + kBytesB;      // 32 f32
-  static constexpr int kOffBar = kOffBias + 128;        // full, empty, accfull, accempty
+  static constexpr int kOffOut = kOffBias + 128;        // [4 warps][512 B] store staging
+  static constexpr int kOffBar = kOffOut + 4 * 512;     // full, empty, accfull, accempty
   static constexpr int kBytes = kOffBar + 8 * (2 * kStages + 2 * kAccs);
   static_assert(kPlane % 128 == 0 && kBytesA % 128 == 0, "TMA destinations are 128-byte aligned");
 };
@@ -664,26 +665,42 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const __grid_c
 #pragma unroll
         for (int c = 0; c < 32; ++c) o[c] = 0.f;
       }
-      if (py < kGrid) {
-        uint4* dst = reinterpret_cast<uint4*>(a.y + cell * kCh);
+      // A warp's 32 cells are 32 consecutive cells of one row (2 KB).  They
+      // go out through a 512-byte staging slot, eight cells per pass, so that
+      // every store instruction writes 512 contiguous bytes.
+      uint4 pk[4];
 #pragma unroll
-        for (int qq = 0; qq < 4; ++qq) dst[qq] = pack8(o + qq * 8);
-        if (tile.pitch < kGrid) {
-          // a narrow tile's columns 32 .. 63 lie outside the window: zeros
-          uint4* far = reinterpret_cast<uint4*>(a.y + act_cell(net, py, px + kGrid / 2) * kCh);
+      for (int qq = 0; qq < 4; ++qq) pk[qq] = pack8(o + qq * 8);
+      const int m0 = warp * 32;
+      const int py0 = y0 + m0 / tile.pitch, px0 = m0 % tile.pitch;
+      uint4* slot = reinterpret_cast<uint4*>(smem + S::kOffOut + warp * 512);
+      uint4* dst = reinterpret_cast<uint4*>(a.y + act_cell(net, py0, px0) * kCh);
+      const uint4 zero = make_uint4(0u, 0u, 0u, 0u);
 #pragma unroll
-          for (int qq = 0; qq < 4; ++qq) far[qq] = make_uint4(0u, 0u, 0u, 0u);
+      for (int pass = 0; pass < 4; ++pass) {
+        if ((lane >> 3) == pass) {
+#pragma unroll
+          for (int qq = 0; qq < 4; ++qq) slot[(lane & 7) * 4 + qq] = pk[qq];
         }
+        __syncwarp();
+        dst[pass * 32 + lane] = slot[lane];
+        __syncwarp();
       }
-      if (y0 == 0 && m < tile.pitch) {
+      if (tile.pitch < kGrid) {
+        // a narrow tile's columns 32 .. 63 lie outside the window: zeros
+        uint4* far = reinterpret_cast<uint4*>(a.y + act_cell(net, py0, px0 + kGrid / 2) * kCh);
+#pragma unroll
+        for (int pass = 0; pass < 4; ++pass) far[pass * 32 + lane] = zero;
+      }
+      if (y0 == 0 && m0 < tile.pitch) {
         // the zero pad row above the grid
-        uint4* pad = reinterpret_cast<uint4*>(a.y + act_cell(net, -1, m) * kCh);
+        uint4* pad = reinterpret_cast<uint4*>(a.y + act_cell(net, -1, px0) * kCh);
 #pragma unroll
-        for (int qq = 0; qq < 4; ++qq) pad[qq] = make_uint4(0u, 0u, 0u, 0u);
+        for (int pass = 0; pass < 4; ++pass) pad[pass * 32 + lane] = zero;
         if (tile.pitch < kGrid) {
-          uint4* far = reinterpret_cast<uint4*>(a.y + act_cell(net, -1, m + kGrid / 2) * kCh);
+          uint4* far = reinterpret_cast<uint4*>(a.y + act_cell(net, -1, px0 + kGrid / 2) * kCh);
 #pragma unroll
-          for (int qq = 0; qq < 4; ++qq) far[qq] = make_uint4(0u, 0u, 0u, 0u);
+          for (int pass = 0; pass < 4; ++pass) far[pass * 32 + lane] = zero;
         }
       }
     }
