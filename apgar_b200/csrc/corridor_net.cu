@@ -7,7 +7,9 @@
 // cw x ch cells lie inside the window.  Tensors are NHWC bf16 [net][66][64][C]
 // (grid row y stored at y + 1); the producers write the pad row above and
 // grid rows 0 .. ch with the cells outside the window as zeros ("same"
-// padding at the window border), which is all an in-window output reads.
+// padding at the window border), which is all an in-window output reads
+// (for a window at most 31 columns wide, the convolutions write columns
+// 0 .. 31 only).
 //
 // Layers 1-5 (3x3, 16 -> 32 then 32 -> 32, bias, ReLU) run as implicit GEMMs
 // on the 5th-generation tensor cores: a tile is 128 output cells (two rows of
@@ -686,22 +688,13 @@ __global__ void __launch_bounds__(kConvThreads) conv3x3_tc_kernel(const __grid_c
         dst[pass * 32 + lane] = slot[lane];
         __syncwarp();
       }
-      if (tile.pitch < kGrid) {
-        // a narrow tile's columns 32 .. 63 lie outside the window: zeros
-        uint4* far = reinterpret_cast<uint4*>(a.y + act_cell(net, py0, px0 + kGrid / 2) * kCh);
-#pragma unroll
-        for (int pass = 0; pass < 4; ++pass) far[pass * 32 + lane] = zero;
-      }
+      // (a narrow tile's columns 32 .. 63 are left as they are: only narrow
+      // tiles, which never read them, consume this net's activations)
       if (y0 == 0 && m0 < tile.pitch) {
         // the zero pad row above the grid
         uint4* pad = reinterpret_cast<uint4*>(a.y + act_cell(net, -1, px0) * kCh);
 #pragma unroll
         for (int pass = 0; pass < 4; ++pass) pad[pass * 32 + lane] = zero;
-        if (tile.pitch < kGrid) {
-          uint4* far = reinterpret_cast<uint4*>(a.y + act_cell(net, -1, px0 + kGrid / 2) * kCh);
-#pragma unroll
-          for (int pass = 0; pass < 4; ++pass) far[pass * 32 + lane] = zero;
-        }
       }
     }
   }
@@ -886,16 +879,20 @@ __global__ void __launch_bounds__(256, 3) head_forward_kernel(const __nv_bfloat1
     return;
   }
   for (int i = threadIdx.x; i < 9 * kCh; i += blockDim.x) ws[i] = w6[i];
-  // window rows of the halo: y0 - 1 .. y0 + kHeadRows, clipped to [0, ch)
+  // window rows of the halo: y0 - 1 .. y0 + kHeadRows, clipped to [0, ch);
+  // the first 32 columns only when the window is no wider
   const int r0 = max(y0 - 1, 0), r1 = min(y0 + kHeadRows, ch - 1);
+  const int cols = cw <= kGrid / 2 ? kGrid / 2 : kGrid;
   const uint8_t* src = reinterpret_cast<const uint8_t*>(act + act_cell(net, r0, 0) * kCh);
-  const int chunks = (r1 - r0 + 1) * kGrid * 4;
+  const int chunks = (r1 - r0 + 1) * cols * 4;
   const uint32_t base = static_cast<uint32_t>(__cvta_generic_to_shared(hs));
   for (int u = threadIdx.x; u < chunks; u += blockDim.x) {
-    const int c = u >> 2, q = u & 3;                  // staged cell (rows from r0), chunk
-    const int slot = (r0 - (y0 - 1)) * kGrid + c;     // stage row 0 is y0 - 1
+    const int q = u & 3, cc = u >> 2;
+    const int row = cc / cols, col = cc % cols;           // from r0
+    const int c = row * kGrid + col;                      // staged cell (rows from r0)
+    const int slot = (r0 - (y0 - 1)) * kGrid + c;         // stage row 0 is y0 - 1
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(base + slot * 64 + ((q ^ (c & 3)) << 4)),
-                 "l"(src + static_cast<size_t>(u) * 16)
+                 "l"(src + (static_cast<size_t>(c) * 4 + q) * 16)
                  : "memory");
   }
   asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");

@@ -681,7 +681,9 @@ APGAR_B200_API int apgar_b200_compile_legal_edges(const apgar_b200_edge_rules* r
  * net's window as zeros: the pad row above the grid and grid rows 0 .. ch
  * (coarse height ch; row ch is all zeros).  Rows below are left as they are:
  * they reach only cells outside the window, whose outputs are written as
- * zeros, and the gradients read inputs inside the window only;
+ * zeros, and the gradients read inputs inside the window only.  So are the
+ * convolutions' columns 32 .. 63 of a window at most 31 coarse columns wide,
+ * whose tiles cover columns 0 .. 31 only (the rasters write all 64);
  * logits and dlogit f32 [count][64][64]; labels u8
  * [count][64][64]; dims u32 [count] (coarse width | height << 8 | scale << 16).
  * params f32 [apgar_b200_cnn_param_count()]: per layer l w[32][9][cin_l] then
