@@ -400,14 +400,19 @@ __device__ __forceinline__ uint4 halo_chunk(const uint8_t* halo, int m, int t, i
 // cells.  The A operand of tap (dy, dx) for the 128 output cells is the
 // staged run that starts at cell (1 + dy) * 64 + dx: K-major, 8-cell groups
 // 128 bytes apart (SBO), the two chunks of a K = 16 step one plane apart
-// (LBO).  No im2col copy.  B: the weights, [32 rows][9 * CIN], K-major.
+// (LBO).  No im2col copy.  B: the weights, [32 rows][9 * CIN], K-major.  A
+// narrow tile (a window at most 31 columns wide) stages rows y0 - 1 .. y0 + 4
+// of 32 cells instead and its runs use a 32-cell row pitch.
 //
 // Roles (warp-specialised, 192 threads): warp 4 lane 0 loads stages with TMA
 // (a 3-D tensor map over the NHWC tensor, {8 channels, chunk, cell}, whose
 // box {8, 1, 256} lands one plane: the NHWC -> planar transposition is done
-// by the copy engine); warp 5 lane 0 issues the MMAs; warps 0-3 (TMEM lanes
-// 0-127) drain the accumulators.  Stages and accumulators form rings handed
-// over by mbarriers, so loads, MMAs and epilogues of different tiles overlap.
+// by the copy engine; narrow tiles through a 4-D map, box {8, 1, 32, 6});
+// warp 5 lane 0 issues the MMAs; warps 0-3 (TMEM lanes 0-127) drain the
+// accumulators and store each warp's 32 cells through a 512-byte shared slot
+// (every store instruction 512 contiguous bytes).  Stages and accumulators
+// form rings handed over by mbarriers, so loads, MMAs and epilogues of
+// different tiles overlap.
 // Pipeline depth: stages (A tiles in flight) and accumulators per CTA, CTAs
 // per SM.
 constexpr int kConvStages = 3, kConvAccs = 2, kConvPerSm = 3;
