@@ -64,6 +64,8 @@ SRCS=(
   src/gpu/planar_router.cc
   src/adapters/kicad_fixture.cc
   src/benchmark/planar_corpus.cc
+  src/candidates/route_candidate.cc
+  src/candidates/gpu_candidate_adapter.cc
 )
 mkdir -p "$PATCHED/obj"
 OBJS=()
@@ -77,9 +79,6 @@ for src in "${SRCS[@]}"; do
   OBJS+=("$obj")
 done
 for pid in "${PIDS[@]}"; do wait "$pid"; done  # each compile's own status
-# the candidate adapter's generator switch: compiled only (not linked here)
-"$CXX" "${PFLAGS[@]}" -c "$PATCHED/src/candidates/gpu_candidate_adapter.cc" \
-  -o "$PATCHED/obj/gpu_candidate_adapter.o"
 rm -f "$PATCHED/libapgar_ref_patched.a"
 ar rcs "$PATCHED/libapgar_ref_patched.a" "${OBJS[@]}"
 "$CXX" "${PFLAGS[@]}" -Wall -Wextra -I"$ROOT/include" -c "$HERE/b200_planar_backend.cc" \

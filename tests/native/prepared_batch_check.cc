@@ -17,7 +17,13 @@
 //    generator.  Every reached item must be sealed with authenticated CUDA
 //    producer evidence at the reference CPU A* cost, and every other item
 //    must be the CPU A*'s own outcome.  RouteWithPreparedPlanarGpuBackend
-//    (single route) must give the CPU cost too.
+//    (single route) must give the CPU cost too.  Every sealed item is then
+//    turned into a route candidate by the reference's candidate adapter
+//    (BuildGeneratedCandidateFromGpuBatchItem, one item at a time, and
+//    BuildGeneratedCandidatesFromGpuBatchItems over the batch, which must
+//    agree), with the CUDA provenance of its generator, and the candidate
+//    must pass the reference's admission (AdmitRouteCandidate: exact
+//    geometry, resources, metrics and signatures recomputed).
 // 2. Each of the reference's fault classes, injected on the host by the
 //    decorator over the shim, must fail the first query (or the whole batch,
 //    or the route) with the invariant id the reference names for it.
@@ -33,6 +39,8 @@
 #include <vector>
 
 #include "apgar/benchmark/planar_corpus.h"
+#include "apgar/candidates/gpu_candidate_adapter.h"
+#include "apgar/candidates/route_candidate.h"
 #include "apgar/gpu/cuda_backend.h"
 #include "apgar/gpu/fault_injecting_backend.h"
 #include "apgar/gpu/planar_router.h"
@@ -49,6 +57,7 @@ using gpu::PlanarGenerator;
 namespace {
 
 int failures = 0;
+std::size_t admitted = 0;  // sealed items the candidate adapter and admission accepted
 void check(bool ok, const std::string& what) {
   if (!ok) {
     ++failures;
@@ -142,6 +151,64 @@ const char* name_of(PlanarGenerator g) {
   return g == PlanarGenerator::kB200Persistent ? "persistent" : "persistent-workspace";
 }
 
+// The sealed items of one batch through the reference's candidate adapter and
+// admission; the candidate generator kind follows the patched mapping
+// (compact paths as the sweep's, the full workspace as the frontier's).
+void convert_items(const benchmark::PlanarCorpusCase& c,
+                   const std::vector<gpu::PlanarCandidateBatchQuery>& queries,
+                   const gpu::PlanarCandidateBatch& batch, PlanarGenerator g, const std::string& tag) {
+  const candidates::CandidateGeneratorKind kind = g == PlanarGenerator::kB200Persistent
+                                                      ? candidates::CandidateGeneratorKind::kCudaSweep
+                                                      : candidates::CandidateGeneratorKind::kCudaFrontier;
+  std::vector<routing::NormalizedCandidateGenerationPolicy> policies;
+  policies.reserve(queries.size());
+  for (const auto& q : queries) {
+    auto norm = routing::NormalizeCandidateGenerationPolicy(c.compiled_board, q.request.candidate_policy);
+    if (auto* np = std::get_if<routing::NormalizedCandidateGenerationPolicy>(&norm)) {
+      policies.push_back(*np);
+    } else {
+      check(false, tag + ": policy normalisation failed");
+      return;
+    }
+  }
+  std::vector<candidates::GpuCandidateBatchBuildRequest> requests;
+  std::vector<candidates::CandidateDraftBuildResult> singles;
+  for (const gpu::PlanarCandidateBatchItem& item : batch.items) {
+    if (std::get_if<gpu::PlanarGpuRoute>(&item.result()) == nullptr) continue;
+    const std::size_t i = static_cast<std::size_t>(item.query_id() - 1);
+    if (i >= queries.size()) continue;  // reported by the caller
+    const std::string qtag = tag + " query " + std::to_string(item.query_id());
+    requests.push_back(candidates::GpuCandidateBatchBuildRequest{
+        .query = queries[i], .normalized_policy = policies[i], .item = item});
+    singles.push_back(candidates::BuildGeneratedCandidateFromGpuBatchItem(
+        c.board, c.compiled_board, queries[i], policies[i], batch, item));
+    const auto* gen = std::get_if<candidates::GeneratedRouteCandidate>(&singles.back());
+    if (gen == nullptr) {
+      const auto& rej = std::get<candidates::CandidateRejection>(singles.back());
+      check(false, qtag + ": candidate rejected: " + rej.invariant_id + " " + rej.detail);
+      continue;
+    }
+    check(gen->provenance.generator == kind, qtag + ": candidate generator kind");
+    check(gen->provenance.backend == candidates::CandidateBackendKind::kCuda, qtag + ": CUDA backend");
+    check(gen->provenance.query_identity == item.query_id(), qtag + ": query identity");
+    const auto admission = candidates::AdmitRouteCandidate(
+        candidates::CandidateAdmissionContext{c.board, c.compiled_board, queries[i].request}, *gen);
+    if (const auto* rej = std::get_if<candidates::CandidateRejection>(&admission)) {
+      check(false, qtag + ": admission rejected: " + rej->invariant_id + " " + rej->detail);
+      continue;
+    }
+    ++admitted;
+  }
+  const auto batched =
+      candidates::BuildGeneratedCandidatesFromGpuBatchItems(c.board, c.compiled_board, batch, requests);
+  if (const auto* list = std::get_if<std::vector<candidates::CandidateDraftBuildResult>>(&batched)) {
+    check(*list == singles, tag + ": batch conversion equals the per-item conversion");
+  } else {
+    const auto& f = std::get<candidates::GpuCandidateBatchBuildFailure>(batched);
+    check(false, tag + ": batch conversion failed: " + f.invariant_id + " " + f.detail);
+  }
+}
+
 // Part 1: one case through the prepared batch and single-route paths.
 std::size_t run_case(const benchmark::PlanarCorpusCase& c, gpu::IPlanarRouteBackend& backend,
                      std::uint64_t batch_id) {
@@ -205,6 +272,7 @@ std::size_t run_case(const benchmark::PlanarCorpusCase& c, gpu::IPlanarRouteBack
               qtag + ": failure " + f.invariant_id + " " + f.detail);
       }
     }
+    convert_items(c, queries, batch, g, tag);
   }
   return sealed;
 }
@@ -320,8 +388,9 @@ int main() {
   // compact-path class), which the corpus lists last
   run_faults(corpus.back(), *backend);
   if (failures == 0) {
-    std::printf("prepared ok: %zu cases, %zu items sealed at the CPU A* cost, 13 fault classes\n",
-                corpus.size(), sealed);
+    std::printf("prepared ok: %zu cases, %zu items sealed at the CPU A* cost, %zu route candidates "
+                "built and admitted by the reference's candidate adapter, 13 fault classes\n",
+                corpus.size(), sealed, admitted);
     return 0;
   }
   std::printf("prepared FAILED: %d checks\n", failures);
