@@ -210,8 +210,8 @@ __host__ __device__ inline GroupSmem group_smem(int L, int G, int max_rows) {
   size_t off = 0;
   s.modified = off;
   off += (static_cast<size_t>(max_rows) * sizeof(int16_t) + 15) & ~size_t(15);
-  s.edges = off;  // [G][L][first, last] of the previous row
-  off += static_cast<size_t>(G) * L * 2 * sizeof(uint32_t);
+  s.edges = off;  // [2 buffers][G][L][first, last] of the previous row
+  off += 2 * static_cast<size_t>(G) * L * 2 * sizeof(uint32_t);
   s.sums = off;  // [G][L][aE, bE, aW, bW]
   off += static_cast<size_t>(G) * L * 4 * sizeof(uint32_t);
   s.flags = off;  // [2 parities][G]: bit 0 via improved, bit 1 changed, bit 8+l layer l changed
@@ -260,7 +260,8 @@ __global__ void __launch_bounds__(groups_per_block(G) * G * 32)
   const GroupSmem gs = group_smem(L, G, max_rows);
   unsigned char* my_smem = smem_raw + gs.total * gi;
   int16_t* modified = reinterpret_cast<int16_t*>(my_smem + gs.modified);
-  uint32_t* sh_edge = reinterpret_cast<uint32_t*>(my_smem + gs.edges);
+  uint32_t* const sh_edges = reinterpret_cast<uint32_t*>(my_smem + gs.edges);
+  constexpr int kEdgeBuf = G * L * 2;  // entries of one edge buffer
   uint32_t* sh_sum = reinterpret_cast<uint32_t*>(my_smem + gs.sums);
   uint32_t* sh_flags = reinterpret_cast<uint32_t*>(my_smem + gs.flags);
 
@@ -297,6 +298,10 @@ __global__ void __launch_bounds__(groups_per_block(G) * G * 32)
 
     bool converged = false, cancelled = false;
     int parity = 0;
+    // The row step reads its predecessor row's warp-edge labels from buffer
+    // eb and publishes its own into the other buffer before its last group
+    // vote, which therefore also ends the step (no barrier of its own).
+    int eb = 0;
     uint32_t prv[L][C], nxt[L][C];
     uint32_t pf[L], nf[L], nvb[L];
     for (uint32_t k = 1; k <= p.max_sweeps; ++k) {
@@ -355,7 +360,7 @@ __global__ void __launch_bounds__(groups_per_block(G) * G * 32)
             if (lane == 0 || lane == 31) {
 #pragma unroll
               for (int l = 0; l < L; ++l) {
-                sh_edge[(g * L + l) * 2 + (lane == 0 ? 0 : 1)] =
+                sh_edges[eb * kEdgeBuf + (g * L + l) * 2 + (lane == 0 ? 0 : 1)] =
                     lane == 0 ? prv[l][0] : prv[l][C - 1];
               }
             }
@@ -432,6 +437,7 @@ __global__ void __launch_bounds__(groups_per_block(G) * G * 32)
           uint32_t left = __shfl_up_sync(0xFFFFFFFFu, prv[l][C - 1], 1);
           uint32_t right = __shfl_down_sync(0xFFFFFFFFu, prv[l][0], 1);
           if constexpr (G > 1) {
+            const uint32_t* const sh_edge = sh_edges + eb * kEdgeBuf;
             if (lane == 0) left = (g > 0) ? sh_edge[((g - 1) * L + l) * 2 + 1] : kLabelInf;
             if (lane == 31) right = (g + 1 < G) ? sh_edge[((g + 1) * L + l) * 2 + 0] : kLabelInf;
           } else {
@@ -612,6 +618,17 @@ __global__ void __launch_bounds__(groups_per_block(G) * G * 32)
           }
           uint32_t warp_flags = __reduce_or_sync(0xFFFFFFFFu, lane_flags);
           if constexpr (G > 1) {
+            // this pass's row edges for the next step (final if the vote ends
+            // the row): buffer eb ^ 1 is read by no warp until the next step,
+            // and every read of it by the previous step came before this
+            // step's first barrier
+            if (lane == 0 || lane == 31) {
+#pragma unroll
+              for (int l = 0; l < L; ++l) {
+                sh_edges[(eb ^ 1) * kEdgeBuf + (g * L + l) * 2 + (lane == 0 ? 0 : 1)] =
+                    lane == 0 ? v[l][0] : v[l][C - 1];
+              }
+            }
             if (lane == 0) sh_flags[parity * G + g] = warp_flags;
             group_sync<G>(barrier_id);
             warp_flags = 0;
@@ -636,14 +653,6 @@ __global__ void __launch_bounds__(groups_per_block(G) * G * 32)
           any_change = true;
         }
         ++stat_rows;
-        if constexpr (G > 1) {
-          if (lane == 0 || lane == 31) {
-#pragma unroll
-            for (int l = 0; l < L; ++l) {
-              sh_edge[(g * L + l) * 2 + (lane == 0 ? 0 : 1)] = lane == 0 ? v[l][0] : v[l][C - 1];
-            }
-          }
-        }
 #pragma unroll
         for (int l = 0; l < L; ++l) {
 #pragma unroll
@@ -651,8 +660,12 @@ __global__ void __launch_bounds__(groups_per_block(G) * G * 32)
           pf[l] = cf[l];
         }
         have_prev = true;
-        // edges and the modified map are read by the whole group next step
-        group_sync<G>(barrier_id);
+        eb ^= 1;
+        // The step's last vote barrier published the edges; every thread
+        // wrote modified[r] itself (the same value) and reads only its own
+        // lane's cells of the slab.  A faulted row left the pass loop before
+        // its vote, so it ends with a barrier of its own.
+        if (fault) group_sync<G>(barrier_id);
       }
       if (!any_change && k >= 2) {
         converged = true;
