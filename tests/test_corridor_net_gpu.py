@@ -186,6 +186,74 @@ def test_training_lowers_the_loss_and_certifies_more_nets():
         dev_h.close()
 
 
+def _band_of_area(nets, areas):
+    """The unlearned corridor of each net with exactly areas[i] coarse cells
+    inside its window: the cells nearest the start-goal segment (Chebyshev
+    distance, then Euclidean), plus both terminals."""
+    (sx, sy), (gx, gy), _ = corridor.terminals_coarse(nets)
+    g = corridor.COARSE
+    ys, xs = np.mgrid[0:g, 0:g]
+    out = np.zeros((len(nets), g, g), dtype=bool)
+    for i in range(len(nets)):
+        _, cw, ch = corridor.coarse_dims(nets["win_w"][i], nets["win_h"][i])
+        inside = ((xs < cw) & (ys < ch)).ravel()
+        steps = int(max(abs(gx[i] - sx[i]), abs(gy[i] - sy[i]), 1))
+        t = np.linspace(0.0, 1.0, 2 * steps + 1)
+        px = sx[i] + t * (gx[i] - sx[i])
+        py = sy[i] + t * (gy[i] - sy[i])
+        cheb = np.maximum(np.abs(xs[..., None] - np.rint(px)),
+                          np.abs(ys[..., None] - np.rint(py))).min(axis=2).ravel()
+        eucl = np.hypot(xs[..., None] - px, ys[..., None] - py).min(axis=2).ravel()
+        order = np.lexsort((eucl, cheb))
+        order = order[inside[order]]
+        mask = np.zeros(g * g, dtype=bool)
+        mask[order[:int(areas[i])]] = True
+        mask[int(sy[i]) * g + int(sx[i])] = True
+        mask[int(gy[i]) * g + int(gx[i])] = True
+        out[i] = mask.reshape(g, g)
+    return out
+
+
+def test_trained_corridors_certify_more_than_unlearned_corridors_of_equal_area():
+    """What the shipped network gains over the method without it: on held-out
+    nets of the medium distribution, at the corridor sizes the learned form
+    uses, its corridors are certified more often than the fixed start-goal
+    band with exactly the same number of coarse cells per net (measured:
+    0.62 against 0.54 at dilation 1, 0.94 against 0.91 at the shipped policy's
+    dilation 3); neither changes a result.  At much tighter corridors
+    (threshold 0, no dilation) the band does as well or better, so the policy
+    stays in this range."""
+    lat, nets = synth.config_medium(5, nets=256, size=1024)
+    cells = nets["win_w"].astype(np.int64) * nets["win_h"].astype(np.int64) * lat.layers
+    policy = learned.load_policy()
+    nets = np.ascontiguousarray(nets[cells <= policy["max_window_cells"]])
+    dev = apgar_b200.DeviceLattice(lat)
+    try:
+        plan = dev.plan(nets, generator="frontier")
+        plan.execute()
+        plain, _ = plan.readback(want_paths=False)
+        r, d = learned.rasters(plan)
+        logits = learned.CorridorNet.load().forward(r, d)
+
+        def certified(words):
+            plan.set_corridors(words)
+            plan.execute()
+            res, _ = plan.readback(want_paths=False)
+            assert np.array_equal(res["cost"], plain["cost"])  # results never depend on it
+            return float((plan.corridor_status() == corridor.CERTIFIED).mean())
+
+        rates = {}
+        for dilate, margin in ((1, 0.04), (policy["dilate"], 0.0)):
+            bits = learned.corridors(plan, logits, d, threshold=policy["threshold"], dilate=dilate)
+            areas = corridor.unpack(_u32(bits)).sum(axis=(1, 2))
+            band = torch.from_numpy(corridor.pack(_band_of_area(nets, areas)).view(np.int32))
+            rates[dilate] = (certified(bits), certified(band.cuda().view(torch.uint32)))
+            assert rates[dilate][0] > rates[dilate][1] + margin, rates
+        plan.close()
+    finally:
+        dev.close()
+
+
 def test_window_limit_proposes_no_corridor():
     import torch
 
