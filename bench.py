@@ -322,6 +322,18 @@ def round0_sample(args, lat, segs, dev):
     }
 
 
+def medium_config(args, world, lat):
+    """The medium workload's `config`, the same dict in both arms (what
+    differs between runs, such as the frontier schedule, is reported beside
+    it)."""
+    return {
+        "workload": WORKLOAD, "nets_per_gpu": args.nets,
+        "lattice": [lat.layers, lat.height, lat.width], "seed": args.seed,
+        "parallelism": f"weak x{world} (independent net batches)",
+        "l2": "label words (5.4 GB) larger than L2 (126 MB) and cleared every step",
+    }
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -343,7 +355,8 @@ def run_reference(args, rank, world):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1000.0 / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u32",
         "data": "synthetic",
-        "config": {"workload": WORKLOAD, "step": f"A* over {len(sample)} nets of the batch"},
+        "config": medium_config(args, world, lat),
+        "form": f"CPU A* port over {len(sample)} nets of the batch per step",
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": f"{len(sample)} nets per step, all {threads} host threads"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -855,16 +868,12 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": avg_ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic",
-            "config": {
-                "workload": WORKLOAD, "form": "persistent work-stealing frontier (bucketed A*)",
-                "nets_per_gpu": len(nets), "lattice": [lat.layers, lat.height, lat.width],
-                "seed": args.seed, "parallelism": f"weak x{world} (independent net batches)",
-                "l2": "label words (5.4 GB) larger than L2 (126 MB) and cleared every step",
-                "certified_per_step": cert_all,
-                "schedule": dict(schedule.describe(),
-                                 chosen_by="autotuner (untimed, on this batch)" if tuning else "default"),
-                "tuning_ms": [[row[0], row[1]] for row in tuning],
-            },
+            "config": medium_config(args, world, lat),
+            "form": "persistent work-stealing frontier (bucketed A*)",
+            "certified_per_step": cert_all,
+            "schedule": dict(schedule.describe(),
+                             chosen_by="autotuner (untimed, on this batch)" if tuning else "default"),
+            "tuning_ms": [[row[0], row[1]] for row in tuning],
             "gpu_launches": int(info["kernel_launches"]) * args.steps,
             "roofline": {
                 "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
