@@ -62,10 +62,18 @@ def test_generator_patch_applies_to_the_reference(tmp_path):
 @pytest.mark.gpu
 def test_prepared_batch_path_of_the_reference_on_gpu():
     """RouteCandidateBatchWithPreparedPlanarGpuBackend of the patched reference
-    over this backend: every corpus item sealed at the CPU A* cost, and every
-    fault class raises the reference's invariant id."""
+    over this backend: every corpus item sealed at the CPU A* cost, every
+    sealed item turned into a route candidate by the reference's candidate
+    adapter and admitted, and every fault class raises the reference's
+    invariant id."""
+    import re
+
     if not os.path.exists(PREPARED):
         pytest.skip("prepared-path check not built (needs the reference sources at build time)")
     out = subprocess.run([PREPARED], capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, (out.stdout + out.stderr)[-4000:]
-    assert "prepared ok" in out.stdout
+    m = re.search(r"prepared ok: (\d+) cases, (\d+) items sealed at the CPU A\* cost, (\d+) route "
+                  r"candidates built and admitted", out.stdout)
+    assert m is not None, out.stdout[-2000:]
+    cases, sealed, admitted = (int(g) for g in m.groups())
+    assert cases == 11 and sealed > 0 and admitted == sealed, m.group(0)
