@@ -87,3 +87,8 @@ def test_reference_arm_prints_one_json_line():
                 "cpu_baseline", "e2e", "config"):
         assert key in line
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "port"
+    # the same static config dict as the device arm's line (medium_config)
+    assert line["config"] == {
+        "workload": line["config"]["workload"], "nets_per_gpu": 32, "lattice": [4, 256, 256],
+        "seed": 2, "parallelism": "weak x1 (independent net batches)",
+        "l2": "label words (5.4 GB) larger than L2 (126 MB) and cleared every step"}
